@@ -1,0 +1,248 @@
+/*
+ * stardust_pm.h -- C ABI of the B200 particle-mesh gravity step.
+ *
+ * This is the drop-in boundary for the reference's PM path. The reference
+ * (chdnl0420-svg/stardust) exposes it as the C++ class `Sim`
+ * (src/sim/Sim.h:854-1135), a Pimpl that owns every device buffer. This header
+ * restates the same operations as plain C: an opaque handle, POD config,
+ * plain pointers and sizes, integer status codes. No CUDA or torch types appear
+ * in any signature; streams are passed as `void*` (a cudaStream_t).
+ *
+ * Error convention (reference: sticky g_failed / g_failMsg, Sim.cu:52-75). Every
+ * call returns SD_OK (0) or a negative SD_E* code. The first failure is recorded
+ * process-wide (sd_failed / sd_last_error); unlike the reference, later calls are
+ * not silently skipped: they still validate and run, so one bad call does not
+ * poison unrelated handles. A CUDA error inside a kernel launch marks the handle
+ * failed and its later step calls return SD_E_CUDA.
+ *
+ * Units: positions in box units [0,1), periodic box of side 1. Densities are in
+ * count units (each particle deposits total weight 1), as in the reference.
+ */
+#ifndef STARDUST_PM_H
+#define STARDUST_PM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SD_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------------- */
+enum {
+    SD_OK = 0,
+    SD_E_ARG = -1,        /* invalid argument (null pointer, bad size, bad enum) */
+    SD_E_CUDA = -2,       /* a CUDA runtime call or kernel failed */
+    SD_E_NOMEM = -3,      /* device allocation failed / does not fit */
+    SD_E_STATE = -4,      /* call not valid in the current state (e.g. not initialised) */
+    SD_E_IO = -5,         /* state file could not be read or written */
+    SD_E_FORMAT = -6,     /* state file is not a valid STARDUST v1/v2 file */
+    SD_E_UNSUPPORTED = -7 /* configuration this build does not implement */
+};
+
+/* ---- enums ----------------------------------------------------------------- */
+/* Boundary (Sim.h:20 `enum class Boundary { Isolated, Periodic }`). */
+enum { SD_BOUNDARY_ISOLATED = 0, SD_BOUNDARY_PERIODIC = 1 };
+
+/* Particle order used by the sort (Sim.cu:2476-2486 is SD_ORDER_ROWMAJOR). */
+enum {
+    SD_ORDER_ROWMAJOR = 0, /* reference key: (cz*G+cy)*G+cx of the containing cell */
+    SD_ORDER_MORTON = 1,   /* 30-bit Morton code of the containing cell */
+    SD_ORDER_TILED = 2     /* CIC base-cell rows in 4x4 row tiles (fused deposit/gather) */
+};
+
+/* Time integrator. SD_INT_KD is the reference's kick-then-drift
+ * (kIntegrate Sim.cu:822,842). SD_INT_KDK is leapfrog: the first step opens
+ * with a half kick, later steps kick by (dt_prev + dt)/2, and sd_synchronize
+ * closes with the last half kick. */
+enum { SD_INT_KD = 0, SD_INT_KDK = 1 };
+
+/* Force units. SD_UNITS_REFERENCE: a = -(gravity/N) grad(phi), lap(phi) = counts
+ * (Sim.cu:3107-3109, 528-557). SD_UNITS_NEWTON: Newtonian gravity with
+ * G_N = gravity and total mass 1 (each particle 1/N), i.e. the reference
+ * formula scaled by 4*pi*G^3. */
+enum { SD_UNITS_REFERENCE = 0, SD_UNITS_NEWTON = 1 };
+
+/* Memory side of a pointer argument. */
+enum { SD_HOST = 0, SD_DEVICE = 1 };
+
+/* ---- configuration (SimConfig, Sim.h:157-796; plain-PM fields) ------------- */
+typedef struct sd_config {
+    int32_t particle_count;   /* SimConfig::particleCount (Sim.h:166) */
+    int32_t grid_size;        /* SimConfig::gridSize (Sim.h:167); clamped to a power of two in [16,512] */
+    int32_t boundary;         /* SimConfig::boundary (Sim.h:278) */
+    float gravity;            /* SimConfig::gravity (Sim.h:280) */
+    float softening_cells;    /* SimConfig::softeningCells (Sim.h:315), Gaussian in k for periodic */
+    float time_scale;         /* SimConfig::timeScale (Sim.h:316): sd_step_auto dt = 0.0016*dtScaleFor(ts) */
+    int32_t sort_interval;    /* SimConfig::sortInterval (Sim.h:317); 0 = never sort */
+    float length_scale;       /* SimConfig::lengthScale (Sim.h:172), light-speed clamp */
+    float time_unit_scale;    /* SimConfig::timeUnitScale (Sim.h:180), light-speed clamp */
+    int32_t order;            /* SD_ORDER_* */
+    int32_t integrator;       /* SD_INT_* */
+    int32_t units;            /* SD_UNITS_* */
+    int32_t diagnostics;      /* 1 = FP64 energy and momentum every step (sd_diagnostics) */
+    int32_t keep_density;     /* 1 = keep the step-start density for sd_density_device_ptr (4 B/cell more traffic) */
+    int32_t reserved[6];
+} sd_config;
+
+/* Per-step timings (SimTimings, Sim.h:844-852), milliseconds of device time. */
+typedef struct sd_timings {
+    float sort_ms;     /* key + radix sort + reorder */
+    float deposit_ms;  /* CIC deposit (+ the first FFT pass where fused) */
+    float poisson_ms;  /* FFT passes and Green's function */
+    float gather_ms;   /* gather + kick + drift */
+    float total_ms;
+    float dt_used;
+    float max_speed;
+    int32_t steps;     /* steps covered by these numbers */
+} sd_timings;
+
+/* FP64 diagnostics of the last step (computed on the device). */
+typedef struct sd_diagnostics {
+    double kinetic;      /* sum 1/2 m v^2, m = 1/N (after momentum zeroing) */
+    double potential;    /* 1/2 sum m phi(x_i), phi in the configured units */
+    double momentum[3];  /* sum m v (after zeroing: ~0) */
+    double mean_velocity_removed[3];
+    double live_count;
+} sd_diagnostics;
+
+typedef struct sd_sim sd_sim;  /* opaque; the reference's Sim::Impl */
+
+/* ---- process-level --------------------------------------------------------- */
+int sd_abi_version(void);
+/* Sim::deviceAvailable (Sim.cu:3903-3906). Returns 1 when a CUDA device exists. */
+int sd_device_available(void);
+/* Sim::failed / Sim::failMessage (Sim.h:994-995). */
+int sd_failed(void);
+const char* sd_last_error(void);
+void sd_clear_error(void);
+/* Default config: the reference's SimConfig defaults for the plain-PM fields
+ * (boundary periodic, gravity 1, sortInterval 1, softening 3 cells). */
+int sd_config_default(sd_config* cfg);
+/* Sim::maxGridSize (Sim.cu:4158): 256 isolated, 512 periodic. */
+int sd_max_grid_size(int boundary);
+/* Sim::estimateBytes (Sim.cu:3935-3998), for this implementation's buffers. */
+size_t sd_estimate_bytes(int particle_count, int grid_size, int boundary);
+
+/* ---- lifetime (Sim::Sim / ~Sim, Sim.cu:3900-3901) --------------------------- */
+int sd_create(sd_sim** out, int device);
+int sd_destroy(sd_sim* sim);
+/* Stream for all work of this handle (default: a stream the handle creates). */
+int sd_set_stream(sd_sim* sim, void* cuda_stream);
+
+/* ---- configuration (Sim::init / reconfigure / reset, Sim.cu:4068-4238) ------ */
+int sd_init(sd_sim* sim, const sd_config* cfg);
+int sd_reconfigure(sd_sim* sim, const sd_config* cfg);
+/* Sim::reset: zero time and step count, empty all slots (the reference's
+ * Filament preset is not part of this path; scenes are loaded with
+ * sd_set_particles / sd_load_state). */
+int sd_reset(sd_sim* sim);
+int sd_get_config(const sd_sim* sim, sd_config* out);
+
+/* ---- particle buffers (Sim::loadState's upload path, Sim.cu:5096-5101; ------
+ * particlePosDevicePtr / particleVelDevicePtr, Sim.h:1128-1129).
+ * pos, vel: float4[n] (x,y,z,w). n <= particle_count; slots >= n become empty.
+ * `where` is SD_HOST or SD_DEVICE. */
+int sd_set_particles(sd_sim* sim, const float* pos, const float* vel, int n, int where);
+int sd_get_particles(sd_sim* sim, float* pos, float* vel, int n, int where);
+/* Device pointers (float4 arrays as float*), valid until the next step or
+ * reconfigure. Pending momentum corrections are applied first. */
+const float* sd_particle_pos_device_ptr(sd_sim* sim);
+const float* sd_particle_vel_device_ptr(sd_sim* sim);
+/* Density of the step-start positions of the last step (Sim::densityDevicePtr,
+ * Sim.h:1082), G^3 floats z-major. */
+const float* sd_density_device_ptr(sd_sim* sim);
+int sd_get_density(sd_sim* sim, float* out, int where);
+/* Potential of the last force solve, G^3 floats z-major, configured units. */
+int sd_get_potential(sd_sim* sim, float* out, int where);
+/* Accelerations the current positions would receive (solves the field for the
+ * current positions without moving particles): float4[n], w = 0. */
+int sd_get_accel(sd_sim* sim, float* out, int n, int where);
+
+/* ---- stepping (Sim::step, Sim.cu:4240-4525) -------------------------------- */
+/* Advance by exactly dt (no CFL clamp). */
+int sd_step(sd_sim* sim, float dt);
+/* The reference's step(): dt = 0.0016*dtScaleFor(time_scale) clamped to
+ * 0.8*cell/vmax (Sim.cu:4255-4269); blocks for the vmax read like the reference. */
+int sd_step_auto(sd_sim* sim);
+/* nsteps fixed-dt steps; replays a captured CUDA graph after the first call. */
+int sd_steps(sd_sim* sim, float dt, int nsteps);
+/* Leapfrog: apply the closing half kick so velocities are synchronous with
+ * positions (no-op for SD_INT_KD). */
+int sd_synchronize(sd_sim* sim);
+/* Sort and reorder only (sortParticles, Sim.cu:3656-3671). perm (optional,
+ * int32[n]) receives, for each new slot, the old slot it came from. */
+int sd_sort_only(sd_sim* sim, int32_t* perm, int where);
+
+/* ---- state (Sim::saveState / loadState, Sim.cu:4985-5120; STARDUST v2) ------- */
+int sd_save_state(sd_sim* sim, const char* path);
+int sd_load_state(sd_sim* sim, const char* path);
+
+/* ---- queries and measurements ----------------------------------------------- */
+int sd_timings_get(const sd_sim* sim, sd_timings* out);             /* Sim::timings */
+double sd_sim_time(const sd_sim* sim);                              /* Sim::simTime */
+int sd_grid_size(const sd_sim* sim);                                /* Sim::gridSize */
+int sd_particle_count(const sd_sim* sim);                           /* Sim::particleCount */
+int sd_active_count(const sd_sim* sim);                             /* Sim::activeCount */
+int sd_step_count(const sd_sim* sim);
+double sd_measure_total_grid_mass(sd_sim* sim);                     /* Sim.cu:4890-4906 */
+double sd_measure_max_density(sd_sim* sim);                         /* Sim.cu:4908-4924 */
+double sd_measure_kinetic_energy(sd_sim* sim);                      /* Sim.cu:5141-5149 */
+int sd_diagnostics_get(sd_sim* sim, sd_diagnostics* out);
+/* Number of kernel launches the handle issued since creation. */
+long long sd_kernel_launches(const sd_sim* sim);
+
+/* ---- stage entry points on caller buffers (device pointers) ----------------
+ * Each runs one stage of the step on `stream` with caller-owned memory, so the
+ * stages can be checked one at a time. Workspace sizes come from the *_bytes
+ * queries; workspaces must be 256-byte aligned. */
+
+/* kCellKey (Sim.cu:2476-2486) for order SD_ORDER_*: keys_plus1[i] = key + 1
+ * (empty slot -> 0), so an unsigned sort puts empty slots first as CUB does with
+ * the reference's signed -1. */
+int sd_cell_keys(const float* pos, int n, int grid_size, int order, uint32_t* keys_plus1, void* stream);
+/* Bits a stable sort of keys_plus1 must cover for this grid and order. */
+int sd_key_bits(int grid_size, int order);
+/* Stable LSD radix sort of (keys, vals) over the low key_bits bits
+ * (cub::DeviceRadixSort::SortPairs, Sim.cu:3659-3667). vals_in == NULL means
+ * the identity 0..n-1. Results land in keys_out / vals_out; keys_tmp / vals_tmp
+ * are ping-pong buffers of n entries; workspace from sd_sort_workspace_bytes. */
+size_t sd_sort_workspace_bytes(int n);
+int sd_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t* keys_out, int32_t* vals_out,
+                  uint32_t* keys_tmp, int32_t* vals_tmp, int n, int key_bits, void* workspace,
+                  size_t workspace_bytes, void* stream);
+/* kReorder (Sim.cu:2488-2495): dst[i] = src[perm[i]] for float4 pos and vel. */
+int sd_reorder(const float* pos_in, const float* vel_in, const int32_t* perm, float* pos_out, float* vel_out,
+               int n, void* stream);
+/* Deterministic CIC deposit (kScatter Sim.cu:503-521 with int64 fixed-point
+ * sums): rho[G^3] in count units. workspace: sd_deposit_workspace_bytes. */
+size_t sd_deposit_workspace_bytes(int grid_size);
+int sd_deposit(const float* pos, int n, int grid_size, float* rho, void* workspace, size_t workspace_bytes,
+               void* stream);
+/* Periodic Poisson solve rho -> phi with the reference's Green's function
+ * (kPoissonPeriodic Sim.cu:528-557, cuFFT R2C/C2R Sim.cu:3592,3601).
+ * workspace: sd_poisson_workspace_bytes. */
+size_t sd_poisson_workspace_bytes(int grid_size);
+int sd_poisson(const float* rho, int grid_size, float softening_cells, float* phi, void* workspace,
+               size_t workspace_bytes, void* stream);
+/* Gather + kick + drift (kGridAccel Sim.cu:589-611 folded into sampleAcc /
+ * kIntegrate Sim.cu:614-629, 685-906). pot_scale = gravity/N. mean_vel (3
+ * floats, device, may be NULL) is subtracted from each loaded velocity (the
+ * deferred momentum zeroing of the previous step). mom_out (device, 4 doubles,
+ * may be NULL) receives sum vx, vy, vz and the live count of the new
+ * velocities, in a fixed summation order. */
+int sd_gather_kick_drift(const float* phi, int grid_size, float pot_scale, float* pos, float* vel, int n,
+                         float dt_kick, float dt_drift, float c2, const float* mean_vel, double* mom_out,
+                         void* workspace, size_t workspace_bytes, void* stream);
+size_t sd_gather_workspace_bytes(int n);
+/* Per-particle accelerations from phi (the same arithmetic as the kick). */
+int sd_interpolate_accel(const float* phi, int grid_size, float pot_scale, const float* pos, float* acc_out,
+                         int n, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STARDUST_PM_H */

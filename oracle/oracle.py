@@ -1,0 +1,265 @@
+"""Python bindings of the CPU oracle (``pm_oracle.c``) plus FP64 references.
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()`` and
+the ``cpu_baseline`` leg of ``bench.py`` as the checker. The product path never
+imports this module.
+
+The C functions restate the reference's periodic PM step (chdnl0420-svg/stardust,
+``src/sim/Sim.cu``); each wrapper names the reference lines it follows.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle_pm.so")
+
+KEY_ROWMAJOR = 0  # kCellKey, Sim.cu:2476-2486
+KEY_MORTON = 1
+KEY_TILEROW = 2
+
+FIXED_ONE = np.float32(4294967296.0)
+
+_lib = None
+
+
+def build() -> str:
+    """Compile ``liboracle_pm.so`` with the Makefile beside this file."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        P = ctypes.c_void_p
+        i32, f32 = ctypes.c_int, ctypes.c_float
+        L.or_cell_keys.argtypes = [P, i32, i32, i32, P]
+        L.or_stable_sort_perm.argtypes = [P, i32, i32, P]
+        L.or_reorder.argtypes = [P, P, i32, P]
+        L.or_deposit_fixed.argtypes = [P, i32, i32, P]
+        L.or_fixed_to_float.argtypes = [P, ctypes.c_size_t, P]
+        L.or_deposit_float.argtypes = [P, i32, i32, P]
+        L.or_poisson_periodic.argtypes = [P, i32, f32, P]
+        L.or_grid_accel.argtypes = [P, i32, f32, P]
+        L.or_integrate.argtypes = [P, P, P, i32, i32, f32, f32, f32]
+        L.or_momentum_zero.argtypes = [P, P, i32, P]
+        L.or_max_speed.argtypes = [P, P, i32]
+        L.or_max_speed.restype = f32
+        L.or_step.argtypes = [P, P, i32, i32, f32, f32, f32, f32, f32, i32, i32, P, P]
+        L.or_step.restype = i32
+        L.or_num_threads.restype = i32
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _f4(a) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    assert a.ndim == 2 and a.shape[1] == 4
+    return a
+
+
+def num_threads() -> int:
+    return int(lib().or_num_threads())
+
+
+def key_bits(G: int, mode: int) -> int:
+    """Bits of the shifted key (key + 1) that a stable LSD sort must cover."""
+    top = G * G if mode == KEY_TILEROW else G ** 3
+    return int(top).bit_length()
+
+
+def cell_keys(pos, G: int, mode: int = KEY_ROWMAJOR) -> np.ndarray:
+    pos = _f4(pos)
+    out = np.empty(len(pos), np.int32)
+    lib().or_cell_keys(_p(pos), len(pos), G, mode, _p(out))
+    return out
+
+
+def stable_sort_perm(keys: np.ndarray, bits: int = 32) -> np.ndarray:
+    keys = np.ascontiguousarray(keys, np.int32)
+    perm = np.empty(len(keys), np.int32)
+    lib().or_stable_sort_perm(_p(keys), len(keys), bits, _p(perm))
+    return perm
+
+
+def deposit_fixed(pos, G: int) -> np.ndarray:
+    """int64 fixed-point CIC sums (weights rounded to multiples of 2^-32)."""
+    pos = _f4(pos)
+    acc = np.zeros(G ** 3, np.int64)
+    lib().or_deposit_fixed(_p(pos), len(pos), G, _p(acc))
+    return acc.reshape(G, G, G)
+
+
+def fixed_to_float(acc: np.ndarray) -> np.ndarray:
+    acc = np.ascontiguousarray(acc, np.int64)
+    out = np.empty(acc.shape, np.float32)
+    lib().or_fixed_to_float(_p(acc), acc.size, _p(out))
+    return out
+
+
+def density_fixed(pos, G: int) -> np.ndarray:
+    return fixed_to_float(deposit_fixed(pos, G))
+
+
+def density_float(pos, G: int) -> np.ndarray:
+    """The reference's float deposit (kScatter, Sim.cu:503-521), index order."""
+    pos = _f4(pos)
+    rho = np.zeros(G ** 3, np.float32)
+    lib().or_deposit_float(_p(pos), len(pos), G, _p(rho))
+    return rho.reshape(G, G, G)
+
+
+def poisson_periodic(rho: np.ndarray, soft_cells: float) -> np.ndarray:
+    """kPoissonPeriodic + cuFFT round trip (Sim.cu:528-557, 3586-3603), float."""
+    rho = np.ascontiguousarray(rho, np.float32)
+    G = rho.shape[0]
+    phi = np.empty_like(rho)
+    lib().or_poisson_periodic(_p(rho), G, soft_cells, _p(phi))
+    return phi
+
+
+def grid_accel(phi: np.ndarray, pot_scale: float) -> np.ndarray:
+    """kGridAccel, periodic (Sim.cu:589-611). Returns (G,G,G,4) float32."""
+    phi = np.ascontiguousarray(phi, np.float32)
+    G = phi.shape[0]
+    acc = np.empty((G, G, G, 4), np.float32)
+    lib().or_grid_accel(_p(phi), G, pot_scale, _p(acc))
+    return acc
+
+
+def integrate(acc, pos, vel, dt_kick: float, dt_drift: float, c2: float = 1.0e4):
+    """Plain-PM kIntegrate on a periodic box (Sim.cu:685-906). Returns new (pos, vel)."""
+    acc = np.ascontiguousarray(acc, np.float32)
+    pos = _f4(pos).copy()
+    vel = _f4(vel).copy()
+    G = acc.shape[0]
+    lib().or_integrate(_p(acc), _p(pos), _p(vel), len(pos), G, dt_kick, dt_drift, c2)
+    return pos, vel
+
+
+def momentum_zero(pos, vel):
+    """kMomentumAccum + kSubtractMeanVelDev (Sim.cu:2252-2291)."""
+    pos = _f4(pos)
+    vel = _f4(vel).copy()
+    out = np.zeros(4, np.float64)
+    lib().or_momentum_zero(_p(pos), _p(vel), len(pos), _p(out))
+    return vel, out
+
+
+def max_speed(pos, vel) -> float:
+    pos, vel = _f4(pos), _f4(vel)
+    return float(lib().or_max_speed(_p(pos), _p(vel), len(pos)))
+
+
+def step(pos, vel, G: int, gravity: float, soft_cells: float, dt_kick: float, dt_drift: float,
+         c2: float = 1.0e4, key_mode: int = KEY_ROWMAJOR, deterministic: bool = True):
+    """One reference-order step (Sim::step, Sim.cu:4240-4525, extras off).
+
+    Returns (pos, vel, rho, momentum sums)."""
+    pos = _f4(pos).copy()
+    vel = _f4(vel).copy()
+    rho = np.empty(G ** 3, np.float32)
+    mom = np.zeros(4, np.float64)
+    rc = lib().or_step(_p(pos), _p(vel), len(pos), G, gravity, soft_cells, dt_kick, dt_drift, c2,
+                       key_mode, 1 if deterministic else 0, _p(rho), _p(mom))
+    if rc != 0:
+        raise MemoryError("oracle step: allocation failed")
+    return pos, vel, rho.reshape(G, G, G), mom
+
+
+# ---------------------------------------------------------------------------
+# FP64 references (numpy)
+# ---------------------------------------------------------------------------
+
+def green_periodic_f64(G: int, soft_cells: float) -> np.ndarray:
+    """The reference's periodic Green's function on the rfft half spectrum, FP64:
+    -1/(4 pi^2 k^2) * exp(-k^2 s^2 / 2), s = 2 pi soft / G, k = 0 -> 0
+    (kPoissonPeriodic, Sim.cu:528-557; FFT normalisation 1/G^3 included)."""
+    k = np.fft.fftfreq(G, d=1.0 / G)
+    kx = np.arange(G // 2 + 1, dtype=np.float64)
+    k2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + kx[None, None, :] ** 2
+    with np.errstate(divide="ignore"):
+        m = -1.0 / (4.0 * np.pi ** 2 * k2) / float(G) ** 3
+    m[0, 0, 0] = 0.0
+    if soft_cells > 0:
+        s = 2.0 * np.pi * soft_cells / G
+        m *= np.exp(-0.5 * k2 * s * s)
+    return m
+
+
+def poisson_periodic_f64(rho: np.ndarray, soft_cells: float) -> np.ndarray:
+    """FP64 periodic solve with the reference's conventions (unnormalised FFT
+    pair, Green's function scaled by 1/G^3)."""
+    G = rho.shape[0]
+    spec = np.fft.rfftn(rho.astype(np.float64))
+    spec *= green_periodic_f64(G, soft_cells)
+    return np.fft.irfftn(spec, s=rho.shape, axes=(0, 1, 2)) * float(G) ** 3
+
+
+def central_gradient_f64(phi: np.ndarray, pot_scale: float) -> np.ndarray:
+    """kGridAccel's central difference in FP64: (G,G,G,3) with axes (x,y,z)."""
+    G = phi.shape[0]
+    h = 0.5 * G * pot_scale
+    ax = -(np.roll(phi, -1, axis=2) - np.roll(phi, 1, axis=2)) * h
+    ay = -(np.roll(phi, -1, axis=1) - np.roll(phi, 1, axis=1)) * h
+    az = -(np.roll(phi, -1, axis=0) - np.roll(phi, 1, axis=0)) * h
+    return np.stack([ax, ay, az], axis=-1)
+
+
+def cic_weights_f64(pos: np.ndarray, G: int):
+    """CIC base cells and the 8 corner weights in FP64 (Sim.cu:509-518)."""
+    g = pos[:, :3].astype(np.float64) * G - 0.5
+    i = np.floor(g).astype(np.int64)
+    f = g - i
+    out_idx, out_w = [], []
+    for k in range(8):
+        o = np.array([k & 1, (k >> 1) & 1, (k >> 2) & 1])
+        c = (i + o) % G
+        w = np.prod(np.where(o[None, :] == 1, f, 1.0 - f), axis=1)
+        out_idx.append(c)
+        out_w.append(w)
+    return out_idx, out_w
+
+
+def density_f64(pos: np.ndarray, G: int) -> np.ndarray:
+    live = pos[:, 0] >= 0
+    p = pos[live]
+    rho = np.zeros((G, G, G), np.float64)
+    idx, w = cic_weights_f64(p, G)
+    for c, wk in zip(idx, w):
+        np.add.at(rho, (c[:, 2], c[:, 1], c[:, 0]), wk)
+    return rho
+
+
+def pm_accel_f64(pos: np.ndarray, G: int, pot_scale: float, soft_cells: float) -> np.ndarray:
+    """Per-particle PM acceleration in FP64 with the reference's operators: CIC
+    deposit, periodic Green's function, central difference, CIC gather."""
+    rho = density_f64(pos, G)
+    phi = poisson_periodic_f64(rho, soft_cells)
+    grad = central_gradient_f64(phi, pot_scale)
+    idx, w = cic_weights_f64(pos, G)
+    a = np.zeros((len(pos), 3), np.float64)
+    for c, wk in zip(idx, w):
+        a += grad[c[:, 2], c[:, 1], c[:, 0]] * wk[:, None]
+    return a
+
+
+def force_error(a: np.ndarray, a_ref: np.ndarray) -> dict:
+    """eps = RMS(|a - a_ref|) / RMS(|a_ref|), the reference's scoring metric
+    (.drive/nbody-simulator/method-search/scoring.md:38), plus the max."""
+    d = np.linalg.norm(np.asarray(a, np.float64) - a_ref, axis=1)
+    r = np.sqrt(np.mean(np.sum(a_ref * a_ref, axis=1)))
+    return {"rms_rel": float(np.sqrt(np.mean(d * d)) / r), "max_rel": float(d.max() / r)}

@@ -1,0 +1,151 @@
+// ref_harness.cu -- C entry points over the reference's public Sim API.
+//
+// TEST INFRASTRUCTURE ONLY. Linked with the unmodified reference core
+// (src/sim/Sim.cu) into oracle/_ref/libsimref.so; used on a GPU box to produce
+// golden fixtures and to time the reference. It touches the reference only
+// through class Sim (src/sim/Sim.h:854-1135): inputs go in through a STARDUST v2
+// state file and Sim::loadState (Sim.cu:5041-5120), the only public way to hand
+// the reference an arbitrary particle set; outputs come back through
+// particlePosDevicePtr / particleVelDevicePtr / densityDevicePtr / timings.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "Sim.h"
+
+// src/app/Forensics.h declares these; the reference's Forensics.cpp is
+// MSVC-CRT-only, so the harness provides silent versions.
+namespace fx {
+void begin(const char*) {}
+void line(const char*, ...) {}
+void mark(const char*, ...) {}
+void endOk() {}
+bool lastSessionCrashed() { return false; }
+const char* logDir() { return "."; }
+}  // namespace fx
+
+namespace {
+// The STARDUST v2 header as the reference reads it (Sim.cu:4985-4997).
+struct Header {
+    char magic[8];
+    int32_t version, count, gridSize, preset, boundary;
+    float gravity, simTime;
+    float bhX, bhY, bhRs, bhMass;
+    int32_t bhActive;
+    int32_t reserved[5];
+};
+static_assert(sizeof(Header) == 76, "header layout");
+
+SimConfig plain_pm(int n, int G, float gravity, float soft, float time_scale, int sort_interval) {
+    SimConfig c;  // reference defaults, then every non-gravity feature off
+    c.particleCount = n;
+    c.gridSize = G;
+    c.boundary = Boundary::Periodic;
+    c.preset = Preset::Empty;
+    c.gravity = gravity;
+    c.softeningCells = soft;
+    c.timeScale = time_scale;
+    c.sortInterval = sort_interval;
+    c.pressureEnabled = false;
+    c.coolingEnabled = false;
+    c.starFormationEnabled = false;
+    c.contactEnabled = false;
+    c.blackHoleEnabled = false;
+    c.strongForceEnabled = false;
+    c.emForceEnabled = false;
+    c.weakForceEnabled = false;
+    c.collapseEnabled = false;
+    c.darkEnergy = 0.f;
+    c.softBoundR = 0.f;
+    c.spin = 0.f;
+    c.hubble = 0.f;
+    c.velDispersion = 0.f;
+    c.darkMatterFraction = 0.f;
+    return c;
+}
+}  // namespace
+
+extern "C" {
+
+void* ref_create() { return new Sim(); }
+
+void ref_destroy(void* h) { delete static_cast<Sim*>(h); }
+
+int ref_failed() { return Sim::failed() ? 1 : 0; }
+
+const char* ref_fail_message() {
+    static std::string m;
+    m = Sim::failMessage();
+    return m.c_str();
+}
+
+// Configure plain PM and load (pos, vel) through a state file at tmp_path.
+int ref_load(void* h, const float* pos, const float* vel, int n, int G, float gravity, float soft, float time_scale,
+             int sort_interval, const char* tmp_path) {
+    Sim* s = static_cast<Sim*>(h);
+    s->init(plain_pm(n, G, gravity, soft, time_scale, sort_interval));
+    if (Sim::failed()) return -2;
+    Header hd;
+    std::memset(&hd, 0, sizeof(hd));
+    std::memcpy(hd.magic, "STARDUST", 8);
+    hd.version = 2;
+    hd.count = n;
+    hd.gridSize = G;
+    hd.preset = (int)Preset::Empty;
+    hd.boundary = (int)Boundary::Periodic;
+    hd.gravity = gravity;
+    FILE* f = std::fopen(tmp_path, "wb");
+    if (!f) return -5;
+    bool ok = std::fwrite(&hd, sizeof(hd), 1, f) == 1 && std::fwrite(pos, 16, (size_t)n, f) == (size_t)n &&
+              std::fwrite(vel, 16, (size_t)n, f) == (size_t)n;
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return -5;
+    if (!s->loadState(tmp_path)) return -6;
+    cudaDeviceSynchronize();
+    return Sim::failed() ? -2 : 0;
+}
+
+int ref_step(void* h) {
+    static_cast<Sim*>(h)->step();
+    return Sim::failed() ? -2 : 0;
+}
+
+int ref_steps(void* h, int k) {
+    Sim* s = static_cast<Sim*>(h);
+    for (int i = 0; i < k; ++i) s->step();
+    cudaDeviceSynchronize();
+    return Sim::failed() ? -2 : 0;
+}
+
+int ref_get(void* h, float* pos, float* vel, int n) {
+    Sim* s = static_cast<Sim*>(h);
+    if (cudaMemcpy(pos, s->particlePosDevicePtr(), 16 * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess) return -2;
+    if (cudaMemcpy(vel, s->particleVelDevicePtr(), 16 * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess) return -2;
+    return 0;
+}
+
+int ref_density(void* h, float* out, int G) {
+    Sim* s = static_cast<Sim*>(h);
+    const size_t cells = (size_t)G * G * G;
+    if (cudaMemcpy(out, s->densityDevicePtr(), 4 * cells, cudaMemcpyDeviceToHost) != cudaSuccess) return -2;
+    return 0;
+}
+
+// scatterMs, poissonMs, gatherMs, totalMs, dtUsed, maxSpeed (Sim.h:844-852)
+int ref_timings(void* h, float* out6) {
+    const SimTimings t = static_cast<Sim*>(h)->timings();
+    out6[0] = t.scatterMs;
+    out6[1] = t.poissonMs;
+    out6[2] = t.gatherMs;
+    out6[3] = t.totalMs;
+    out6[4] = t.dtUsed;
+    out6[5] = t.maxSpeed;
+    return 0;
+}
+
+double ref_sim_time(void* h) { return static_cast<Sim*>(h)->simTime(); }
+
+}  // extern "C"

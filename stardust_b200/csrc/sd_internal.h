@@ -1,0 +1,76 @@
+// sd_internal.h -- host-side helpers shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/stardust_pm.h"
+
+namespace sd {
+
+// Sticky process-wide error record (the reference's g_failed / g_failMsg,
+// Sim.cu:52-75): the first failure's message is kept until sd_clear_error.
+int fail(int code, const char* fmt, ...);
+int check_cuda(cudaError_t e, const char* what, const char* file, int line);
+
+// Launch accounting: every kernel launch of the library goes through
+// count_launch so sd_kernel_launches can report how many ran.
+void count_launch(long long n = 1);
+long long launches();
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Stage launchers (defined in the .cu files). All return SD_OK or SD_E_*.
+int launch_cell_keys(const float4* pos, int n, int G, int order, uint32_t* keys, cudaStream_t s);
+size_t sort_workspace_bytes(int n);
+int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t* keys_out, int32_t* vals_out,
+                      uint32_t* keys_tmp, int32_t* vals_tmp, int n, int key_bits, void* ws, size_t ws_bytes,
+                      cudaStream_t s);
+int launch_reorder(const float4* pos_in, const float4* vel_in, const int32_t* perm, float4* pos_out,
+                   float4* vel_out, int n, cudaStream_t s);
+
+size_t deposit_workspace_bytes(int G);
+int launch_deposit_fixed(const float4* pos, int n, int G, long long* acc, cudaStream_t s);
+int launch_clear_u64(long long* a, size_t n, cudaStream_t s);
+int launch_fixed_to_float(const long long* acc, int G, float* rho, int clear, cudaStream_t s);
+
+// Poisson plan: twiddles and Green's tables for one grid size (device memory).
+struct PoissonPlan {
+    int G = 0;
+    float soft = -1.f;
+    float2* tw = nullptr;    // W_G^m = exp(-2 pi i m / G), m < G (FP64-built, rounded)
+    float* gexp = nullptr;   // exp(-(2 pi soft / G)^2 k^2 / 2), k = 0..G/2 (FP64-built)
+    float scale = 0.f;       // 1 / (4 pi^2 G^3)
+};
+int poisson_plan_build(PoissonPlan& p, int G, float soft);
+void poisson_plan_free(PoissonPlan& p);
+size_t poisson_spectrum_elems(int G);  // complex elements of one spectrum buffer
+// rho_fixed != nullptr: the first pass reads the int64 fixed-point grid (and
+// zeroes it); otherwise it reads rho_float.
+int launch_poisson(const PoissonPlan& p, const long long* rho_fixed, const float* rho_float, int clear_fixed,
+                   float* rho_keep, float2* specA, float2* specB, float* phi, cudaStream_t s);
+
+size_t gather_partials(int n);
+int launch_gather_kick_drift(const float* phi, int G, float pot_scale, float4* pos, float4* vel, int n,
+                             float dt_kick, float dt_drift, float c2, const float* mean_vel,
+                             double* partials, double* mom_out, float* mean_out, cudaStream_t s);
+int launch_interpolate_accel(const float* phi, int G, float pot_scale, const float4* pos, float4* acc, int n,
+                             cudaStream_t s);
+int launch_apply_mean(float4* vel, const float4* pos, int n, const float* mean_vel, cudaStream_t s);
+int launch_max_speed(const float4* pos, const float4* vel, int n, const float* mean_vel, float* out,
+                     cudaStream_t s);
+int launch_energy(const float* phi, int G, const float4* pos, const float4* vel, int n, const float* mean_vel,
+                  double* partials, double* out8, cudaStream_t s);
+int launch_reduce_grid(const float* rho, size_t cells, int op, double* partials, double* out, cudaStream_t s);
+int launch_hide_range(float4* pos, float4* vel, int from, int to, cudaStream_t s);
+
+}  // namespace sd
+
+#define SD_CUDA(x) ::sd::check_cuda((x), #x, __FILE__, __LINE__)
+#define SD_LAUNCHED(s)                                                        \
+    do {                                                                      \
+        ::sd::count_launch();                                                 \
+        cudaError_t e_ = cudaGetLastError();                                  \
+        if (e_ != cudaSuccess) return ::sd::check_cuda(e_, "launch", __FILE__, __LINE__); \
+    } while (0)

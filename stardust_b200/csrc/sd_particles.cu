@@ -1,0 +1,442 @@
+// sd_particles.cu -- per-particle kernels: CIC deposit, gather + kick + drift,
+// momentum sums, speed, energy and small grid reductions.
+//
+// Reference counterparts: kScatter (Sim.cu:503-521), kGridAccel (Sim.cu:589-611),
+// sampleAcc and kIntegrate (Sim.cu:614-629, 685-906), kMaxSpeed (Sim.cu:2923-2930),
+// kMomentumAccum / kSubtractMeanVelDev (Sim.cu:2252-2291).
+//
+// Design points:
+//  * The deposit rounds each CIC weight once to a multiple of 2^-32 and adds it to
+//    an int64 grid. Integer addition is associative, so the density is the same
+//    whatever order the atomics land in: bit-exact run to run, and bit-exact
+//    against the oracle's fixed-point deposit.
+//  * No force grid is stored. The gather reads the potential and forms the
+//    reference's central difference for each of the 8 CIC corners with the
+//    reference's arithmetic; given the same phi the kick is bit-identical to the
+//    reference's accG route (kGridAccel then sampleAcc), and it saves writing and
+//    re-reading a float4 grid (32 B per cell).
+//  * Momentum zeroing is deferred: the kernel that writes the new velocities also
+//    sums them (FP64 per block, then a fixed-order final sum), and the mean is
+//    subtracted as the next consumer loads each velocity. The float arithmetic
+//    (v - (float)(sum/count)) is the reference's.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "sd_common.cuh"
+#include "sd_internal.h"
+
+namespace sd {
+
+namespace {
+
+constexpr int kGatherThreads = 256;
+
+__global__ void __launch_bounds__(256) k_deposit_fixed(const float4* __restrict__ pos, int n, int G,
+                                                       unsigned long long* __restrict__ acc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = pos[i];
+    if (p.x < 0.f) return;
+    int ix, iy, iz;
+    float fx, fy, fz;
+    cic_axis(p.x, G, ix, fx);
+    cic_axis(p.y, G, iy, fy);
+    cic_axis(p.z, G, iz, fz);
+    const int m = G - 1;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int cx = (ix + (k & 1)) & m;
+        const int cy = (iy + ((k >> 1) & 1)) & m;
+        const int cz = (iz + ((k >> 2) & 1)) & m;
+        const long long q = fixed_weight(cic_weight(k, fx, fy, fz));
+        atomicAdd(acc + ((size_t)cz * G + cy) * G + cx, (unsigned long long)q);
+    }
+}
+
+__global__ void k_fixed_to_float(long long* __restrict__ acc, size_t cells, float* __restrict__ rho, int clear) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cells) return;
+    rho[i] = fixed_to_float(acc[i]);
+    if (clear) acc[i] = 0;
+}
+
+__global__ void k_clear_u64(unsigned long long* __restrict__ a, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = 0ull;
+}
+
+// CIC-interpolated central-difference gradient of phi at p (the reference's
+// kGridAccel values sampled with sampleAcc's weights and FMA order).
+__device__ __forceinline__ float3 gather_accel(const float* __restrict__ phi, int G, float h, float4 p) {
+    int ix, iy, iz;
+    float fx, fy, fz;
+    cic_axis(p.x, G, ix, fx);
+    cic_axis(p.y, G, iy, fy);
+    cic_axis(p.z, G, iz, fz);
+    const int m = G - 1;
+    float3 a = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float w = cic_weight(k, fx, fy, fz);
+        const int cx = (ix + (k & 1)) & m;
+        const int cy = (iy + ((k >> 1) & 1)) & m;
+        const int cz = (iz + ((k >> 2) & 1)) & m;
+        const size_t row = ((size_t)cz * G + cy) * G;
+        const float gx = __fmul_rn(-__fsub_rn(__ldg(phi + row + ((cx + 1) & m)), __ldg(phi + row + ((cx - 1) & m))), h);
+        const float gy = __fmul_rn(-__fsub_rn(__ldg(phi + ((size_t)cz * G + ((cy + 1) & m)) * G + cx),
+                                              __ldg(phi + ((size_t)cz * G + ((cy - 1) & m)) * G + cx)),
+                                   h);
+        const float gz = __fmul_rn(-__fsub_rn(__ldg(phi + ((size_t)((cz + 1) & m) * G + cy) * G + cx),
+                                              __ldg(phi + ((size_t)((cz - 1) & m) * G + cy) * G + cx)),
+                                   h);
+        a.x = __fmaf_rn(gx, w, a.x);
+        a.y = __fmaf_rn(gy, w, a.y);
+        a.z = __fmaf_rn(gz, w, a.z);
+    }
+    return a;
+}
+
+// FP64 block sum of 4 values into partials[blockIdx.x*4 + j], fixed tree order.
+__device__ __forceinline__ void block_sum4(double v0, double v1, double v2, double v3, double* partials) {
+    __shared__ double red[4][kGatherThreads / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v0 += __shfl_down_sync(0xffffffffu, v0, o);
+        v1 += __shfl_down_sync(0xffffffffu, v1, o);
+        v2 += __shfl_down_sync(0xffffffffu, v2, o);
+        v3 += __shfl_down_sync(0xffffffffu, v3, o);
+    }
+    if (lane == 0) { red[0][w] = v0; red[1][w] = v1; red[2][w] = v2; red[3][w] = v3; }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double s = 0.0;
+        for (int j = 0; j < kGatherThreads / 32; ++j) s += red[threadIdx.x][j];
+        partials[(size_t)blockIdx.x * 4 + threadIdx.x] = s;
+    }
+}
+
+__global__ void __launch_bounds__(kGatherThreads) k_gather_kick_drift(const float* __restrict__ phi, int G, float h,
+                                                                      float4* __restrict__ pos, float4* __restrict__ vel,
+                                                                      int n, float dt_kick, float dt_drift, float c2,
+                                                                      const float* __restrict__ mean_vel,
+                                                                      double* __restrict__ partials) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double sx = 0.0, sy = 0.0, sz = 0.0, cnt = 0.0;
+    if (i < n) {
+        float4 p = pos[i];
+        if (p.x >= 0.f) {
+            float4 v = vel[i];
+            if (mean_vel) {
+                v.x = __fsub_rn(v.x, mean_vel[0]);
+                v.y = __fsub_rn(v.y, mean_vel[1]);
+                v.z = __fsub_rn(v.z, mean_vel[2]);
+            }
+            const float3 a = gather_accel(phi, G, h, p);
+            v.x = __fmaf_rn(a.x, dt_kick, v.x);
+            v.y = __fmaf_rn(a.y, dt_kick, v.y);
+            v.z = __fmaf_rn(a.z, dt_kick, v.z);
+            {  // light-speed clamp (Sim.cu:834-840)
+                const float sp2 = __fmaf_rn(v.z, v.z, __fmaf_rn(v.y, v.y, __fmul_rn(v.x, v.x)));
+                if (sp2 > c2) {
+                    const float k = sqrtf(__fdiv_rn(c2, sp2));
+                    v.x = __fmul_rn(v.x, k);
+                    v.y = __fmul_rn(v.y, k);
+                    v.z = __fmul_rn(v.z, k);
+                }
+            }
+            p.x = __fmaf_rn(v.x, dt_drift, p.x);
+            p.y = __fmaf_rn(v.y, dt_drift, p.y);
+            p.z = __fmaf_rn(v.z, dt_drift, p.z);
+            if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z) || !isfinite(v.x) || !isfinite(v.y) ||
+                !isfinite(v.z)) {
+                pos[i] = make_float4(-1.f, -1.f, -1.f, 0.f);
+                vel[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+                p.x = __fsub_rn(p.x, floorf(p.x));
+                p.y = __fsub_rn(p.y, floorf(p.y));
+                p.z = __fsub_rn(p.z, floorf(p.z));
+                pos[i] = p;
+                vel[i] = v;
+                sx = v.x; sy = v.y; sz = v.z; cnt = 1.0;
+            }
+        }
+    }
+    if (partials) block_sum4(sx, sy, sz, cnt, partials);
+}
+
+// Fixed-order sum of the per-block partials; mean = (float)(sum / count).
+__global__ void __launch_bounds__(256) k_finalize_mean(const double* __restrict__ partials, int blocks,
+                                                       double* __restrict__ mom_out, float* __restrict__ mean_out) {
+    __shared__ double red[4][256];
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < blocks; b += 256)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) s[j] += partials[(size_t)b * 4 + j];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) red[j][threadIdx.x] = s[j];
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) red[j][threadIdx.x] += red[j][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        if (mom_out)
+            for (int j = 0; j < 4; ++j) mom_out[j] = red[j][0];
+        if (mean_out) {
+            const double c = red[3][0];
+            for (int j = 0; j < 3; ++j) mean_out[j] = (c >= 1.0) ? (float)(red[j][0] / c) : 0.f;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_interpolate_accel(const float* __restrict__ phi, int G, float h,
+                                                           const float4* __restrict__ pos, float4* __restrict__ acc,
+                                                           int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = pos[i];
+    if (p.x < 0.f) {
+        acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const float3 a = gather_accel(phi, G, h, p);
+    acc[i] = make_float4(a.x, a.y, a.z, 0.f);
+}
+
+__global__ void k_apply_mean(float4* __restrict__ vel, const float4* __restrict__ pos, int n,
+                             const float* __restrict__ mean_vel) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || pos[i].x < 0.f) return;
+    float4 v = vel[i];
+    v.x = __fsub_rn(v.x, mean_vel[0]);
+    v.y = __fsub_rn(v.y, mean_vel[1]);
+    v.z = __fsub_rn(v.z, mean_vel[2]);
+    vel[i] = v;
+}
+
+__global__ void k_max_speed(const float4* __restrict__ pos, const float4* __restrict__ vel, int n,
+                            const float* __restrict__ mean_vel, float* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float s = 0.f;
+    if (i < n && pos[i].x >= 0.f) {
+        float4 v = vel[i];
+        if (mean_vel) {
+            v.x = __fsub_rn(v.x, mean_vel[0]);
+            v.y = __fsub_rn(v.y, mean_vel[1]);
+            v.z = __fsub_rn(v.z, mean_vel[2]);
+        }
+        s = sqrtf(__fmaf_rn(v.z, v.z, __fmaf_rn(v.y, v.y, __fmul_rn(v.x, v.x))));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s = fmaxf(s, __shfl_down_sync(0xffffffffu, s, o));
+    if ((threadIdx.x & 31) == 0 && s > 0.f) atomicMax(reinterpret_cast<int*>(out), __float_as_int(s));
+}
+
+// Kinetic and potential energy and momentum, FP64, two-level fixed order.
+// partials: 8 doubles per block: KE, PE, px, py, pz, count, -, -.
+__global__ void __launch_bounds__(kGatherThreads) k_energy(const float* __restrict__ phi, int G,
+                                                           const float4* __restrict__ pos,
+                                                           const float4* __restrict__ vel, int n,
+                                                           const float* __restrict__ mean_vel,
+                                                           double* __restrict__ partials) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ke = 0.0, pe = 0.0, px = 0.0, py = 0.0, pz = 0.0, c = 0.0;
+    if (i < n) {
+        const float4 p = pos[i];
+        if (p.x >= 0.f) {
+            float4 v = vel[i];
+            if (mean_vel) {
+                v.x = __fsub_rn(v.x, mean_vel[0]);
+                v.y = __fsub_rn(v.y, mean_vel[1]);
+                v.z = __fsub_rn(v.z, mean_vel[2]);
+            }
+            ke = 0.5 * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+            px = v.x; py = v.y; pz = v.z; c = 1.0;
+            if (phi) {
+                int ix, iy, iz;
+                float fx, fy, fz;
+                cic_axis(p.x, G, ix, fx);
+                cic_axis(p.y, G, iy, fy);
+                cic_axis(p.z, G, iz, fz);
+                const int m = G - 1;
+                double f = 0.0;
+                for (int k = 0; k < 8; ++k) {
+                    const int cx = (ix + (k & 1)) & m, cy = (iy + ((k >> 1) & 1)) & m, cz = (iz + ((k >> 2) & 1)) & m;
+                    f += (double)cic_weight(k, fx, fy, fz) * (double)phi[((size_t)cz * G + cy) * G + cx];
+                }
+                pe = 0.5 * f;
+            }
+        }
+    }
+    __shared__ double red[6][kGatherThreads / 32];
+    double vals[6] = {ke, pe, px, py, pz, c};
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 6; ++j)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vals[j] += __shfl_down_sync(0xffffffffu, vals[j], o);
+    if (lane == 0)
+#pragma unroll
+        for (int j = 0; j < 6; ++j) red[j][w] = vals[j];
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        double s = 0.0;
+        if (threadIdx.x < 6)
+            for (int k = 0; k < kGatherThreads / 32; ++k) s += red[threadIdx.x][k];
+        partials[(size_t)blockIdx.x * 8 + threadIdx.x] = s;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_finalize8(const double* __restrict__ partials, int blocks,
+                                                   double* __restrict__ out) {
+    __shared__ double red[8][256];
+    double s[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s[j] = 0.0;
+    for (int b = threadIdx.x; b < blocks; b += 256)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) s[j] += partials[(size_t)b * 8 + j];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) red[j][threadIdx.x] = s[j];
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) red[j][threadIdx.x] += red[j][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x < 8) out[threadIdx.x] = red[threadIdx.x][0];
+}
+
+// op 0: sum, 1: max. Grid-stride, 8 partial doubles per block slot (only [0] used).
+__global__ void __launch_bounds__(256) k_reduce_grid(const float* __restrict__ a, size_t n, int op,
+                                                     double* __restrict__ partials) {
+    double acc = (op == 1) ? -INFINITY : 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const double v = a[i];
+        acc = (op == 1) ? fmax(acc, v) : acc + v;
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] = (op == 1) ? fmax(red[threadIdx.x], red[threadIdx.x + o])
+                                                          : red[threadIdx.x] + red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partials[blockIdx.x] = red[0];
+}
+
+__global__ void k_reduce_final(const double* __restrict__ partials, int blocks, int op, double* __restrict__ out) {
+    if (threadIdx.x != 0) return;
+    double acc = (op == 1) ? -INFINITY : 0.0;
+    for (int b = 0; b < blocks; ++b) acc = (op == 1) ? fmax(acc, partials[b]) : acc + partials[b];
+    *out = acc;
+}
+
+__global__ void k_hide_range(float4* __restrict__ pos, float4* __restrict__ vel, int from, int to) {
+    const int i = from + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= to) return;
+    pos[i] = make_float4(-1.f, -1.f, -1.f, 0.f);
+    vel[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+}  // namespace
+
+size_t deposit_workspace_bytes(int G) { return align_up(sizeof(long long) * (size_t)G * G * G, 256); }
+
+int launch_deposit_fixed(const float4* pos, int n, int G, long long* acc, cudaStream_t s) {
+    if (n <= 0) return SD_OK;
+    k_deposit_fixed<<<(n + 255) / 256, 256, 0, s>>>(pos, n, G, reinterpret_cast<unsigned long long*>(acc));
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
+
+int launch_clear_u64(long long* a, size_t n, cudaStream_t s) {
+    k_clear_u64<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(reinterpret_cast<unsigned long long*>(a), n);
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
+
+int launch_fixed_to_float(const long long* acc, int G, float* rho, int clear, cudaStream_t s) {
+    const size_t cells = (size_t)G * G * G;
+    k_fixed_to_float<<<(unsigned)((cells + 255) / 256), 256, 0, s>>>(const_cast<long long*>(acc), cells, rho, clear);
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
+
+size_t gather_partials(int n) { return (size_t)((n + kGatherThreads - 1) / kGatherThreads); }
+
+int launch_gather_kick_drift(const float* phi, int G, float pot_scale, float4* pos, float4* vel, int n,
+                             float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
+                             double* mom_out, float* mean_out, cudaStream_t s) {
+    if (n <= 0) return SD_OK;
+    const float h = (0.5f * (float)G) * pot_scale;  // Sim.cu:604
+    const int blocks = (int)gather_partials(n);
+    k_gather_kick_drift<<<blocks, kGatherThreads, 0, s>>>(phi, G, h, pos, vel, n, dt_kick, dt_drift, c2, mean_vel,
+                                                          partials);
+    SD_LAUNCHED(s);
+    if (partials && (mom_out || mean_out)) {
+        k_finalize_mean<<<1, 256, 0, s>>>(partials, blocks, mom_out, mean_out);
+        SD_LAUNCHED(s);
+    }
+    return SD_OK;
+}
+
+int launch_interpolate_accel(const float* phi, int G, float pot_scale, const float4* pos, float4* acc, int n,
+                             cudaStream_t s) {
+    if (n <= 0) return SD_OK;
+    const float h = (0.5f * (float)G) * pot_scale;
+    k_interpolate_accel<<<(n + 255) / 256, 256, 0, s>>>(phi, G, h, pos, acc, n);
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
+
+int launch_apply_mean(float4* vel, const float4* pos, int n, const float* mean_vel, cudaStream_t s) {
+    if (n <= 0) return SD_OK;
+    k_apply_mean<<<(n + 255) / 256, 256, 0, s>>>(vel, pos, n, mean_vel);
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
+
+int launch_max_speed(const float4* pos, const float4* vel, int n, const float* mean_vel, float* out,
+                     cudaStream_t s) {
+    if (SD_CUDA(cudaMemsetAsync(out, 0, sizeof(float), s)) != SD_OK) return SD_E_CUDA;
+    if (n <= 0) return SD_OK;
+    k_max_speed<<<(n + 255) / 256, 256, 0, s>>>(pos, vel, n, mean_vel, out);
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
+
+int launch_energy(const float* phi, int G, const float4* pos, const float4* vel, int n, const float* mean_vel,
+                  double* partials, double* out8, cudaStream_t s) {
+    if (n <= 0) return SD_OK;
+    const int blocks = (n + kGatherThreads - 1) / kGatherThreads;
+    k_energy<<<blocks, kGatherThreads, 0, s>>>(phi, G, pos, vel, n, mean_vel, partials);
+    SD_LAUNCHED(s);
+    k_finalize8<<<1, 256, 0, s>>>(partials, blocks, out8);
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
+
+int launch_reduce_grid(const float* a, size_t cells, int op, double* partials, double* out, cudaStream_t s) {
+    const int blocks = 296;
+    k_reduce_grid<<<blocks, 256, 0, s>>>(a, cells, op, partials);
+    SD_LAUNCHED(s);
+    k_reduce_final<<<1, 32, 0, s>>>(partials, blocks, op, out);
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
+
+int launch_hide_range(float4* pos, float4* vel, int from, int to, cudaStream_t s) {
+    if (to <= from) return SD_OK;
+    k_hide_range<<<(to - from + 255) / 256, 256, 0, s>>>(pos, vel, from, to);
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
+
+}  // namespace sd

@@ -1,0 +1,1005 @@
+// sd_sim.cu -- the simulation handle and the C ABI (include/stardust_pm.h).
+//
+// Reference counterpart: class Sim and Sim::Impl (src/sim/Sim.h:854-1135,
+// src/sim/Sim.cu:2937-3168, 3895-4525, 4985-5120). One handle owns its device
+// buffers and a stream; all work is issued on that stream with no host
+// synchronisation inside a step (the reference syncs twice per step: the vmax
+// read and the end-of-step event; sd_step_auto keeps the vmax read).
+//
+// Step pipeline (periodic, plain PM):
+//   [sort]    keys -> stable LSD radix sort -> reorder pos/vel (ping-pong buffers)
+//   deposit   int64 fixed-point CIC into `acc`
+//   Poisson   pass A (reads and clears acc) .. pass E -> phi
+//   gather    gradient of phi at the 8 corners + kick + clamp + drift + wrap,
+//             FP64 momentum partials -> mean, subtracted at the next load
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <atomic>
+#include <mutex>
+#include <vector>
+
+#include "sd_internal.h"
+
+// ---------------------------------------------------------------------------
+// sticky error record and launch accounting
+// ---------------------------------------------------------------------------
+namespace sd {
+namespace {
+std::mutex g_err_mu;
+bool g_failed = false;
+char g_msg[512] = {0};
+std::atomic<long long> g_launches{0};
+}  // namespace
+
+int fail(int code, const char* fmt, ...) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    if (!g_failed) {
+        g_failed = true;
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(g_msg, sizeof(g_msg), fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+int check_cuda(cudaError_t e, const char* what, const char* file, int line) {
+    if (e == cudaSuccess) return SD_OK;
+    const char* base = strrchr(file, '/');
+    fail(e == cudaErrorMemoryAllocation ? SD_E_NOMEM : SD_E_CUDA, "%s: %s (%s:%d)", what, cudaGetErrorString(e),
+         base ? base + 1 : file, line);
+    return e == cudaErrorMemoryAllocation ? SD_E_NOMEM : SD_E_CUDA;
+}
+
+void count_launch(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launches() { return g_launches.load(std::memory_order_relaxed); }
+}  // namespace sd
+
+using namespace sd;
+
+// ---------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------
+struct sd_sim {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    bool configured = false;
+    bool cuda_failed = false;
+    sd_config cfg{};
+    int N = 0;          // slots (allocN)
+    int G = 0;
+    int active = 0;     // slots loaded by the last set_particles / load_state
+    double sim_time = 0.0;
+    int step_count = 0;
+
+    float4 *pos = nullptr, *vel = nullptr, *pos2 = nullptr, *vel2 = nullptr;
+    uint32_t *keys = nullptr, *keys2 = nullptr, *keys3 = nullptr;
+    int32_t *vals = nullptr, *vals2 = nullptr;
+    void* sort_ws = nullptr;
+    size_t sort_ws_bytes = 0;
+    long long* acc = nullptr;
+    float2 *specA = nullptr, *specB = nullptr;
+    float* phi = nullptr;
+    float* rho = nullptr;        // kept density (keep_density)
+    double* partials = nullptr;  // gather / energy / reduction partials
+    size_t partials_count = 0;
+    double* mom = nullptr;       // 8 doubles: momentum sums of the last step, energy results
+    float* mean = nullptr;       // 4 floats: pending mean velocity; [3] = max speed scratch
+    bool mean_pending = false;
+    bool rho_valid = false;
+    PoissonPlan plan;
+
+    // leapfrog
+    bool lf_open = false;
+    float lf_dt_prev = 0.f;
+
+    // timings of the last eager step
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool ev_valid = false;
+    sd_timings tm{};
+    sd_diagnostics diag{};
+    bool diag_valid = false;
+
+    // captured steps for sd_steps
+    cudaGraphExec_t graph = nullptr;
+    float graph_dt = 0.f;
+    long long graph_launches = 0;  // kernels inside one replay
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int ceil_pow2_clamp(int g, int cap) {
+    if (g <= 0) g = 64;
+    if (g > cap) g = cap;
+    if (g < 16) g = 16;
+    int p = 16;
+    while (p * 2 <= g) p *= 2;  // round down to a power of two (Sim.cu:4081-4086)
+    return p;
+}
+
+float light_speed_sq(float length_scale, float time_unit_scale) {
+    // lightSpeedSqFor (Sim.h:133-148): c = (1e7 * tus) / (1e5 * ls)
+    const double L = 1.0e5 * (double)(length_scale > 1e-6f ? length_scale : 1e-6f);
+    const double T = 1.0e7 * (double)(time_unit_scale > 1e-6f ? time_unit_scale : 1e-6f);
+    const float c = (float)(T / (L > 1e-30 ? L : 1e-30));
+    return c * c;
+}
+
+float dt_scale_for(float ts) {  // dtScaleFor (Sim.h:89-93)
+    if (ts <= 1.0f) return ts;
+    return (ts <= 3.0f) ? 1.0f : (ts / 3.0f);
+}
+
+int key_bits_for(int G, int order) {
+    const long long top = (order == SD_ORDER_TILED) ? (long long)G * G : (long long)G * G * G;
+    int b = 0;
+    while ((1ll << b) < top + 1) ++b;
+    return b;
+}
+
+float pot_scale_of(const sd_sim* s) {
+    const double n = (double)(s->N > 0 ? s->N : 1);
+    if (s->cfg.units == SD_UNITS_NEWTON)
+        return (float)(4.0 * 3.14159265358979323846 * (double)s->G * s->G * s->G * (double)s->cfg.gravity / n);
+    return s->cfg.gravity / (float)(s->N > 0 ? s->N : 1);  // potScale (Sim.cu:3107-3109)
+}
+
+template <class T>
+void free_dev(T*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+void free_buffers(sd_sim* s) {
+    free_dev(s->pos); free_dev(s->vel); free_dev(s->pos2); free_dev(s->vel2);
+    free_dev(s->keys); free_dev(s->keys2); free_dev(s->keys3);
+    free_dev(s->vals); free_dev(s->vals2);
+    if (s->sort_ws) cudaFree(s->sort_ws);
+    s->sort_ws = nullptr;
+    s->sort_ws_bytes = 0;
+    free_dev(s->acc); free_dev(s->specA); free_dev(s->specB); free_dev(s->phi); free_dev(s->rho);
+    free_dev(s->partials); free_dev(s->mom); free_dev(s->mean);
+    poisson_plan_free(s->plan);
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+    s->configured = false;
+}
+
+template <class T>
+int alloc_dev(T*& p, size_t count) {
+    if (cudaMalloc((void**)&p, sizeof(T) * (count > 0 ? count : 1)) != cudaSuccess) {
+        cudaGetLastError();
+        p = nullptr;
+        return fail(SD_E_NOMEM, "cudaMalloc of %zu bytes failed", sizeof(T) * count);
+    }
+    return SD_OK;
+}
+
+size_t estimate_bytes(int n, int G) {
+    const size_t N = (size_t)(n > 0 ? n : 1), cells = (size_t)G * G * G;
+    size_t b = 0;
+    b += sizeof(float4) * N * 4;                       // pos, vel, pos2, vel2
+    b += (sizeof(uint32_t) * 3 + sizeof(int32_t) * 2) * N;
+    b += sort_workspace_bytes((int)N);
+    b += sizeof(long long) * cells;                    // fixed-point deposit
+    b += 2 * sizeof(float2) * poisson_spectrum_elems(G);
+    b += sizeof(float) * cells * 2;                    // phi, kept density
+    b += sizeof(double) * 8 * (gather_partials((int)N) + 1024);
+    return b;
+}
+
+int allocate(sd_sim* s) {
+    free_buffers(s);
+    const size_t N = (size_t)s->N, cells = (size_t)s->G * s->G * s->G;
+    int rc = SD_OK;
+    rc = rc ? rc : alloc_dev(s->pos, N);
+    rc = rc ? rc : alloc_dev(s->vel, N);
+    rc = rc ? rc : alloc_dev(s->pos2, N);
+    rc = rc ? rc : alloc_dev(s->vel2, N);
+    rc = rc ? rc : alloc_dev(s->keys, N);
+    rc = rc ? rc : alloc_dev(s->keys2, N);
+    rc = rc ? rc : alloc_dev(s->keys3, N);
+    rc = rc ? rc : alloc_dev(s->vals, N);
+    rc = rc ? rc : alloc_dev(s->vals2, N);
+    s->sort_ws_bytes = sort_workspace_bytes(s->N);
+    if (!rc && cudaMalloc(&s->sort_ws, s->sort_ws_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        rc = fail(SD_E_NOMEM, "cudaMalloc of sort workspace failed");
+    }
+    rc = rc ? rc : alloc_dev(s->acc, cells);
+    rc = rc ? rc : alloc_dev(s->specA, poisson_spectrum_elems(s->G));
+    rc = rc ? rc : alloc_dev(s->specB, poisson_spectrum_elems(s->G));
+    rc = rc ? rc : alloc_dev(s->phi, cells);
+    if (!rc && s->cfg.keep_density) rc = alloc_dev(s->rho, cells);
+    s->partials_count = 8 * (gather_partials(s->N) + 1024);
+    rc = rc ? rc : alloc_dev(s->partials, s->partials_count);
+    rc = rc ? rc : alloc_dev(s->mom, 8);
+    rc = rc ? rc : alloc_dev(s->mean, 4);
+    if (rc) {
+        free_buffers(s);
+        return rc;
+    }
+    rc = poisson_plan_build(s->plan, s->G, s->cfg.softening_cells);
+    if (rc) {
+        free_buffers(s);
+        return rc;
+    }
+    // zeroed state: empty slots, clear fixed-point grid, no pending mean
+    if (SD_CUDA(cudaMemsetAsync(s->acc, 0, sizeof(long long) * cells, s->stream)) ||
+        SD_CUDA(cudaMemsetAsync(s->mean, 0, sizeof(float) * 4, s->stream)) ||
+        SD_CUDA(cudaMemsetAsync(s->mom, 0, sizeof(double) * 8, s->stream)) ||
+        SD_CUDA(cudaMemsetAsync(s->phi, 0, sizeof(float) * cells, s->stream))) {
+        free_buffers(s);
+        return SD_E_CUDA;
+    }
+    rc = launch_hide_range(s->pos, s->vel, 0, s->N, s->stream);
+    if (rc) return rc;
+    s->configured = true;
+    return SD_OK;
+}
+
+int validate_config(const sd_config* c) {
+    if (!c) return fail(SD_E_ARG, "config: null");
+    if (c->particle_count <= 0 || c->particle_count > 400000000)
+        return fail(SD_E_ARG, "config: particle_count %d out of range", c->particle_count);
+    if (c->boundary != SD_BOUNDARY_PERIODIC)
+        return fail(SD_E_UNSUPPORTED, "config: only the periodic boundary is implemented");
+    if (c->order < SD_ORDER_ROWMAJOR || c->order > SD_ORDER_TILED) return fail(SD_E_ARG, "config: bad order");
+    if (c->integrator != SD_INT_KD && c->integrator != SD_INT_KDK) return fail(SD_E_ARG, "config: bad integrator");
+    if (c->units != SD_UNITS_REFERENCE && c->units != SD_UNITS_NEWTON) return fail(SD_E_ARG, "config: bad units");
+    return SD_OK;
+}
+
+int sim_error(sd_sim* s, int rc) {
+    if (rc == SD_E_CUDA) s->cuda_failed = true;
+    return rc;
+}
+
+// Apply the pending mean-velocity subtraction to the stored velocities.
+int materialize(sd_sim* s) {
+    if (!s->mean_pending) return SD_OK;
+    int rc = launch_apply_mean(s->vel, s->pos, s->N, s->mean, s->stream);
+    if (rc) return sim_error(s, rc);
+    if (SD_CUDA(cudaMemsetAsync(s->mean, 0, sizeof(float) * 3, s->stream))) return sim_error(s, SD_E_CUDA);
+    s->mean_pending = false;
+    return SD_OK;
+}
+
+int ensure_events(sd_sim* s) {
+    if (s->ev[0]) return SD_OK;
+    for (auto& e : s->ev)
+        if (SD_CUDA(cudaEventCreate(&e))) return SD_E_CUDA;
+    return SD_OK;
+}
+
+// Sort + reorder (sortParticles, Sim.cu:3656-3671).
+int do_sort(sd_sim* s, int32_t* perm_out_dev) {
+    int rc = launch_cell_keys(s->pos, s->N, s->G, s->cfg.order, s->keys, s->stream);
+    if (rc) return rc;
+    rc = launch_sort_pairs(s->keys, nullptr, s->keys2, s->vals, s->keys3, s->vals2, s->N,
+                           key_bits_for(s->G, s->cfg.order), s->sort_ws, s->sort_ws_bytes, s->stream);
+    if (rc) return rc;
+    rc = launch_reorder(s->pos, s->vel, s->vals, s->pos2, s->vel2, s->N, s->stream);
+    if (rc) return rc;
+    if (perm_out_dev &&
+        SD_CUDA(cudaMemcpyAsync(perm_out_dev, s->vals, sizeof(int32_t) * s->N, cudaMemcpyDeviceToDevice, s->stream)))
+        return SD_E_CUDA;
+    float4* t = s->pos; s->pos = s->pos2; s->pos2 = t;
+    t = s->vel; s->vel = s->vel2; s->vel2 = t;
+    return SD_OK;
+}
+
+// Field for the current positions: deposit + Poisson -> phi (computeAccel, Sim.cu:3605-3633).
+int do_field(sd_sim* s, bool keep) {
+    int rc = launch_deposit_fixed(s->pos, s->N, s->G, s->acc, s->stream);
+    if (rc) return rc;
+    rc = launch_poisson(s->plan, s->acc, nullptr, 1, keep ? s->rho : nullptr, s->specA, s->specB, s->phi, s->stream);
+    if (rc) return rc;
+    if (keep) s->rho_valid = true;
+    return SD_OK;
+}
+
+int do_step(sd_sim* s, float dt, bool sort, bool timed) {
+    if (!s->configured) return fail(SD_E_STATE, "step: not initialised");
+    if (s->cuda_failed) return SD_E_CUDA;
+    float dt_kick = dt, dt_drift = dt;
+    if (s->cfg.integrator == SD_INT_KDK) {
+        dt_kick = s->lf_open ? 0.5f * (s->lf_dt_prev + dt) : 0.5f * dt;
+        s->lf_open = true;
+        s->lf_dt_prev = dt;
+    }
+    int rc = SD_OK;
+    if (timed && (rc = ensure_events(s))) return sim_error(s, rc);
+    if (timed) cudaEventRecord(s->ev[0], s->stream);
+    if (sort && (rc = do_sort(s, nullptr))) return sim_error(s, rc);
+    if (timed) cudaEventRecord(s->ev[1], s->stream);
+    const bool keep = s->cfg.keep_density && s->rho;
+    if ((rc = launch_deposit_fixed(s->pos, s->N, s->G, s->acc, s->stream))) return sim_error(s, rc);
+    if (timed) cudaEventRecord(s->ev[2], s->stream);
+    if ((rc = launch_poisson(s->plan, s->acc, nullptr, 1, keep ? s->rho : nullptr, s->specA, s->specB, s->phi,
+                             s->stream)))
+        return sim_error(s, rc);
+    if (keep) s->rho_valid = true;
+    if (timed) cudaEventRecord(s->ev[3], s->stream);
+    const float c2 = light_speed_sq(s->cfg.length_scale, s->cfg.time_unit_scale);
+    // The mean written last step is read here as the correction for the loaded
+    // velocities; the finalize kernel then overwrites it with this step's mean.
+    rc = launch_gather_kick_drift(s->phi, s->G, pot_scale_of(s), s->pos, s->vel, s->N, dt_kick, dt_drift, c2,
+                                  s->mean, s->partials, s->mom, s->mean, s->stream);
+    if (rc) return sim_error(s, rc);
+    s->mean_pending = true;
+    if (timed) cudaEventRecord(s->ev[4], s->stream);
+    s->ev_valid = timed;
+    if (s->cfg.diagnostics) {
+        // FP64 energy and momentum after the step (phi is that of the step-start positions)
+        rc = launch_energy(s->phi, s->G, s->pos, s->vel, s->N, s->mean, s->partials, s->mom, s->stream);
+        if (rc) return sim_error(s, rc);
+        s->diag_valid = true;
+    }
+    s->sim_time += dt;
+    ++s->step_count;
+    return SD_OK;
+}
+
+bool sort_due(const sd_sim* s) {
+    return s->cfg.sort_interval > 0 && (s->step_count % s->cfg.sort_interval) == 0;
+}
+
+int copy_in(void* dst, const void* src, size_t bytes, int where, cudaStream_t st) {
+    const cudaMemcpyKind k = (where == SD_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    return SD_CUDA(cudaMemcpyAsync(dst, src, bytes, k, st));
+}
+
+int copy_out(void* dst, const void* src, size_t bytes, int where, cudaStream_t st) {
+    const cudaMemcpyKind k = (where == SD_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    int rc = SD_CUDA(cudaMemcpyAsync(dst, src, bytes, k, st));
+    if (rc == SD_OK && where == SD_HOST) rc = SD_CUDA(cudaStreamSynchronize(st));
+    return rc;
+}
+
+int reconfigure(sd_sim* s, const sd_config* c) {
+    int rc = validate_config(c);
+    if (rc) return rc;
+    const int G = ceil_pow2_clamp(c->grid_size, sd_max_grid_size(c->boundary));
+    const bool structural = !s->configured || c->particle_count != s->N || G != s->G ||
+                            c->boundary != s->cfg.boundary || (c->keep_density && !s->rho);
+    const bool soft_changed = c->softening_cells != s->cfg.softening_cells;
+    s->cfg = *c;
+    s->cfg.grid_size = G;
+    if (!structural) {
+        if (s->graph) cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+        return soft_changed ? poisson_plan_build(s->plan, s->G, s->cfg.softening_cells) : SD_OK;
+    }
+    s->N = c->particle_count;
+    s->G = G;
+    rc = allocate(s);
+    if (rc) return rc;
+    s->active = 0;
+    s->sim_time = 0.0;
+    s->step_count = 0;
+    s->mean_pending = false;
+    s->lf_open = false;
+    s->rho_valid = false;
+    s->cuda_failed = false;
+    return SD_OK;
+}
+
+// STARDUST v1/v2 header (Sim.cu:4985-4997), byte-compatible.
+struct StateHeader {
+    char magic[8];
+    int32_t version;
+    int32_t count;
+    int32_t gridSize;
+    int32_t preset;
+    int32_t boundary;
+    float gravity;
+    float simTime;
+    float bhX, bhY, bhRs, bhMass;
+    int32_t bhActive;
+    int32_t reserved[5];
+};
+static_assert(sizeof(StateHeader) == 76, "STARDUST header layout");
+constexpr size_t kBlackHoleRecord = 48;  // sizeof(BlackHoleState) (Sim.h:813-825)
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int sd_abi_version(void) { return SD_ABI_VERSION; }
+
+int sd_device_available(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n > 0 ? 1 : 0;
+}
+
+int sd_failed(void) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    return g_failed ? 1 : 0;
+}
+
+const char* sd_last_error(void) { return g_msg; }
+
+void sd_clear_error(void) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_failed = false;
+    g_msg[0] = 0;
+}
+
+int sd_config_default(sd_config* c) {
+    if (!c) return fail(SD_E_ARG, "config_default: null");
+    memset(c, 0, sizeof(*c));
+    c->particle_count = 2000000;  // Sim.h:166
+    c->grid_size = 128;           // Sim.h:167
+    c->boundary = SD_BOUNDARY_PERIODIC;
+    c->gravity = 1.0f;
+    c->softening_cells = 3.0f;    // Sim.h:315
+    c->time_scale = 1.0f;         // Sim.h:316
+    c->sort_interval = 1;
+    c->length_scale = 1.0f;       // Sim.h:172
+    c->time_unit_scale = 1.0f;    // Sim.h:180
+    c->order = SD_ORDER_ROWMAJOR;
+    c->integrator = SD_INT_KD;
+    c->units = SD_UNITS_REFERENCE;
+    c->diagnostics = 0;
+    c->keep_density = 1;
+    return SD_OK;
+}
+
+int sd_max_grid_size(int boundary) { return boundary == SD_BOUNDARY_ISOLATED ? 256 : 512; }
+
+size_t sd_estimate_bytes(int particle_count, int grid_size, int boundary) {
+    const int G = ceil_pow2_clamp(grid_size, sd_max_grid_size(boundary));
+    return estimate_bytes(particle_count, G);
+}
+
+int sd_create(sd_sim** out, int device) {
+    if (!out) return fail(SD_E_ARG, "create: null out");
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return fail(SD_E_CUDA, "create: no CUDA device %d", device);
+    }
+    sd_sim* s = new sd_sim();
+    s->device = device;
+    DeviceGuard g(device);
+    if (SD_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking))) {
+        delete s;
+        return SD_E_CUDA;
+    }
+    s->own_stream = true;
+    sd_config_default(&s->cfg);
+    *out = s;
+    return SD_OK;
+}
+
+int sd_destroy(sd_sim* s) {
+    if (!s) return SD_OK;
+    DeviceGuard g(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    free_buffers(s);
+    for (auto& e : s->ev)
+        if (e) cudaEventDestroy(e);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return SD_OK;
+}
+
+int sd_set_stream(sd_sim* s, void* stream) {
+    if (!s) return fail(SD_E_ARG, "set_stream: null handle");
+    DeviceGuard g(s->device);
+    cudaStreamSynchronize(s->stream);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    s->stream = (cudaStream_t)stream;
+    s->own_stream = false;
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+    return SD_OK;
+}
+
+int sd_init(sd_sim* s, const sd_config* c) {
+    if (!s) return fail(SD_E_ARG, "init: null handle");
+    DeviceGuard g(s->device);
+    s->configured = false;
+    return reconfigure(s, c);
+}
+
+int sd_reconfigure(sd_sim* s, const sd_config* c) {
+    if (!s) return fail(SD_E_ARG, "reconfigure: null handle");
+    DeviceGuard g(s->device);
+    return reconfigure(s, c);
+}
+
+int sd_reset(sd_sim* s) {
+    if (!s || !s->configured) return fail(SD_E_STATE, "reset: not initialised");
+    DeviceGuard g(s->device);
+    s->sim_time = 0.0;
+    s->step_count = 0;
+    s->active = 0;
+    s->mean_pending = false;
+    s->lf_open = false;
+    s->rho_valid = false;
+    if (SD_CUDA(cudaMemsetAsync(s->mean, 0, sizeof(float) * 4, s->stream))) return SD_E_CUDA;
+    return launch_hide_range(s->pos, s->vel, 0, s->N, s->stream);
+}
+
+int sd_get_config(const sd_sim* s, sd_config* out) {
+    if (!s || !out) return fail(SD_E_ARG, "get_config: null");
+    *out = s->cfg;
+    return SD_OK;
+}
+
+int sd_set_particles(sd_sim* s, const float* pos, const float* vel, int n, int where) {
+    if (!s || !s->configured) return fail(SD_E_STATE, "set_particles: not initialised");
+    if (!pos || !vel || n < 0 || n > s->N) return fail(SD_E_ARG, "set_particles: bad arguments (n=%d)", n);
+    DeviceGuard g(s->device);
+    int rc = copy_in(s->pos, pos, sizeof(float4) * (size_t)n, where, s->stream);
+    if (!rc) rc = copy_in(s->vel, vel, sizeof(float4) * (size_t)n, where, s->stream);
+    if (!rc) rc = launch_hide_range(s->pos, s->vel, n, s->N, s->stream);
+    if (!rc && SD_CUDA(cudaMemsetAsync(s->mean, 0, sizeof(float) * 4, s->stream))) rc = SD_E_CUDA;
+    if (!rc && where == SD_HOST) rc = SD_CUDA(cudaStreamSynchronize(s->stream));
+    if (rc) return sim_error(s, rc);
+    s->active = n;
+    s->mean_pending = false;
+    s->lf_open = false;
+    s->rho_valid = false;
+    return SD_OK;
+}
+
+int sd_get_particles(sd_sim* s, float* pos, float* vel, int n, int where) {
+    if (!s || !s->configured) return fail(SD_E_STATE, "get_particles: not initialised");
+    if (n < 0 || n > s->N) return fail(SD_E_ARG, "get_particles: bad n=%d", n);
+    DeviceGuard g(s->device);
+    int rc = materialize(s);
+    if (!rc && pos) rc = copy_out(pos, s->pos, sizeof(float4) * (size_t)n, where, s->stream);
+    if (!rc && vel) rc = copy_out(vel, s->vel, sizeof(float4) * (size_t)n, where, s->stream);
+    return rc ? sim_error(s, rc) : SD_OK;
+}
+
+const float* sd_particle_pos_device_ptr(sd_sim* s) {
+    if (!s || !s->configured) return nullptr;
+    DeviceGuard g(s->device);
+    materialize(s);
+    return reinterpret_cast<const float*>(s->pos);
+}
+
+const float* sd_particle_vel_device_ptr(sd_sim* s) {
+    if (!s || !s->configured) return nullptr;
+    DeviceGuard g(s->device);
+    materialize(s);
+    return reinterpret_cast<const float*>(s->vel);
+}
+
+const float* sd_density_device_ptr(sd_sim* s) {
+    if (!s || !s->configured || !s->rho || !s->rho_valid) return nullptr;
+    return s->rho;
+}
+
+int sd_get_density(sd_sim* s, float* out, int where) {
+    if (!s || !s->configured || !out) return fail(SD_E_STATE, "get_density: not initialised");
+    DeviceGuard g(s->device);
+    if (!s->rho) return fail(SD_E_STATE, "get_density: keep_density is off");
+    if (!s->rho_valid) {  // no step yet: density of the current positions
+        int rc = do_field(s, true);
+        if (rc) return sim_error(s, rc);
+    }
+    return copy_out(out, s->rho, sizeof(float) * (size_t)s->G * s->G * s->G, where, s->stream);
+}
+
+int sd_get_potential(sd_sim* s, float* out, int where) {
+    if (!s || !s->configured || !out) return fail(SD_E_STATE, "get_potential: not initialised");
+    DeviceGuard g(s->device);
+    return copy_out(out, s->phi, sizeof(float) * (size_t)s->G * s->G * s->G, where, s->stream);
+}
+
+int sd_get_accel(sd_sim* s, float* out, int n, int where) {
+    if (!s || !s->configured || !out) return fail(SD_E_STATE, "get_accel: not initialised");
+    if (n < 0 || n > s->N) return fail(SD_E_ARG, "get_accel: bad n=%d", n);
+    DeviceGuard g(s->device);
+    int rc = do_field(s, s->cfg.keep_density && s->rho);
+    if (rc) return sim_error(s, rc);
+    float4* dst = reinterpret_cast<float4*>(out);
+    float4* tmp = nullptr;
+    if (where == SD_HOST) tmp = s->pos2;  // scratch: pos2 is free between steps
+    rc = launch_interpolate_accel(s->phi, s->G, pot_scale_of(s), s->pos, tmp ? tmp : dst, n, s->stream);
+    if (rc) return sim_error(s, rc);
+    if (tmp) return copy_out(out, tmp, sizeof(float4) * (size_t)n, SD_HOST, s->stream);
+    return SD_OK;
+}
+
+int sd_step(sd_sim* s, float dt) {
+    if (!s) return fail(SD_E_ARG, "step: null handle");
+    DeviceGuard g(s->device);
+    const bool sort = sort_due(s);
+    int rc = do_step(s, dt, sort, true);
+    if (rc) return rc;
+    s->tm.dt_used = dt;
+    s->tm.steps = 1;
+    return SD_OK;
+}
+
+int sd_step_auto(sd_sim* s) {
+    if (!s || !s->configured) return fail(SD_E_STATE, "step_auto: not initialised");
+    DeviceGuard g(s->device);
+    // CFL (Sim.cu:4255-4269): vmax of the current (momentum-zeroed) velocities.
+    int rc = launch_max_speed(s->pos, s->vel, s->N, s->mean_pending ? s->mean : nullptr, s->mean + 3, s->stream);
+    if (rc) return sim_error(s, rc);
+    float vmax = 0.f;
+    rc = copy_out(&vmax, s->mean + 3, sizeof(float), SD_HOST, s->stream);
+    if (rc) return sim_error(s, rc);
+    const float cell = 1.0f / (float)s->G;
+    float dt = 0.0016f * dt_scale_for(s->cfg.time_scale);
+    const float dt_max = (vmax > 1e-6f) ? (0.8f * cell / vmax) : dt;
+    if (dt > dt_max) dt = dt_max;
+    rc = do_step(s, dt, sort_due(s), true);
+    if (rc) return rc;
+    s->tm.dt_used = dt;
+    s->tm.max_speed = vmax;
+    s->tm.steps = 1;
+    return SD_OK;
+}
+
+int sd_steps(sd_sim* s, float dt, int nsteps) {
+    if (!s || !s->configured) return fail(SD_E_STATE, "steps: not initialised");
+    if (nsteps < 0) return fail(SD_E_ARG, "steps: negative count");
+    DeviceGuard g(s->device);
+    const bool graphable = (s->cfg.sort_interval == 0 || s->cfg.sort_interval == 1) && !s->cfg.diagnostics;
+    int done = 0;
+    // leapfrog opening kick and odd counts run eagerly
+    while (done < nsteps && (!graphable || (s->cfg.integrator == SD_INT_KDK && !s->lf_open))) {
+        int rc = do_step(s, dt, sort_due(s), false);
+        if (rc) return rc;
+        ++done;
+    }
+    if (done >= nsteps) return SD_OK;
+    const bool sort = s->cfg.sort_interval == 1;
+    // A captured graph covers two steps so the pos/pos2 ping-pong returns to the
+    // same buffers; it is rebuilt when dt changes.
+    if (!s->graph || s->graph_dt != dt) {
+        if (s->graph) cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+        cudaGraph_t graph = nullptr;
+        if (SD_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal))) return sim_error(s, SD_E_CUDA);
+        const double t0 = s->sim_time;
+        const int c0 = s->step_count;
+        const bool lf0 = s->lf_open;
+        const float lfd = s->lf_dt_prev;
+        const bool mp0 = s->mean_pending;
+        const long long l0 = launches();
+        int rc = do_step(s, dt, sort, false);
+        if (!rc) rc = do_step(s, dt, sort, false);
+        cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+        // capture only recorded the kernels; count them per replay instead
+        s->graph_launches = launches() - l0;
+        count_launch(-s->graph_launches);
+        // capture recorded work only; restore the host-side counters
+        s->sim_time = t0;
+        s->step_count = c0;
+        s->lf_open = lf0;
+        s->lf_dt_prev = lfd;
+        s->mean_pending = mp0;
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (SD_CUDA(e)) return sim_error(s, SD_E_CUDA);
+        e = cudaGraphInstantiate(&s->graph, graph, 0);
+        cudaGraphDestroy(graph);
+        if (SD_CUDA(e)) return sim_error(s, SD_E_CUDA);
+        s->graph_dt = dt;
+    }
+    while (nsteps - done >= 2) {
+        if (SD_CUDA(cudaGraphLaunch(s->graph, s->stream))) return sim_error(s, SD_E_CUDA);
+        count_launch(s->graph_launches);
+        s->sim_time += 2.0 * dt;
+        s->step_count += 2;
+        s->mean_pending = true;
+        if (s->cfg.integrator == SD_INT_KDK) {
+            s->lf_open = true;
+            s->lf_dt_prev = dt;
+        }
+        done += 2;
+    }
+    if (done < nsteps) {
+        int rc = do_step(s, dt, sort_due(s), false);
+        if (rc) return rc;
+    }
+    s->ev_valid = false;
+    return SD_OK;
+}
+
+int sd_synchronize(sd_sim* s) {
+    if (!s || !s->configured) return fail(SD_E_STATE, "synchronize: not initialised");
+    if (s->cfg.integrator != SD_INT_KDK || !s->lf_open) return SD_OK;
+    DeviceGuard g(s->device);
+    int rc = do_field(s, false);
+    if (rc) return sim_error(s, rc);
+    const float c2 = light_speed_sq(s->cfg.length_scale, s->cfg.time_unit_scale);
+    rc = launch_gather_kick_drift(s->phi, s->G, pot_scale_of(s), s->pos, s->vel, s->N, 0.5f * s->lf_dt_prev, 0.f,
+                                  c2, s->mean, s->partials, s->mom, s->mean, s->stream);
+    if (rc) return sim_error(s, rc);
+    s->mean_pending = true;
+    s->lf_open = false;
+    return SD_OK;
+}
+
+int sd_sort_only(sd_sim* s, int32_t* perm, int where) {
+    if (!s || !s->configured) return fail(SD_E_STATE, "sort_only: not initialised");
+    DeviceGuard g(s->device);
+    int32_t* dev_perm = nullptr;
+    if (perm && where == SD_DEVICE) dev_perm = perm;
+    int rc = do_sort(s, dev_perm);
+    if (rc) return sim_error(s, rc);
+    if (perm && where == SD_HOST) {
+        // do_sort leaves the permutation in vals
+        rc = copy_out(perm, s->vals, sizeof(int32_t) * (size_t)s->N, SD_HOST, s->stream);
+        if (rc) return sim_error(s, rc);
+    }
+    s->rho_valid = false;
+    return SD_OK;
+}
+
+int sd_save_state(sd_sim* s, const char* path) {
+    if (!s || !s->configured || !path) return fail(SD_E_STATE, "save_state: not initialised");
+    DeviceGuard g(s->device);
+    const int n = (s->active > 0) ? s->active : s->N;
+    std::vector<float4> hp((size_t)n), hv((size_t)n);
+    int rc = sd_get_particles(s, reinterpret_cast<float*>(hp.data()), reinterpret_cast<float*>(hv.data()), n, SD_HOST);
+    if (rc) return rc;
+    StateHeader h;
+    memset(&h, 0, sizeof(h));
+    memcpy(h.magic, "STARDUST", 8);
+    h.version = 2;
+    h.count = n;
+    h.gridSize = s->G;
+    h.preset = 1;  // Preset::Empty: the particles are the scene
+    h.boundary = s->cfg.boundary;
+    h.gravity = s->cfg.gravity;
+    h.simTime = (float)s->sim_time;
+    h.bhX = h.bhY = 0.5f;
+    FILE* f = fopen(path, "wb");
+    if (!f) return fail(SD_E_IO, "save_state: cannot open %s", path);
+    bool ok = fwrite(&h, sizeof(h), 1, f) == 1 && fwrite(hp.data(), sizeof(float4), (size_t)n, f) == (size_t)n &&
+              fwrite(hv.data(), sizeof(float4), (size_t)n, f) == (size_t)n;
+    ok = (fclose(f) == 0) && ok;
+    return ok ? SD_OK : fail(SD_E_IO, "save_state: write failed for %s", path);
+}
+
+int sd_load_state(sd_sim* s, const char* path) {
+    if (!s || !path) return fail(SD_E_ARG, "load_state: null");
+    DeviceGuard g(s->device);
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(SD_E_IO, "load_state: cannot open %s", path);
+    StateHeader h;
+    if (fread(&h, sizeof(h), 1, f) != 1 || memcmp(h.magic, "STARDUST", 8) != 0 || (h.version != 1 && h.version != 2) ||
+        h.count <= 0 || h.count > 100000000) {
+        fclose(f);
+        return fail(SD_E_FORMAT, "load_state: %s is not a STARDUST v1/v2 file", path);
+    }
+    if (h.version >= 2) {
+        const int bh = h.reserved[0];
+        if (bh < 0 || bh > 8) {
+            fclose(f);
+            return fail(SD_E_FORMAT, "load_state: bad black-hole count %d", bh);
+        }
+        // Black holes are outside the plain-PM path: their records are skipped.
+        if (bh > 0 && fseek(f, (long)(kBlackHoleRecord * (size_t)bh), SEEK_CUR) != 0) {
+            fclose(f);
+            return fail(SD_E_FORMAT, "load_state: truncated black-hole records");
+        }
+    }
+    sd_config c = s->cfg;
+    c.particle_count = h.count;
+    c.grid_size = h.gridSize;
+    c.boundary = h.boundary;
+    c.gravity = h.gravity;
+    int rc = reconfigure(s, &c);
+    if (rc) {
+        fclose(f);
+        return rc;
+    }
+    const int n = h.count < s->N ? h.count : s->N;
+    std::vector<float4> hp((size_t)n), hv((size_t)n);
+    const bool ok = fread(hp.data(), sizeof(float4), (size_t)n, f) == (size_t)n &&
+                    fread(hv.data(), sizeof(float4), (size_t)n, f) == (size_t)n;
+    fclose(f);
+    if (!ok) return fail(SD_E_FORMAT, "load_state: truncated particle data");
+    rc = sd_set_particles(s, reinterpret_cast<const float*>(hp.data()), reinterpret_cast<const float*>(hv.data()), n,
+                          SD_HOST);
+    if (rc) return rc;
+    s->sim_time = h.simTime;
+    return SD_OK;
+}
+
+int sd_timings_get(const sd_sim* s, sd_timings* out) {
+    if (!s || !out) return fail(SD_E_ARG, "timings: null");
+    *out = s->tm;
+    if (s->ev_valid) {
+        DeviceGuard g(s->device);
+        cudaEventSynchronize(s->ev[4]);
+        float ms[4] = {0, 0, 0, 0}, tot = 0.f;
+        for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&ms[i], s->ev[i], s->ev[i + 1]);
+        cudaEventElapsedTime(&tot, s->ev[0], s->ev[4]);
+        out->sort_ms = ms[0];
+        out->deposit_ms = ms[1];
+        out->poisson_ms = ms[2];
+        out->gather_ms = ms[3];
+        out->total_ms = tot;
+    }
+    return SD_OK;
+}
+
+double sd_sim_time(const sd_sim* s) { return s ? s->sim_time : 0.0; }
+int sd_grid_size(const sd_sim* s) { return s ? s->G : 0; }
+int sd_particle_count(const sd_sim* s) { return s ? s->N : 0; }
+int sd_active_count(const sd_sim* s) { return s ? s->active : 0; }
+int sd_step_count(const sd_sim* s) { return s ? s->step_count : 0; }
+
+static double reduce_rho(sd_sim* s, int op) {
+    if (!s || !s->configured || !s->rho) return 0.0;
+    DeviceGuard g(s->device);
+    if (!s->rho_valid && do_field(s, true)) return 0.0;
+    double out = 0.0;
+    if (launch_reduce_grid(s->rho, (size_t)s->G * s->G * s->G, op, s->partials, s->mom + 7, s->stream)) return 0.0;
+    if (copy_out(&out, s->mom + 7, sizeof(double), SD_HOST, s->stream)) return 0.0;
+    return out;
+}
+
+double sd_measure_total_grid_mass(sd_sim* s) { return reduce_rho(s, 0); }
+double sd_measure_max_density(sd_sim* s) { return reduce_rho(s, 1); }
+
+double sd_measure_kinetic_energy(sd_sim* s) {
+    if (!s || !s->configured) return 0.0;
+    DeviceGuard g(s->device);
+    double out[8];
+    if (launch_energy(nullptr, s->G, s->pos, s->vel, s->N, s->mean_pending ? s->mean : nullptr, s->partials, s->mom,
+                      s->stream))
+        return 0.0;
+    if (copy_out(out, s->mom, sizeof(double) * 8, SD_HOST, s->stream)) return 0.0;
+    return out[0] / (double)(s->N > 0 ? s->N : 1);  // m = 1/N (Sim.cu:5141-5149)
+}
+
+int sd_diagnostics_get(sd_sim* s, sd_diagnostics* out) {
+    if (!s || !out || !s->configured) return fail(SD_E_ARG, "diagnostics: null");
+    DeviceGuard g(s->device);
+    double d[8];
+    // momentum sums of the last gather (before zeroing) and energies after zeroing
+    int rc = launch_energy(s->phi, s->G, s->pos, s->vel, s->N, s->mean_pending ? s->mean : nullptr, s->partials,
+                           s->mom, s->stream);
+    if (rc) return sim_error(s, rc);
+    rc = copy_out(d, s->mom, sizeof(double) * 8, SD_HOST, s->stream);
+    if (rc) return sim_error(s, rc);
+    float mean[4] = {0, 0, 0, 0};
+    rc = copy_out(mean, s->mean, sizeof(float) * 4, SD_HOST, s->stream);
+    if (rc) return sim_error(s, rc);
+    // a = -pot_scale grad(phi): the potential per unit mass is pot_scale * phi; m = 1/N.
+    const double m = 1.0 / (double)(s->N > 0 ? s->N : 1);
+    out->kinetic = d[0] * m;
+    out->potential = d[1] * (double)pot_scale_of(s) * m;
+    out->momentum[0] = d[2] * m;
+    out->momentum[1] = d[3] * m;
+    out->momentum[2] = d[4] * m;
+    for (int j = 0; j < 3; ++j) out->mean_velocity_removed[j] = s->mean_pending ? mean[j] : 0.0;
+    out->live_count = d[5];
+    return SD_OK;
+}
+
+long long sd_kernel_launches(const sd_sim* s) {
+    (void)s;
+    return launches();
+}
+
+// ---- stage entry points ----------------------------------------------------
+
+int sd_key_bits(int grid_size, int order) { return key_bits_for(grid_size, order); }
+
+int sd_cell_keys(const float* pos, int n, int G, int order, uint32_t* keys, void* stream) {
+    if (!pos || !keys || n < 0 || G < 16 || (G & (G - 1)) || order < 0 || order > 2)
+        return fail(SD_E_ARG, "cell_keys: bad arguments");
+    return launch_cell_keys(reinterpret_cast<const float4*>(pos), n, G, order, keys, (cudaStream_t)stream);
+}
+
+size_t sd_sort_workspace_bytes(int n) { return sort_workspace_bytes(n); }
+
+int sd_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t* keys_out, int32_t* vals_out,
+                  uint32_t* keys_tmp, int32_t* vals_tmp, int n, int key_bits, void* ws, size_t ws_bytes,
+                  void* stream) {
+    return launch_sort_pairs(keys_in, vals_in, keys_out, vals_out, keys_tmp, vals_tmp, n, key_bits, ws, ws_bytes,
+                             (cudaStream_t)stream);
+}
+
+int sd_reorder(const float* pos_in, const float* vel_in, const int32_t* perm, float* pos_out, float* vel_out, int n,
+               void* stream) {
+    if (!pos_in || !vel_in || !perm || !pos_out || !vel_out || n < 0) return fail(SD_E_ARG, "reorder: bad arguments");
+    return launch_reorder(reinterpret_cast<const float4*>(pos_in), reinterpret_cast<const float4*>(vel_in), perm,
+                          reinterpret_cast<float4*>(pos_out), reinterpret_cast<float4*>(vel_out), n,
+                          (cudaStream_t)stream);
+}
+
+size_t sd_deposit_workspace_bytes(int G) { return deposit_workspace_bytes(G); }
+
+int sd_deposit(const float* pos, int n, int G, float* rho, void* ws, size_t ws_bytes, void* stream) {
+    if (!pos || !rho || !ws || n < 0 || G < 16 || G > 512 || (G & (G - 1)))
+        return fail(SD_E_ARG, "deposit: bad arguments");
+    if (ws_bytes < deposit_workspace_bytes(G)) return fail(SD_E_ARG, "deposit: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    long long* acc = reinterpret_cast<long long*>(ws);
+    int rc = launch_clear_u64(acc, (size_t)G * G * G, st);
+    if (!rc) rc = launch_deposit_fixed(reinterpret_cast<const float4*>(pos), n, G, acc, st);
+    if (!rc) rc = launch_fixed_to_float(acc, G, rho, 0, st);
+    return rc;
+}
+
+size_t sd_poisson_workspace_bytes(int G) { return 2 * align_up(sizeof(float2) * poisson_spectrum_elems(G), 256); }
+
+int sd_poisson(const float* rho, int G, float soft, float* phi, void* ws, size_t ws_bytes, void* stream) {
+    if (!rho || !phi || !ws || G < 16 || G > 512 || (G & (G - 1))) return fail(SD_E_ARG, "poisson: bad arguments");
+    if (ws_bytes < sd_poisson_workspace_bytes(G)) return fail(SD_E_ARG, "poisson: workspace too small");
+    // plans are cached per (G, softening); the cache is never freed (small: G float2 + G/2 floats)
+    static std::mutex mu;
+    static std::vector<PoissonPlan*> cache;
+    PoissonPlan* plan = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (PoissonPlan* p : cache)
+            if (p->G == G && p->soft == soft) plan = p;
+        if (!plan) {
+            plan = new PoissonPlan();
+            int rc = poisson_plan_build(*plan, G, soft);
+            if (rc) {
+                delete plan;
+                return rc;
+            }
+            cache.push_back(plan);
+        }
+    }
+    float2* A = reinterpret_cast<float2*>(ws);
+    float2* B = reinterpret_cast<float2*>((char*)ws + align_up(sizeof(float2) * poisson_spectrum_elems(G), 256));
+    return launch_poisson(*plan, nullptr, rho, 0, nullptr, A, B, phi, (cudaStream_t)stream);
+}
+
+size_t sd_gather_workspace_bytes(int n) { return sizeof(double) * 4 * gather_partials(n); }
+
+int sd_gather_kick_drift(const float* phi, int G, float pot_scale, float* pos, float* vel, int n, float dt_kick,
+                         float dt_drift, float c2, const float* mean_vel, double* mom_out, void* ws, size_t ws_bytes,
+                         void* stream) {
+    if (!phi || !pos || !vel || n < 0 || G < 16 || (G & (G - 1))) return fail(SD_E_ARG, "gather: bad arguments");
+    if (mom_out && (!ws || ws_bytes < sd_gather_workspace_bytes(n))) return fail(SD_E_ARG, "gather: workspace too small");
+    return launch_gather_kick_drift(phi, G, pot_scale, reinterpret_cast<float4*>(pos), reinterpret_cast<float4*>(vel),
+                                    n, dt_kick, dt_drift, c2, mean_vel, mom_out ? (double*)ws : nullptr, mom_out,
+                                    nullptr, (cudaStream_t)stream);
+}
+
+int sd_interpolate_accel(const float* phi, int G, float pot_scale, const float* pos, float* acc, int n, void* stream) {
+    if (!phi || !pos || !acc || n < 0 || G < 16 || (G & (G - 1))) return fail(SD_E_ARG, "interpolate: bad arguments");
+    return launch_interpolate_accel(phi, G, pot_scale, reinterpret_cast<const float4*>(pos),
+                                    reinterpret_cast<float4*>(acc), n, (cudaStream_t)stream);
+}
+
+}  // extern "C"

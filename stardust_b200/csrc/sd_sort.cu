@@ -1,0 +1,335 @@
+// sd_sort.cu -- cell keys, stable LSD radix sort and particle reorder.
+//
+// Replaces kCellKey (Sim.cu:2476-2486), cub::DeviceRadixSort::SortPairs
+// (Sim.cu:3659-3667) and kReorder (Sim.cu:2488-2495).
+//
+// The sort is a classic stable LSD radix sort with 8-bit digits, written for
+// sm_100a, in three kernels per digit pass:
+//   1. k_digit_counts: each 2048-key tile counts its digits in shared memory and
+//      writes them digit-major (count[d * tiles + t]);
+//   2. an exclusive scan of that digit-major array gives, for every (digit,tile),
+//      the global output offset -- digit-major order is what makes the result
+//      stable across tiles;
+//   3. k_digit_scatter: each tile ranks its keys stably (per warp, in input order,
+//      with __match_any_sync on the digit), stages them digit-sorted in shared
+//      memory and writes each digit run contiguously.
+// No kernel waits on another block, so nothing can spin. Keys are key+1 as
+// uint32, so the empty slot (reference key -1) sorts first, as CUB does with the
+// reference's signed keys.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "sd_common.cuh"
+#include "sd_internal.h"
+
+namespace sd {
+
+namespace {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per tile
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+constexpr int kWarps = kSortThreads / 32;
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__global__ void __launch_bounds__(256) k_cell_keys(const float4* __restrict__ pos, int n, int G, int order,
+                                                   uint32_t* __restrict__ keys) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    keys[i] = order_key_plus1(pos[i], G, order);
+}
+
+// Inclusive warp scan.
+__device__ __forceinline__ unsigned warp_inclusive(unsigned v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Exclusive scan across a 256-thread block; *total receives the block sum.
+__device__ __forceinline__ unsigned block_exclusive(unsigned v, unsigned* warp_sums, unsigned* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned inc = warp_inclusive(v);
+    if (lane == 31) warp_sums[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        const unsigned s = (lane < (int)(blockDim.x >> 5)) ? warp_sums[lane] : 0u;
+        const unsigned si = warp_inclusive(s);
+        if (lane < (int)(blockDim.x >> 5)) warp_sums[lane] = si - s;
+        if (lane == 31) warp_sums[32] = si;
+    }
+    __syncthreads();
+    const unsigned r = warp_sums[w] + inc - v;
+    if (total) *total = warp_sums[32];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(kSortThreads) k_digit_counts(const uint32_t* __restrict__ keys, int n, int shift,
+                                                               unsigned mask, unsigned* __restrict__ counts,
+                                                               int tiles) {
+    __shared__ unsigned hist[kRadix];
+    for (int d = threadIdx.x; d < kRadix; d += kSortThreads) hist[d] = 0u;
+    __syncthreads();
+    const int base = blockIdx.x * kSortTile;
+#pragma unroll
+    for (int it = 0; it < kSortItems; ++it) {
+        const int idx = base + it * kSortThreads + threadIdx.x;
+        if (idx < n) atomicAdd(&hist[(keys[idx] >> shift) & mask], 1u);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < kRadix; d += kSortThreads) counts[(size_t)d * tiles + blockIdx.x] = hist[d];
+}
+
+__global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* __restrict__ keys_in,
+                                                                const int32_t* __restrict__ vals_in,
+                                                                uint32_t* __restrict__ keys_out,
+                                                                int32_t* __restrict__ vals_out, int n, int shift,
+                                                                unsigned mask, const unsigned* __restrict__ offsets,
+                                                                int tiles) {
+    __shared__ unsigned warp_cnt[kWarps][kRadix];
+    __shared__ unsigned local_start[kRadix];
+    __shared__ unsigned scan_tmp[33];
+    __shared__ uint32_t skeys[kSortTile];
+    __shared__ int32_t svals[kSortTile];
+
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortThreads) (&warp_cnt[0][0])[i] = 0u;
+    __syncthreads();
+
+    const int tile0 = blockIdx.x * kSortTile;
+    const unsigned lt = lanemask_lt();
+    uint32_t k[kSortItems];
+    int32_t v[kSortItems];
+    unsigned rank[kSortItems];
+    // Each warp owns a contiguous run of 32*kSortItems inputs, visited in order.
+#pragma unroll
+    for (int it = 0; it < kSortItems; ++it) {
+        const int idx = tile0 + w * 32 * kSortItems + it * 32 + lane;
+        const bool valid = idx < n;
+        k[it] = valid ? keys_in[idx] : 0u;
+        v[it] = valid ? (vals_in ? vals_in[idx] : idx) : 0;
+        const unsigned d = (k[it] >> shift) & mask;
+        const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+        unsigned before = 0u, peers = 0u;
+        if (valid) {
+            peers = __match_any_sync(vmask, d);
+            before = warp_cnt[w][d];
+        }
+        __syncwarp();
+        if (valid) {
+            rank[it] = before + __popc(peers & lt);
+            if ((peers & lt) == 0u) warp_cnt[w][d] = before + __popc(peers);
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // Per digit: exclusive scan over warps, then the block-local digit starts.
+    unsigned dtotal = 0u;
+    for (int d = threadIdx.x; d < kRadix; d += kSortThreads) {
+        unsigned run = 0u;
+#pragma unroll
+        for (int ww = 0; ww < kWarps; ++ww) {
+            const unsigned c = warp_cnt[ww][d];
+            warp_cnt[ww][d] = run;
+            run += c;
+        }
+        dtotal = run;
+    }
+    __syncthreads();
+    {
+        unsigned tot;
+        const unsigned ex = block_exclusive(threadIdx.x < kRadix ? dtotal : 0u, scan_tmp, &tot);
+        if (threadIdx.x < kRadix) local_start[threadIdx.x] = ex;
+    }
+    __syncthreads();
+
+#pragma unroll
+    for (int it = 0; it < kSortItems; ++it) {
+        const int idx = tile0 + w * 32 * kSortItems + it * 32 + lane;
+        if (idx < n) {
+            const unsigned d = (k[it] >> shift) & mask;
+            const unsigned lp = local_start[d] + warp_cnt[w][d] + rank[it];
+            skeys[lp] = k[it];
+            svals[lp] = v[it];
+        }
+    }
+    __syncthreads();
+
+    const int count = min(kSortTile, n - tile0);
+    for (int i = threadIdx.x; i < count; i += kSortThreads) {
+        const uint32_t key = skeys[i];
+        const unsigned d = (key >> shift) & mask;
+        const unsigned dst = offsets[(size_t)d * tiles + blockIdx.x] + ((unsigned)i - local_start[d]);
+        keys_out[dst] = key;
+        vals_out[dst] = svals[i];
+    }
+}
+
+// Exclusive scan of a uint32 array in place: tile sums, scan of sums, rescan.
+__global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(const unsigned* __restrict__ a, size_t m,
+                                                                 unsigned* __restrict__ sums) {
+    __shared__ unsigned tmp[33];
+    const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+    unsigned s = 0u;
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j)
+        if (base + j < m) s += a[base + j];
+    unsigned tot;
+    block_exclusive(s, tmp, &tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_sums(unsigned* __restrict__ sums, int m) {
+    __shared__ unsigned warp_tot[32];
+    __shared__ unsigned carry;
+    if (threadIdx.x == 0) carry = 0u;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int base = 0; base < m; base += 1024) {
+        const int i = base + threadIdx.x;
+        const unsigned v = (i < m) ? sums[i] : 0u;
+        const unsigned inc = warp_inclusive(v);
+        if (lane == 31) warp_tot[w] = inc;
+        __syncthreads();
+        if (w == 0) {
+            const unsigned t = warp_tot[lane];
+            const unsigned ti = warp_inclusive(t);
+            warp_tot[lane] = ti - t;
+        }
+        __syncthreads();
+        const unsigned ex = carry + warp_tot[w] + inc - v;
+        if (i < m) sums[i] = ex;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = ex + v;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(unsigned* __restrict__ a, size_t m,
+                                                             const unsigned* __restrict__ sums) {
+    __shared__ unsigned tmp[33];
+    const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+    unsigned x[kScanItems];
+    unsigned s = 0u;
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        x[j] = (base + j < m) ? a[base + j] : 0u;
+        s += x[j];
+    }
+    unsigned run = block_exclusive(s, tmp, nullptr) + sums[blockIdx.x];
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        if (base + j < m) a[base + j] = run;
+        run += x[j];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_reorder(const float4* __restrict__ pos_in, const float4* __restrict__ vel_in,
+                                                 const int32_t* __restrict__ perm, float4* __restrict__ pos_out,
+                                                 float4* __restrict__ vel_out, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int j = perm[i];
+    pos_out[i] = pos_in[j];
+    vel_out[i] = vel_in[j];
+}
+
+__global__ void k_copy_keys(const uint32_t* __restrict__ kin, const int32_t* __restrict__ vin,
+                            uint32_t* __restrict__ kout, int32_t* __restrict__ vout, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    kout[i] = kin[i];
+    vout[i] = vin ? vin[i] : i;
+}
+
+}  // namespace
+
+int launch_cell_keys(const float4* pos, int n, int G, int order, uint32_t* keys, cudaStream_t s) {
+    if (n <= 0) return SD_OK;
+    k_cell_keys<<<(n + 255) / 256, 256, 0, s>>>(pos, n, G, order, keys);
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
+
+static int scan_tiles_for(size_t m) { return (int)((m + kScanTile - 1) / kScanTile); }
+
+size_t sort_workspace_bytes(int n) {
+    const int tiles = (n + kSortTile - 1) / kSortTile;
+    const size_t m = (size_t)kRadix * (size_t)(tiles > 0 ? tiles : 1);
+    return align_up(m * sizeof(unsigned), 256) + align_up((size_t)scan_tiles_for(m) * sizeof(unsigned), 256);
+}
+
+// Exclusive scan of counts[m] in place, with sums[] from the workspace.
+static int scan_exclusive(unsigned* a, size_t m, unsigned* sums, cudaStream_t s) {
+    const int nt = scan_tiles_for(m);
+    k_scan_tile_sums<<<nt, kScanThreads, 0, s>>>(a, m, sums);
+    SD_LAUNCHED(s);
+    k_scan_sums<<<1, 1024, 0, s>>>(sums, nt);
+    SD_LAUNCHED(s);
+    k_scan_apply<<<nt, kScanThreads, 0, s>>>(a, m, sums);
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
+
+int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t* keys_out, int32_t* vals_out,
+                      uint32_t* keys_tmp, int32_t* vals_tmp, int n, int key_bits, void* ws, size_t ws_bytes,
+                      cudaStream_t s) {
+    if (n < 0 || key_bits < 0 || key_bits > 32) return fail(SD_E_ARG, "sort: bad n=%d or key_bits=%d", n, key_bits);
+    if (n == 0) return SD_OK;
+    if (!keys_in || !keys_out || !vals_out || !keys_tmp || !vals_tmp || !ws)
+        return fail(SD_E_ARG, "sort: null buffer");
+    if (ws_bytes < sort_workspace_bytes(n)) return fail(SD_E_ARG, "sort: workspace too small");
+    if (keys_in == keys_out || (vals_in && vals_in == vals_out))
+        return fail(SD_E_ARG, "sort: input and output buffers must differ");
+    const int passes = (key_bits + kRadixBits - 1) / kRadixBits;
+    if (passes == 0) {
+        k_copy_keys<<<(n + 255) / 256, 256, 0, s>>>(keys_in, vals_in, keys_out, vals_out, n);
+        SD_LAUNCHED(s);
+        return SD_OK;
+    }
+    const int tiles = (n + kSortTile - 1) / kSortTile;
+    const size_t m = (size_t)kRadix * tiles;
+    unsigned* counts = (unsigned*)ws;
+    unsigned* sums = (unsigned*)((char*)ws + align_up(m * sizeof(unsigned), 256));
+
+    const uint32_t* kin = keys_in;
+    const int32_t* vin = vals_in;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = p * kRadixBits;
+        const int bits = (key_bits - shift) < kRadixBits ? (key_bits - shift) : kRadixBits;
+        const unsigned mask = (1u << bits) - 1u;
+        // the last pass lands in *_out; earlier passes alternate so that holds
+        const bool to_out = ((passes - 1 - p) % 2) == 0;
+        uint32_t* kout = to_out ? keys_out : keys_tmp;
+        int32_t* vout = to_out ? vals_out : vals_tmp;
+        k_digit_counts<<<tiles, kSortThreads, 0, s>>>(kin, n, shift, mask, counts, tiles);
+        SD_LAUNCHED(s);
+        int rc = scan_exclusive(counts, m, sums, s);
+        if (rc != SD_OK) return rc;
+        k_digit_scatter<<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, mask, counts, tiles);
+        SD_LAUNCHED(s);
+        kin = kout;
+        vin = vout;
+    }
+    return SD_OK;
+}
+
+int launch_reorder(const float4* pos_in, const float4* vel_in, const int32_t* perm, float4* pos_out,
+                   float4* vel_out, int n, cudaStream_t s) {
+    if (n <= 0) return SD_OK;
+    k_reorder<<<(n + 255) / 256, 256, 0, s>>>(pos_in, vel_in, perm, pos_out, vel_out, n);
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
+
+}  // namespace sd

@@ -1,0 +1,251 @@
+"""Python mirror of the reference's ``Sim`` class over the C ABI.
+
+Method names follow the reference (src/sim/Sim.h:854-1135), in snake_case:
+``init``, ``reconfigure``, ``reset``, ``step``, ``timings``, ``sim_time``,
+``grid_size``, ``particle_count``, ``active_count``, ``save_state``,
+``load_state``, ``measure_total_grid_mass`` ... plus ``step(dt)`` with an explicit
+time step and ``set_particles`` / ``get_particles`` for scene init. Errors raise
+``SdError`` carrying the library's status code and first-failure message (the
+reference's sticky ``Sim::failed()`` / ``failMessage()``, Sim.cu:52-75).
+
+Particle arrays are float32 ``(n, 4)``: host numpy arrays, or CUDA torch tensors
+(passed by device pointer, no host copy).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import asdict, dataclass, fields
+
+import numpy as np
+
+from . import _lib as L
+
+
+@dataclass
+class SimConfig:
+    """Plain-PM fields of the reference's SimConfig (Sim.h:157-796)."""
+
+    particle_count: int = 2_000_000      # Sim.h:166
+    grid_size: int = 128                 # Sim.h:167
+    boundary: int = L.SD_BOUNDARY_PERIODIC
+    gravity: float = 1.0                 # Sim.h:280
+    softening_cells: float = 3.0         # Sim.h:315
+    time_scale: float = 1.0              # Sim.h:316
+    sort_interval: int = 1               # Sim.h:317
+    length_scale: float = 1.0            # Sim.h:172
+    time_unit_scale: float = 1.0         # Sim.h:180
+    order: int = L.SD_ORDER_ROWMAJOR
+    integrator: int = L.SD_INT_KD
+    units: int = L.SD_UNITS_REFERENCE
+    diagnostics: int = 0
+    keep_density: int = 1
+
+    def to_c(self) -> L.SdConfig:
+        c = L.SdConfig()
+        for f in fields(self):
+            setattr(c, f.name, getattr(self, f.name))
+        return c
+
+    @classmethod
+    def from_c(cls, c: L.SdConfig) -> "SimConfig":
+        return cls(**{f.name: getattr(c, f.name) for f in fields(cls)})
+
+    def as_dict(self) -> dict:
+        return asdict(self)
+
+
+def _is_torch_cuda(a) -> bool:
+    return hasattr(a, "is_cuda") and bool(a.is_cuda)
+
+
+def _host_f4(a) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if a.ndim != 2 or a.shape[1] != 4:
+        raise ValueError("particle arrays must be float32 of shape (n, 4)")
+    return a
+
+
+class Sim:
+    """One PM simulation on one GPU (the reference's Sim, Sim.h:854)."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        L.check(L.lib().sd_create(ctypes.byref(self._h), device), "sd_create")
+        self.device = device
+
+    # ---- lifetime ------------------------------------------------------------
+    def close(self) -> None:
+        if self._h:
+            L.lib().sd_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    # ---- static queries --------------------------------------------------------
+    @staticmethod
+    def device_available() -> bool:
+        return bool(L.lib().sd_device_available())
+
+    @staticmethod
+    def failed() -> bool:
+        return bool(L.lib().sd_failed())
+
+    @staticmethod
+    def fail_message() -> str:
+        return L.last_error()
+
+    @staticmethod
+    def max_grid_size(boundary: int = L.SD_BOUNDARY_PERIODIC) -> int:
+        return int(L.lib().sd_max_grid_size(boundary))
+
+    @staticmethod
+    def estimate_bytes(particle_count: int, grid_size: int, boundary: int = L.SD_BOUNDARY_PERIODIC) -> int:
+        return int(L.lib().sd_estimate_bytes(particle_count, grid_size, boundary))
+
+    # ---- configuration -----------------------------------------------------------
+    def init(self, cfg: SimConfig) -> None:
+        c = cfg.to_c()
+        L.check(L.lib().sd_init(self._h, ctypes.byref(c)), "sd_init")
+
+    def reconfigure(self, cfg: SimConfig) -> None:
+        c = cfg.to_c()
+        L.check(L.lib().sd_reconfigure(self._h, ctypes.byref(c)), "sd_reconfigure")
+
+    def reset(self) -> None:
+        L.check(L.lib().sd_reset(self._h), "sd_reset")
+
+    def config(self) -> SimConfig:
+        c = L.SdConfig()
+        L.check(L.lib().sd_get_config(self._h, ctypes.byref(c)), "sd_get_config")
+        return SimConfig.from_c(c)
+
+    # ---- particles --------------------------------------------------------------
+    def set_particles(self, pos, vel) -> None:
+        if _is_torch_cuda(pos):
+            n = int(pos.shape[0])
+            L.check(L.lib().sd_set_particles(self._h, pos.data_ptr(), vel.data_ptr(), n, L.SD_DEVICE),
+                    "sd_set_particles")
+            return
+        p, v = _host_f4(pos), _host_f4(vel)
+        L.check(L.lib().sd_set_particles(self._h, p.ctypes.data, v.ctypes.data, len(p), L.SD_HOST),
+                "sd_set_particles")
+
+    def get_particles(self, n: int | None = None):
+        n = self.particle_count() if n is None else n
+        p = np.empty((n, 4), np.float32)
+        v = np.empty((n, 4), np.float32)
+        L.check(L.lib().sd_get_particles(self._h, p.ctypes.data, v.ctypes.data, n, L.SD_HOST), "sd_get_particles")
+        return p, v
+
+    def get_particles_into(self, pos_t, vel_t) -> None:
+        """Copy into CUDA torch tensors (device to device)."""
+        n = int(pos_t.shape[0])
+        L.check(L.lib().sd_get_particles(self._h, pos_t.data_ptr(), vel_t.data_ptr(), n, L.SD_DEVICE),
+                "sd_get_particles")
+
+    def particle_pos_device_ptr(self) -> int:
+        return int(L.lib().sd_particle_pos_device_ptr(self._h) or 0)
+
+    def particle_vel_device_ptr(self) -> int:
+        return int(L.lib().sd_particle_vel_device_ptr(self._h) or 0)
+
+    def density_device_ptr(self) -> int:
+        return int(L.lib().sd_density_device_ptr(self._h) or 0)
+
+    def density(self) -> np.ndarray:
+        G = self.grid_size()
+        out = np.empty((G, G, G), np.float32)
+        L.check(L.lib().sd_get_density(self._h, out.ctypes.data, L.SD_HOST), "sd_get_density")
+        return out
+
+    def potential(self) -> np.ndarray:
+        G = self.grid_size()
+        out = np.empty((G, G, G), np.float32)
+        L.check(L.lib().sd_get_potential(self._h, out.ctypes.data, L.SD_HOST), "sd_get_potential")
+        return out
+
+    def accel(self, n: int | None = None) -> np.ndarray:
+        n = self.particle_count() if n is None else n
+        out = np.empty((n, 4), np.float32)
+        L.check(L.lib().sd_get_accel(self._h, out.ctypes.data, n, L.SD_HOST), "sd_get_accel")
+        return out
+
+    # ---- stepping -----------------------------------------------------------------
+    def step(self, dt: float | None = None) -> None:
+        """``step()`` is the reference's CFL-clamped step; ``step(dt)`` advances by dt."""
+        if dt is None:
+            L.check(L.lib().sd_step_auto(self._h), "sd_step_auto")
+        else:
+            L.check(L.lib().sd_step(self._h, float(dt)), "sd_step")
+
+    def steps(self, dt: float, n: int) -> None:
+        L.check(L.lib().sd_steps(self._h, float(dt), int(n)), "sd_steps")
+
+    def synchronize(self) -> None:
+        L.check(L.lib().sd_synchronize(self._h), "sd_synchronize")
+
+    def sort_only(self) -> np.ndarray:
+        perm = np.empty(self.particle_count(), np.int32)
+        L.check(L.lib().sd_sort_only(self._h, perm.ctypes.data, L.SD_HOST), "sd_sort_only")
+        return perm
+
+    # ---- state ----------------------------------------------------------------------
+    def save_state(self, path: str) -> None:
+        L.check(L.lib().sd_save_state(self._h, str(path).encode()), "sd_save_state")
+
+    def load_state(self, path: str) -> None:
+        L.check(L.lib().sd_load_state(self._h, str(path).encode()), "sd_load_state")
+
+    # ---- queries -----------------------------------------------------------------------
+    def timings(self) -> dict:
+        t = L.SdTimings()
+        L.check(L.lib().sd_timings_get(self._h, ctypes.byref(t)), "sd_timings_get")
+        return {f[0]: getattr(t, f[0]) for f in L.SdTimings._fields_}
+
+    def sim_time(self) -> float:
+        return float(L.lib().sd_sim_time(self._h))
+
+    def grid_size(self) -> int:
+        return int(L.lib().sd_grid_size(self._h))
+
+    def particle_count(self) -> int:
+        return int(L.lib().sd_particle_count(self._h))
+
+    def active_count(self) -> int:
+        return int(L.lib().sd_active_count(self._h))
+
+    def step_count(self) -> int:
+        return int(L.lib().sd_step_count(self._h))
+
+    def measure_total_grid_mass(self) -> float:
+        return float(L.lib().sd_measure_total_grid_mass(self._h))
+
+    def measure_max_density(self) -> float:
+        return float(L.lib().sd_measure_max_density(self._h))
+
+    def measure_kinetic_energy(self) -> float:
+        return float(L.lib().sd_measure_kinetic_energy(self._h))
+
+    def diagnostics(self) -> dict:
+        d = L.SdDiagnostics()
+        L.check(L.lib().sd_diagnostics_get(self._h, ctypes.byref(d)), "sd_diagnostics_get")
+        return {"kinetic": d.kinetic, "potential": d.potential, "momentum": list(d.momentum),
+                "mean_velocity_removed": list(d.mean_velocity_removed), "live_count": d.live_count}
+
+    @staticmethod
+    def kernel_launches() -> int:
+        return int(L.lib().sd_kernel_launches(None))

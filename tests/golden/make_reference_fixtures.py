@@ -1,0 +1,105 @@
+"""Generate golden fixtures by running the unmodified reference on a GPU.
+
+Usage (on a machine with a CUDA GPU and the prebuilt oracle/_ref/libsimref.so):
+    python tests/golden/make_reference_fixtures.py OUTDIR
+
+For each case it writes ``reference_<name>.npz`` holding the seeded input
+particles, the reference's density after Sim::loadState (deposit of the loaded
+positions), and the particles after one Sim::step() (sort + deposit + cuFFT
+Poisson + gradient + kick/drift + momentum zeroing). Velocities carry a particle
+id in ``w`` (the reference copies w through the sort and the integrator), so the
+reference's sort permutation can be read back. The cases are small so the
+committed files stay small.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from stardust_b200 import scenes  # noqa: E402
+
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libsimref.so")
+
+
+def load_ref():
+    L = ctypes.CDLL(REF_LIB)
+    P, I, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    L.ref_create.restype = P
+    L.ref_destroy.argtypes = [P]
+    L.ref_load.argtypes = [P, P, P, I, I, F, F, F, I, ctypes.c_char_p]
+    L.ref_step.argtypes = [P]
+    L.ref_steps.argtypes = [P, I]
+    L.ref_get.argtypes = [P, P, P, I]
+    L.ref_density.argtypes = [P, P, I]
+    L.ref_timings.argtypes = [P, P]
+    L.ref_fail_message.restype = ctypes.c_char_p
+    L.ref_sim_time.argtypes = [P]
+    L.ref_sim_time.restype = ctypes.c_double
+    return L
+
+
+def run_case(L, pos, vel, G, gravity, soft, dt, tmpdir):
+    n = len(pos)
+    h = L.ref_create()
+    try:
+        path = os.path.join(tmpdir, "in.stardust").encode()
+        # timeScale = dt / 0.0016 gives dt = 0.0016 * dtScaleFor(timeScale) (Sim.h:89-93)
+        ts = np.float32(dt) / np.float32(0.0016)
+        rc = L.ref_load(h, pos.ctypes.data, vel.ctypes.data, n, G, gravity, soft, float(ts), 1, path)
+        if rc != 0:
+            raise RuntimeError(f"ref_load failed: {rc} {L.ref_fail_message()}")
+        rho = np.empty(G ** 3, np.float32)
+        L.ref_density(h, rho.ctypes.data, G)
+        rc = L.ref_step(h)
+        if rc != 0:
+            raise RuntimeError(f"ref_step failed: {L.ref_fail_message()}")
+        p1 = np.empty_like(pos)
+        v1 = np.empty_like(vel)
+        L.ref_get(h, p1.ctypes.data, v1.ctypes.data, n)
+        t = np.empty(6, np.float32)
+        L.ref_timings(h, t.ctypes.data)
+        return rho.reshape(G, G, G), p1, v1, float(t[4])
+    finally:
+        L.ref_destroy(h)
+
+
+def cases():
+    rng = np.random.default_rng(20240)
+    n = 4096
+    c = rng.random((6, 3))
+    xyz = (c[rng.integers(0, 6, n)] + rng.normal(scale=0.05, size=(n, 3))) % 1.0
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = xyz
+    pos[:, :3][pos[:, :3] >= 1.0] = 0.0
+    vel = np.zeros((n, 4), np.float32)
+    vel[:, :3] = rng.normal(scale=0.2, size=(n, 3))
+    yield "clustered_g16", pos, vel, 16, float(4 * np.pi * 16 ** 3), 1.0, 1e-3
+    p, v = scenes.disk_galaxy(8192, 7)
+    yield "disk_g32", p, v, 32, float(4 * np.pi * 32 ** 3), 1.0, 1e-3
+
+
+def main(outdir: str) -> int:
+    os.makedirs(outdir, exist_ok=True)
+    L = load_ref()
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, pos, vel, G, grav, soft, dt in cases():
+            pos = np.ascontiguousarray(pos, np.float32)
+            vel = np.ascontiguousarray(vel, np.float32)
+            vel[:, 3] = np.arange(len(vel), dtype=np.float32)  # id through the reference's sort
+            rho, p1, v1, dt_used = run_case(L, pos, vel, G, grav, soft, dt, tmp)
+            np.savez_compressed(os.path.join(outdir, f"reference_{name}.npz"), pos_in=pos, vel_in=vel,
+                                rho_loaded=rho, pos_out=p1, vel_out=v1, grid=G, gravity=grav, soft=soft,
+                                dt=np.float32(dt_used))
+            print(name, "dt_used", dt_used, "mass", float(rho.sum()))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden")))

@@ -1,0 +1,196 @@
+"""Whole-step parity and behaviour of the simulation handle (through the C ABI)."""
+import numpy as np
+import pytest
+
+from conftest import random_particles
+from stardust_b200 import _lib as L
+from stardust_b200 import scenes
+from stardust_b200.sim import Sim, SimConfig
+
+pytestmark = pytest.mark.gpu
+
+# one step from identical inputs: relative RMS of the velocity change and the
+# absolute position difference (box units) allowed against the oracle
+DV_RTOL = 1e-4
+DP_ATOL = 2e-6
+
+
+def make_sim(cuda, n, G, **kw):
+    cfg = SimConfig(particle_count=n, grid_size=G, **kw)
+    s = Sim(0)
+    s.init(cfg)
+    return s
+
+
+def rel_rms(a, b):
+    d = np.sqrt(np.mean(np.sum((a.astype(np.float64) - b) ** 2, axis=-1)))
+    r = np.sqrt(np.mean(np.sum(b.astype(np.float64) ** 2, axis=-1)))
+    return d / r
+
+
+def wrapdiff(a, b):
+    return (a - b + 0.5) % 1.0 - 0.5
+
+
+@pytest.mark.parametrize("order", [L.SD_ORDER_ROWMAJOR, L.SD_ORDER_MORTON, L.SD_ORDER_TILED])
+def test_one_step_matches_oracle(cuda, oracle, order):
+    G, n = 64, 262_144
+    pos, vel = scenes.disk_galaxy(n, 0)
+    vel[:, 3] = np.arange(n, dtype=np.float32)
+    grav = float(4 * np.pi * G ** 3)  # Newton G = 1 in the reference's formula
+    dt = 1e-3
+    with make_sim(cuda, n, G, gravity=grav, softening_cells=1.0, order=order) as s:
+        s.set_particles(pos, vel)
+        rho0 = s.density()  # density of the loaded positions
+        s.step(dt)
+        p1, v1 = s.get_particles()
+        rho1 = s.density()
+    ref_rho = oracle.density_fixed(pos, G)
+    assert np.array_equal(rho0.view(np.int32), ref_rho.view(np.int32))
+    assert np.array_equal(rho1.view(np.int32), ref_rho.view(np.int32))  # sort does not move particles
+    p_ref, v_ref, _, _ = oracle.step(pos, vel, G, grav, 1.0, dt, dt, key_mode=order)
+    ids, ids_ref = v1[:, 3].astype(np.int64), v_ref[:, 3].astype(np.int64)
+    assert np.array_equal(ids, ids_ref)  # identical sort permutation
+    dv = v1[:, :3] - vel[ids, :3]
+    dv_ref = v_ref[:, :3] - vel[ids_ref, :3]
+    assert rel_rms(dv, dv_ref) < DV_RTOL
+    assert np.abs(wrapdiff(p1[:, :3], p_ref[:, :3])).max() < DP_ATOL
+
+
+def test_multi_step_determinism_and_graph_replay(cuda):
+    G, n = 64, 200_000
+    pos, vel = random_particles(n, 1, empty_every=101, clustered=True)
+    outs = []
+    for mode in ("eager", "eager", "graph"):
+        with make_sim(cuda, n, G, gravity=100.0, softening_cells=1.0) as s:
+            s.set_particles(pos, vel)
+            if mode == "graph":
+                s.steps(1e-3, 7)
+            else:
+                for _ in range(7):
+                    s.step(1e-3)
+            outs.append(s.get_particles())
+            assert s.step_count() == 7
+            assert s.sim_time() == pytest.approx(7e-3)
+    for p, v in outs[1:]:
+        assert np.array_equal(p.view(np.int32), outs[0][0].view(np.int32))
+        assert np.array_equal(v.view(np.int32), outs[0][1].view(np.int32))
+
+
+def test_mass_conservation_and_momentum_zeroing(cuda):
+    # reference invariant: mass conservation over 50 steps, rel < 1e-3 (tests/sim_tests.cpp:31-52)
+    G, n = 64, 100_000
+    pos, vel = random_particles(n, 3, clustered=True)
+    with make_sim(cuda, n, G, gravity=500.0) as s:
+        s.set_particles(pos, vel)
+        m0 = s.measure_total_grid_mass()
+        for _ in range(50):
+            s.step(1e-3)
+        m1 = s.measure_total_grid_mass()
+        p, v = s.get_particles()
+    assert m0 == pytest.approx(n, rel=1e-6)
+    assert abs(m1 - m0) / m0 < 1e-3
+    assert np.abs(v[:, :3].astype(np.float64).mean(axis=0)).max() < 1e-6
+    assert ((p[:, :3] >= 0) & (p[:, :3] < 1)).all()
+
+
+def test_clumping_increases_with_gravity(cuda):
+    # reference invariant (tests/sim_tests.cpp:58-82): stronger gravity -> denser peaks
+    G, n = 32, 50_000
+    pos, vel = random_particles(n, 4)
+    vel[:, :3] = 0
+    peaks = []
+    for grav in (0.0, 5e4):
+        with make_sim(cuda, n, G, gravity=grav, softening_cells=0.5) as s:
+            s.set_particles(pos, vel)
+            for _ in range(60):
+                s.step(5e-3)
+            s.step(1e-6)
+            peaks.append(s.measure_max_density())
+    assert peaks[1] > 1.5 * peaks[0]
+
+
+def test_step_auto_uses_reference_cfl(cuda, oracle):
+    G, n = 32, 20_000
+    pos, vel = random_particles(n, 5)
+    vel[7, :3] = (20.0, 0.0, 0.0)  # fast particle: CFL must clamp
+    with make_sim(cuda, n, G, gravity=1.0, time_scale=1.0) as s:
+        s.set_particles(pos, vel)
+        s.step()
+        t = s.timings()
+    vmax = oracle.max_speed(pos, vel)
+    expect = min(np.float32(0.0016), np.float32(0.8) * np.float32(1.0 / G) / np.float32(vmax))
+    assert t["max_speed"] == pytest.approx(vmax, rel=1e-6)
+    assert t["dt_used"] == pytest.approx(float(expect), rel=1e-6)
+
+
+def test_save_load_round_trip(cuda, tmp_path):
+    G, n = 32, 30_000
+    pos, vel = random_particles(n, 6, empty_every=9)
+    path = tmp_path / "state.bin"
+    with make_sim(cuda, n, G, gravity=50.0) as s:
+        s.set_particles(pos, vel)
+        for _ in range(3):
+            s.step(1e-3)
+        s.save_state(str(path))
+        p_a, v_a = s.get_particles()
+        for _ in range(2):
+            s.step(1e-3)
+        p_b, v_b = s.get_particles()
+    raw = open(path, "rb").read()
+    assert raw[:8] == b"STARDUST" and len(raw) == 76 + 32 * n
+    with make_sim(cuda, 10, 16) as s2:
+        s2.load_state(str(path))
+        assert s2.particle_count() == n and s2.grid_size() == G
+        p_l, v_l = s2.get_particles()
+        assert np.array_equal(p_l, p_a) and np.array_equal(v_l, v_a)
+        assert s2.sim_time() == pytest.approx(3e-3, rel=1e-6)
+        for _ in range(2):
+            s2.step(1e-3)
+        p_c, v_c = s2.get_particles()
+    assert np.array_equal(p_c.view(np.int32), p_b.view(np.int32))
+    assert np.array_equal(v_c.view(np.int32), v_b.view(np.int32))
+
+
+def test_leapfrog_energy_conservation_better_than_kd(cuda):
+    G, n = 32, 40_000
+    pos, vel = scenes.zeldovich(32, 9)
+    n = len(pos)
+    drift = {}
+    for integ in (L.SD_INT_KD, L.SD_INT_KDK):
+        with make_sim(cuda, n, G, gravity=1.0, units=L.SD_UNITS_NEWTON, integrator=integ, softening_cells=1.0,
+                      diagnostics=0) as s:
+            s.set_particles(pos, vel)
+            s.accel()  # field of the current positions for the potential energy
+            d0 = s.diagnostics()
+            for _ in range(40):
+                s.step(2e-3)
+            s.synchronize()
+            s.accel()
+            d1 = s.diagnostics()
+        e0 = d0["kinetic"] + d0["potential"]
+        e1 = d1["kinetic"] + d1["potential"]
+        drift[integ] = abs(e1 - e0) / abs(d0["potential"])
+    assert drift[L.SD_INT_KDK] < drift[L.SD_INT_KD]
+
+
+def test_accel_matches_fp64_pm(cuda, oracle):
+    """Force error of the float pipeline against the FP64 PM oracle on the same grid."""
+    G, n = 64, 100_000
+    pos, vel = random_particles(n, 10, clustered=True)
+    with make_sim(cuda, n, G, gravity=1.0, units=L.SD_UNITS_NEWTON, softening_cells=1.0) as s:
+        s.set_particles(pos, vel)
+        a = s.accel()[:, :3]
+    a64 = oracle.pm_accel_f64(pos, G, 4 * np.pi * G ** 3 / n, 1.0)
+    err = oracle.force_error(a, a64)
+    assert err["rms_rel"] < 1e-5, err
+    assert err["max_rel"] < 1e-3, err
+
+
+def test_kernel_launches_counted(cuda):
+    with make_sim(cuda, 1000, 16) as s:
+        pos, vel = random_particles(1000, 2)
+        s.set_particles(pos, vel)
+        before = Sim.kernel_launches()
+        s.step(1e-3)
+        assert Sim.kernel_launches() - before >= 10
