@@ -145,7 +145,7 @@ def zeldovich(n_side: int = 256, seed: int = 2, rms_cells: float = 0.5, G: float
     psi = np.empty((n, n, n, 3), np.float32)
     for j, kk in enumerate((kx, ky, kz)):
         comp = (1j * (kk / k2) * delta).astype(np.complex64)
-        psi[..., j] = np.fft.irfftn(comp, s=(n, n, n)).astype(np.float32)
+        psi[..., j] = np.fft.irfftn(comp, s=(n, n, n), axes=(0, 1, 2)).astype(np.float32)
         del comp
     del delta
     rms = float(np.sqrt(np.mean(np.sum(psi.astype(np.float64) ** 2, axis=-1))))

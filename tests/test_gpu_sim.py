@@ -100,8 +100,9 @@ def test_clumping_increases_with_gravity(cuda):
     pos, vel = random_particles(n, 4)
     vel[:, :3] = 0
     peaks = []
-    for grav in (0.0, 5e4):
-        with make_sim(cuda, n, G, gravity=grav, softening_cells=0.5) as s:
+    # Newton G = 0 and G = 10 (growth rate sqrt(4 pi G rho) ~ 11 per unit time)
+    for grav in (0.0, 10.0):
+        with make_sim(cuda, n, G, gravity=grav, units=L.SD_UNITS_NEWTON, softening_cells=0.5) as s:
             s.set_particles(pos, vel)
             for _ in range(60):
                 s.step(5e-3)

@@ -18,6 +18,8 @@ POISSON_RTOL = 2e-5
 
 
 def dev(torch, a):
+    """Upload to the GPU. Callers keep the returned tensor alive while a kernel
+    uses its pointer (a dropped temporary goes back to torch's allocator)."""
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
@@ -45,7 +47,8 @@ def test_cell_keys_bit_exact(cuda, lib, oracle, order, G):
     pos, _ = random_particles(100_003, G + order, empty_every=17, clustered=True)
     pos = np.concatenate([pos, edge_positions()])
     keys = cuda.empty(len(pos), dtype=cuda.int32, device="cuda")
-    L.check(lib.sd_cell_keys(dev(cuda, pos).data_ptr(), len(pos), G, order, keys.data_ptr(), None), "keys")
+    pd = dev(cuda, pos)
+    L.check(lib.sd_cell_keys(pd.data_ptr(), len(pos), G, order, keys.data_ptr(), None), "keys")
     sync(cuda)
     ref = oracle.cell_keys(pos, G, order).astype(np.int64) + 1
     assert np.array_equal(keys.cpu().numpy().view(np.uint32).astype(np.int64), ref)
@@ -119,8 +122,8 @@ def test_deposit_bit_exact(cuda, lib, oracle, G, n, clustered):
     pos = np.concatenate([pos, edge_positions()])
     rho = cuda.empty(G ** 3, dtype=cuda.float32, device="cuda")
     w = ws(cuda, lib.sd_deposit_workspace_bytes(G))
-    L.check(lib.sd_deposit(dev(cuda, pos).data_ptr(), len(pos), G, rho.data_ptr(), w.data_ptr(), w.numel(), None),
-            "deposit")
+    pd = dev(cuda, pos)
+    L.check(lib.sd_deposit(pd.data_ptr(), len(pos), G, rho.data_ptr(), w.data_ptr(), w.numel(), None), "deposit")
     sync(cuda)
     got = rho.cpu().numpy().reshape(G, G, G)
     ref = oracle.density_fixed(pos, G)
@@ -136,8 +139,8 @@ def test_deposit_deterministic_across_runs_and_orders(cuda, lib):
     for p in (pos, pos, pos[perm]):
         rho = cuda.empty(G ** 3, dtype=cuda.float32, device="cuda")
         w = ws(cuda, lib.sd_deposit_workspace_bytes(G))
-        L.check(lib.sd_deposit(dev(cuda, p).data_ptr(), len(p), G, rho.data_ptr(), w.data_ptr(), w.numel(), None),
-                "deposit")
+        pd = dev(cuda, p)
+        L.check(lib.sd_deposit(pd.data_ptr(), len(p), G, rho.data_ptr(), w.data_ptr(), w.numel(), None), "deposit")
         outs.append(rho.cpu().numpy())
     assert np.array_equal(outs[0].view(np.int32), outs[1].view(np.int32))
     assert np.array_equal(outs[0].view(np.int32), outs[2].view(np.int32))
@@ -147,8 +150,9 @@ def gpu_poisson(cuda, lib, rho, soft):
     G = rho.shape[0]
     phi = cuda.empty(G ** 3, dtype=cuda.float32, device="cuda")
     w = ws(cuda, lib.sd_poisson_workspace_bytes(G))
-    L.check(lib.sd_poisson(dev(cuda, rho).data_ptr(), G, ctypes.c_float(soft), phi.data_ptr(), w.data_ptr(),
-                           w.numel(), None), "poisson")
+    rd = dev(cuda, rho)
+    L.check(lib.sd_poisson(rd.data_ptr(), G, ctypes.c_float(soft), phi.data_ptr(), w.data_ptr(), w.numel(), None),
+            "poisson")
     sync(cuda)
     return phi.cpu().numpy().reshape(G, G, G)
 
@@ -194,7 +198,8 @@ def test_gather_kick_drift_bit_exact(cuda, lib, oracle, G, n):
     pd, vd = dev(cuda, pos), dev(cuda, vel)
     mom = cuda.zeros(4, dtype=cuda.float64, device="cuda")
     w = ws(cuda, lib.sd_gather_workspace_bytes(n))
-    L.check(lib.sd_gather_kick_drift(dev(cuda, phi).data_ptr(), G, ctypes.c_float(pot_scale), pd.data_ptr(),
+    phid = dev(cuda, phi)
+    L.check(lib.sd_gather_kick_drift(phid.data_ptr(), G, ctypes.c_float(pot_scale), pd.data_ptr(),
                                      vd.data_ptr(), n, ctypes.c_float(dt), ctypes.c_float(dt),
                                      ctypes.c_float(1e4), None, mom.data_ptr(), w.data_ptr(), w.numel(), None),
             "gather")
@@ -216,8 +221,8 @@ def test_gather_light_speed_clamp_and_nan(cuda, lib, oracle):
     vel[1, :3] = (np.nan, 0.0, 0.0)     # NaN -> empty slot
     vel[2, :3] = (np.inf, 0.0, 0.0)
     phi = np.zeros((G, G, G), np.float32)
-    pd, vd = dev(cuda, pos), dev(cuda, vel)
-    L.check(lib.sd_gather_kick_drift(dev(cuda, phi).data_ptr(), G, ctypes.c_float(1.0), pd.data_ptr(),
+    pd, vd, phid = dev(cuda, pos), dev(cuda, vel), dev(cuda, phi)
+    L.check(lib.sd_gather_kick_drift(phid.data_ptr(), G, ctypes.c_float(1.0), pd.data_ptr(),
                                      vd.data_ptr(), len(pos), ctypes.c_float(1e-3), ctypes.c_float(1e-3),
                                      ctypes.c_float(1e4), None, None, None, 0, None), "gather")
     sync(cuda)
@@ -236,8 +241,9 @@ def test_interpolate_accel_matches_oracle_sample(cuda, lib, oracle):
     pos, vel = random_particles(50_000, 8)
     phi = gpu_poisson(cuda, lib, oracle.density_fixed(pos, G), 1.0)
     out = cuda.empty((len(pos), 4), dtype=cuda.float32, device="cuda")
-    L.check(lib.sd_interpolate_accel(dev(cuda, phi).data_ptr(), G, ctypes.c_float(0.5), dev(cuda, pos).data_ptr(),
-                                     out.data_ptr(), len(pos), None), "interp")
+    phid, pd = dev(cuda, phi), dev(cuda, pos)
+    L.check(lib.sd_interpolate_accel(phid.data_ptr(), G, ctypes.c_float(0.5), pd.data_ptr(), out.data_ptr(), len(pos),
+                                     None), "interp")
     sync(cuda)
     acc = oracle.grid_accel(phi, 0.5)
     # kick with dt=1 from zero velocity, no drift: v = a exactly (fma(a, 1, 0) = a)
