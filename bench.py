@@ -302,7 +302,7 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cosmic_web_512")
-    ap.add_argument("--order", type=int, default=0)
+    ap.add_argument("--order", type=int, default=2, help="0 row-major (reference), 1 Morton, 2 tiled (fused deposit)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)
 

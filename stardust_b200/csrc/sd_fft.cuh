@@ -1,29 +1,27 @@
-// sd_fft.cuh -- shared-memory Stockham FFT for many lines per CTA (sm_100a).
+// sd_fft.cuh -- shared-memory Stockham FFT over 16 interleaved lines (sm_100a).
 //
-// A CTA holds L lines of N complex values in shared memory and transforms all
-// of them at once. Stages are mixed radix (8, then 4 or 2 for the remainder),
-// in the self-sorting Stockham form: stage with radix R and sub-transform
-// length Ns reads in[j + r*N/R], multiplies by W_{Ns*R}^{(j mod Ns)*r}, does an
-// R-point DFT in registers and writes out[(j/Ns)*Ns*R + (j mod Ns) + r*Ns].
-// Output is in natural order. Each stage loads all its butterflies into
-// registers, synchronises and stores back in place, so one buffer suffices.
+// A CTA holds 16 lines of N complex values in shared memory, interleaved:
+// element i of line l sits at s[i*16 + l]. All 16 lines are transformed at once.
+// Threads are mapped line-fastest (item u -> line u & 15, butterfly u >> 4), so
+// every load and store of every stage touches two runs of 16 consecutive
+// float2 per warp: the two-wavefront minimum for 8-byte accesses, with no
+// padding and no bank conflicts.
 //
-// Shared-memory layout: element i of a line sits at i + (i >> 4) (one pad slot
-// per 16 float2), which keeps every stage's accesses at or near the two
-// wavefronts per warp that 8-byte accesses need.
+// Stages are mixed radix (8, then 4 or 2 for the remainder) in the self-sorting
+// Stockham form: the stage with radix R and sub-transform length Ns reads
+// in[j + r*N/R], multiplies by W_{Ns*R}^{(j mod Ns)*r}, does an R-point DFT in
+// registers and writes out[(j/Ns)*Ns*R + (j mod Ns) + r*Ns]. Output is in
+// natural order. Each stage loads all its butterflies into registers,
+// synchronises and stores back in place.
 //
-// Twiddles come from a table tw[m] = exp(-2 pi i m / M) of the transform's
-// "table length" M = N * TWS (TWS = table stride); the inverse uses conjugates.
-// Transforms are unnormalised.
+// Twiddles come from a table tw[m] = exp(-2 pi i m / M) of length M = N * TWS
+// (TWS = table stride); the inverse uses conjugates. Transforms are unnormalised.
 #pragma once
 
 #include <cuda_runtime.h>
 
 namespace sd {
 namespace fft {
-
-__host__ __device__ constexpr int pad(int i) { return i + (i >> 4); }
-__host__ __device__ constexpr int line_stride(int n) { return n + (n >> 4) + 1; }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -78,24 +76,23 @@ struct radix_of {
     static constexpr int value = (REM % 8 == 0) ? 8 : ((REM % 4 == 0) ? 4 : 2);
 };
 
-// One Stockham stage on L lines of length N (line stride LS), then recurse.
-template <int N, int Ns, int L, int LS, int NT, int TWS, bool INV>
-__device__ __forceinline__ void stages(float2* s, const float2* tw) {
+// One Stockham stage on the 16 interleaved lines, then recurse.
+template <int N, int Ns, int NT, int TWS, bool INV>
+__device__ __forceinline__ void stages16(float2* s, const float2* tw) {
     if constexpr (Ns < N) {
         constexpr int R = radix_of<N / Ns>::value;
         constexpr int NB = N / R;
-        constexpr int TOT = L * NB;
+        constexpr int TOT = 16 * NB;
         constexpr int PER = (TOT + NT - 1) / NT;
         float2 v[PER][R];
 #pragma unroll
         for (int p = 0; p < PER; ++p) {
-            const int t = threadIdx.x + p * NT;
-            if (TOT % NT == 0 || t < TOT) {
-                const int l = t / NB, j = t % NB, k = j % Ns;
-                const float2* line = s + l * LS;
+            const int u = threadIdx.x + p * NT;
+            if (TOT % NT == 0 || u < TOT) {
+                const int l = u & 15, j = u >> 4, k = j % Ns;
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    float2 x = line[pad(j + r * NB)];
+                    float2 x = s[(j + r * NB) * 16 + l];
                     if (Ns > 1 && r > 0) {
                         float2 w = tw[(k * r * (N / (Ns * R))) * TWS];
                         if (INV) w.y = -w.y;
@@ -108,27 +105,33 @@ __device__ __forceinline__ void stages(float2* s, const float2* tw) {
         __syncthreads();
 #pragma unroll
         for (int p = 0; p < PER; ++p) {
-            const int t = threadIdx.x + p * NT;
-            if (TOT % NT == 0 || t < TOT) {
-                const int l = t / NB, j = t % NB, k = j % Ns;
+            const int u = threadIdx.x + p * NT;
+            if (TOT % NT == 0 || u < TOT) {
+                const int l = u & 15, j = u >> 4, k = j % Ns;
                 dft<R, INV>(v[p]);
-                float2* line = s + l * LS;
                 const int base = (j / Ns) * Ns * R + k;
 #pragma unroll
-                for (int r = 0; r < R; ++r) line[pad(base + r * Ns)] = v[p][r];
+                for (int r = 0; r < R; ++r) s[(base + r * Ns) * 16 + l] = v[p][r];
             }
         }
         __syncthreads();
-        stages<N, Ns * R, L, LS, NT, TWS, INV>(s, tw);
+        stages16<N, Ns * R, NT, TWS, INV>(s, tw);
     }
 }
 
-// Transform L lines of length N held in s (line stride LS). Caller synchronises
-// before the call (data in place); the routine ends with a barrier.
-template <int N, int L, int LS, int NT, int TWS, bool INV>
-__device__ __forceinline__ void lines(float2* s, const float2* tw) {
-    stages<N, 1, L, LS, NT, TWS, INV>(s, tw);
+// Transform the 16 interleaved lines of length N in s. The caller synchronises
+// before the call; the routine ends with a barrier.
+template <int N, int NT, int TWS, bool INV>
+__device__ __forceinline__ void lines16(float2* s, const float2* tw) {
+    stages16<N, 1, NT, TWS, INV>(s, tw);
 }
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 }  // namespace fft
 }  // namespace sd

@@ -45,11 +45,18 @@ struct PoissonPlan {
 };
 int poisson_plan_build(PoissonPlan& p, int G, float soft);
 void poisson_plan_free(PoissonPlan& p);
-size_t poisson_spectrum_elems(int G);  // complex elements of one spectrum buffer
-// rho_fixed != nullptr: the first pass reads the int64 fixed-point grid (and
-// zeroes it); otherwise it reads rho_float.
-int launch_poisson(const PoissonPlan& p, const long long* rho_fixed, const float* rho_float, int clear_fixed,
-                   float* rho_keep, float2* specA, float2* specB, float* phi, cudaStream_t s);
+size_t poisson_spectrum_elems(int G);  // complex elements of the (bricked, padded) spectrum buffer
+// rho_fixed != nullptr: the first pass reads the int64 fixed-point grid and
+// zeroes it; otherwise it reads rho_float. rho_keep (optional) receives the
+// float density. The spectrum buffer is transformed in place.
+int launch_poisson(const PoissonPlan& p, const long long* rho_fixed, const float* rho_float, float* rho_keep,
+                   float2* spec, float* phi, cudaStream_t s);
+// pos != nullptr: the first pass deposits the particles itself (SD_ORDER_TILED
+// order, row_start from launch_row_bounds) instead of reading a density grid.
+int launch_poisson_ex(const PoissonPlan& p, const long long* rho_fixed, const float* rho_float, const float4* pos,
+                      const int* row_start, float* rho_keep, float2* spec, float* phi, cudaStream_t s);
+// row_start[r] = first index i with sorted keys_plus1[i] > r, for r in [0, rows]
+int launch_row_bounds(const uint32_t* keys_plus1, int n, int rows, int* row_start, cudaStream_t s);
 
 size_t gather_partials(int n);
 int launch_gather_kick_drift(const float* phi, int G, float pot_scale, float4* pos, float4* vel, int n,

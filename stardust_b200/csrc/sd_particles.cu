@@ -31,6 +31,7 @@ namespace sd {
 namespace {
 
 constexpr int kGatherThreads = 256;
+constexpr int kGatherMaxBlocks = 4096;
 
 __global__ void __launch_bounds__(256) k_deposit_fixed(const float4* __restrict__ pos, int n, int G,
                                                        unsigned long long* __restrict__ acc) {
@@ -66,8 +67,13 @@ __global__ void k_clear_u64(unsigned long long* __restrict__ a, size_t n) {
     if (i < n) a[i] = 0ull;
 }
 
-// CIC-interpolated central-difference gradient of phi at p (the reference's
-// kGridAccel values sampled with sampleAcc's weights and FMA order).
+// CIC-interpolated central-difference gradient of phi at p: the reference's
+// kGridAccel values (Sim.cu:604-610) sampled with sampleAcc's weights and FMA
+// order (Sim.cu:614-629). The 8 corners' 48 potential reads touch 32 distinct
+// cells; each is loaded once:
+//   A[oy][oz][d]  rows (iy+oy, iz+oz), x = ix-1+d, d < 4
+//   Y[e][oz][ox]  rows (iy-1+3e, iz+oz), x = ix+ox
+//   Z[e][oy][ox]  rows (iy+oy, iz-1+3e), x = ix+ox
 __device__ __forceinline__ float3 gather_accel(const float* __restrict__ phi, int G, float h, float4 p) {
     int ix, iy, iz;
     float fx, fy, fz;
@@ -75,21 +81,45 @@ __device__ __forceinline__ float3 gather_accel(const float* __restrict__ phi, in
     cic_axis(p.y, G, iy, fy);
     cic_axis(p.z, G, iz, fz);
     const int m = G - 1;
+    const size_t G2 = (size_t)G * G;
+    int xs[4];
+#pragma unroll
+    for (int d = 0; d < 4; ++d) xs[d] = (ix - 1 + d) & m;
+    size_t ys[4], zs[4];
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+        ys[d] = (size_t)((iy - 1 + d) & m) * G;
+        zs[d] = (size_t)((iz - 1 + d) & m) * G2;
+    }
+    float A[2][2][4], Y[2][2][2], Z[2][2][2];
+#pragma unroll
+    for (int oy = 0; oy < 2; ++oy)
+#pragma unroll
+        for (int oz = 0; oz < 2; ++oz)
+#pragma unroll
+            for (int d = 0; d < 4; ++d) A[oy][oz][d] = __ldg(phi + zs[1 + oz] + ys[1 + oy] + xs[d]);
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+#pragma unroll
+        for (int o = 0; o < 2; ++o)
+#pragma unroll
+            for (int ox = 0; ox < 2; ++ox) {
+                Y[e][o][ox] = __ldg(phi + zs[1 + o] + ys[3 * e] + xs[1 + ox]);
+                Z[e][o][ox] = __ldg(phi + zs[3 * e] + ys[1 + o] + xs[1 + ox]);
+            }
     float3 a = make_float3(0.f, 0.f, 0.f);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
+        const int ox = k & 1, oy = (k >> 1) & 1, oz = (k >> 2) & 1;
         const float w = cic_weight(k, fx, fy, fz);
-        const int cx = (ix + (k & 1)) & m;
-        const int cy = (iy + ((k >> 1) & 1)) & m;
-        const int cz = (iz + ((k >> 2) & 1)) & m;
-        const size_t row = ((size_t)cz * G + cy) * G;
-        const float gx = __fmul_rn(-__fsub_rn(__ldg(phi + row + ((cx + 1) & m)), __ldg(phi + row + ((cx - 1) & m))), h);
-        const float gy = __fmul_rn(-__fsub_rn(__ldg(phi + ((size_t)cz * G + ((cy + 1) & m)) * G + cx),
-                                              __ldg(phi + ((size_t)cz * G + ((cy - 1) & m)) * G + cx)),
-                                   h);
-        const float gz = __fmul_rn(-__fsub_rn(__ldg(phi + ((size_t)((cz + 1) & m) * G + cy) * G + cx),
-                                              __ldg(phi + ((size_t)((cz - 1) & m) * G + cy) * G + cx)),
-                                   h);
+        const float xp = A[oy][oz][ox + 2], xm = A[oy][oz][ox];
+        const float yp = oy ? Y[1][oz][ox] : A[1][oz][ox + 1];
+        const float ym = oy ? A[0][oz][ox + 1] : Y[0][oz][ox];
+        const float zp = oz ? Z[1][oy][ox] : A[oy][1][ox + 1];
+        const float zm = oz ? A[oy][0][ox + 1] : Z[0][oy][ox];
+        const float gx = __fmul_rn(-__fsub_rn(xp, xm), h);
+        const float gy = __fmul_rn(-__fsub_rn(yp, ym), h);
+        const float gz = __fmul_rn(-__fsub_rn(zp, zm), h);
         a.x = __fmaf_rn(gx, w, a.x);
         a.y = __fmaf_rn(gy, w, a.y);
         a.z = __fmaf_rn(gz, w, a.z);
@@ -117,51 +147,57 @@ __device__ __forceinline__ void block_sum4(double v0, double v1, double v2, doub
     }
 }
 
+// One thread per particle, grid-stride over at most kGatherMaxBlocks blocks so the
+// per-block FP64 partials stay few; the block-to-particle assignment depends only
+// on n, so the sums are deterministic.
 __global__ void __launch_bounds__(kGatherThreads) k_gather_kick_drift(const float* __restrict__ phi, int G, float h,
                                                                       float4* __restrict__ pos, float4* __restrict__ vel,
                                                                       int n, float dt_kick, float dt_drift, float c2,
                                                                       const float* __restrict__ mean_vel,
                                                                       double* __restrict__ partials) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double sx = 0.0, sy = 0.0, sz = 0.0, cnt = 0.0;
-    if (i < n) {
+    const float mx = mean_vel ? mean_vel[0] : 0.f, my = mean_vel ? mean_vel[1] : 0.f,
+                mz = mean_vel ? mean_vel[2] : 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 p = pos[i];
-        if (p.x >= 0.f) {
-            float4 v = vel[i];
-            if (mean_vel) {
-                v.x = __fsub_rn(v.x, mean_vel[0]);
-                v.y = __fsub_rn(v.y, mean_vel[1]);
-                v.z = __fsub_rn(v.z, mean_vel[2]);
-            }
-            const float3 a = gather_accel(phi, G, h, p);
-            v.x = __fmaf_rn(a.x, dt_kick, v.x);
-            v.y = __fmaf_rn(a.y, dt_kick, v.y);
-            v.z = __fmaf_rn(a.z, dt_kick, v.z);
-            {  // light-speed clamp (Sim.cu:834-840)
-                const float sp2 = __fmaf_rn(v.z, v.z, __fmaf_rn(v.y, v.y, __fmul_rn(v.x, v.x)));
-                if (sp2 > c2) {
-                    const float k = sqrtf(__fdiv_rn(c2, sp2));
-                    v.x = __fmul_rn(v.x, k);
-                    v.y = __fmul_rn(v.y, k);
-                    v.z = __fmul_rn(v.z, k);
-                }
-            }
-            p.x = __fmaf_rn(v.x, dt_drift, p.x);
-            p.y = __fmaf_rn(v.y, dt_drift, p.y);
-            p.z = __fmaf_rn(v.z, dt_drift, p.z);
-            if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z) || !isfinite(v.x) || !isfinite(v.y) ||
-                !isfinite(v.z)) {
-                pos[i] = make_float4(-1.f, -1.f, -1.f, 0.f);
-                vel[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            } else {
-                p.x = __fsub_rn(p.x, floorf(p.x));
-                p.y = __fsub_rn(p.y, floorf(p.y));
-                p.z = __fsub_rn(p.z, floorf(p.z));
-                pos[i] = p;
-                vel[i] = v;
-                sx = v.x; sy = v.y; sz = v.z; cnt = 1.0;
+        if (p.x < 0.f) continue;
+        float4 v = vel[i];
+        if (mean_vel) {
+            v.x = __fsub_rn(v.x, mx);
+            v.y = __fsub_rn(v.y, my);
+            v.z = __fsub_rn(v.z, mz);
+        }
+        const float3 a = gather_accel(phi, G, h, p);
+        v.x = __fmaf_rn(a.x, dt_kick, v.x);
+        v.y = __fmaf_rn(a.y, dt_kick, v.y);
+        v.z = __fmaf_rn(a.z, dt_kick, v.z);
+        {  // light-speed clamp (Sim.cu:834-840)
+            const float sp2 = __fmaf_rn(v.z, v.z, __fmaf_rn(v.y, v.y, __fmul_rn(v.x, v.x)));
+            if (sp2 > c2) {
+                const float k = sqrtf(__fdiv_rn(c2, sp2));
+                v.x = __fmul_rn(v.x, k);
+                v.y = __fmul_rn(v.y, k);
+                v.z = __fmul_rn(v.z, k);
             }
         }
+        p.x = __fmaf_rn(v.x, dt_drift, p.x);
+        p.y = __fmaf_rn(v.y, dt_drift, p.y);
+        p.z = __fmaf_rn(v.z, dt_drift, p.z);
+        if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z) || !isfinite(v.x) || !isfinite(v.y) ||
+            !isfinite(v.z)) {
+            pos[i] = make_float4(-1.f, -1.f, -1.f, 0.f);
+            vel[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            continue;
+        }
+        p.x = __fsub_rn(p.x, floorf(p.x));
+        p.y = __fsub_rn(p.y, floorf(p.y));
+        p.z = __fsub_rn(p.z, floorf(p.z));
+        pos[i] = p;
+        vel[i] = v;
+        sx += v.x;
+        sy += v.y;
+        sz += v.z;
+        cnt += 1.0;
     }
     if (partials) block_sum4(sx, sy, sz, cnt, partials);
 }
@@ -243,33 +279,34 @@ __global__ void __launch_bounds__(kGatherThreads) k_energy(const float* __restri
                                                            const float4* __restrict__ vel, int n,
                                                            const float* __restrict__ mean_vel,
                                                            double* __restrict__ partials) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double ke = 0.0, pe = 0.0, px = 0.0, py = 0.0, pz = 0.0, c = 0.0;
-    if (i < n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 p = pos[i];
-        if (p.x >= 0.f) {
-            float4 v = vel[i];
-            if (mean_vel) {
-                v.x = __fsub_rn(v.x, mean_vel[0]);
-                v.y = __fsub_rn(v.y, mean_vel[1]);
-                v.z = __fsub_rn(v.z, mean_vel[2]);
+        if (p.x < 0.f) continue;
+        float4 v = vel[i];
+        if (mean_vel) {
+            v.x = __fsub_rn(v.x, mean_vel[0]);
+            v.y = __fsub_rn(v.y, mean_vel[1]);
+            v.z = __fsub_rn(v.z, mean_vel[2]);
+        }
+        ke += 0.5 * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+        px += v.x;
+        py += v.y;
+        pz += v.z;
+        c += 1.0;
+        if (phi) {
+            int ix, iy, iz;
+            float fx, fy, fz;
+            cic_axis(p.x, G, ix, fx);
+            cic_axis(p.y, G, iy, fy);
+            cic_axis(p.z, G, iz, fz);
+            const int m = G - 1;
+            double f = 0.0;
+            for (int k = 0; k < 8; ++k) {
+                const int cx = (ix + (k & 1)) & m, cy = (iy + ((k >> 1) & 1)) & m, cz = (iz + ((k >> 2) & 1)) & m;
+                f += (double)cic_weight(k, fx, fy, fz) * (double)phi[((size_t)cz * G + cy) * G + cx];
             }
-            ke = 0.5 * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
-            px = v.x; py = v.y; pz = v.z; c = 1.0;
-            if (phi) {
-                int ix, iy, iz;
-                float fx, fy, fz;
-                cic_axis(p.x, G, ix, fx);
-                cic_axis(p.y, G, iy, fy);
-                cic_axis(p.z, G, iz, fz);
-                const int m = G - 1;
-                double f = 0.0;
-                for (int k = 0; k < 8; ++k) {
-                    const int cx = (ix + (k & 1)) & m, cy = (iy + ((k >> 1) & 1)) & m, cz = (iz + ((k >> 2) & 1)) & m;
-                    f += (double)cic_weight(k, fx, fy, fz) * (double)phi[((size_t)cz * G + cy) * G + cx];
-                }
-                pe = 0.5 * f;
-            }
+            pe += 0.5 * f;
         }
     }
     __shared__ double red[6][kGatherThreads / 32];
@@ -369,7 +406,10 @@ int launch_fixed_to_float(const long long* acc, int G, float* rho, int clear, cu
     return SD_OK;
 }
 
-size_t gather_partials(int n) { return (size_t)((n + kGatherThreads - 1) / kGatherThreads); }
+size_t gather_partials(int n) {
+    const int b = (n + kGatherThreads - 1) / kGatherThreads;
+    return (size_t)(b < 1 ? 1 : (b > kGatherMaxBlocks ? kGatherMaxBlocks : b));
+}
 
 int launch_gather_kick_drift(const float* phi, int G, float pot_scale, float4* pos, float4* vel, int n,
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
@@ -415,7 +455,7 @@ int launch_max_speed(const float4* pos, const float4* vel, int n, const float* m
 int launch_energy(const float* phi, int G, const float4* pos, const float4* vel, int n, const float* mean_vel,
                   double* partials, double* out8, cudaStream_t s) {
     if (n <= 0) return SD_OK;
-    const int blocks = (n + kGatherThreads - 1) / kGatherThreads;
+    const int blocks = (int)gather_partials(n);  // partials hold 8 doubles per block
     k_energy<<<blocks, kGatherThreads, 0, s>>>(phi, G, pos, vel, n, mean_vel, partials);
     SD_LAUNCHED(s);
     k_finalize8<<<1, 256, 0, s>>>(partials, blocks, out8);

@@ -1,19 +1,21 @@
-// sd_poisson.cu -- periodic Poisson solve: five passes over the grid, all
-// hand-written (the reference calls cuFFT R2C, kPoissonPeriodic, cuFFT C2R:
-// Sim.cu:3586-3603, 528-557).
+// sd_poisson.cu -- periodic Poisson solve rho -> phi, all passes hand-written
+// (the reference calls cuFFT R2C, kPoissonPeriodic, cuFFT C2R: Sim.cu:3586-3603,
+// 528-557).
 //
-// Layouts (complex = float2, H = G/2, P = H+1 kx bins):
-//   rho, phi : real [z][y][x]
-//   specA    : [z][kx][y]  (y contiguous)    -- written by A and D
-//   specB    : [kx][ky][z] (z contiguous)    -- written by B and C
-// Passes:
-//   A  x-lines real->complex (+ int64 fixed-point -> float conversion), write specA
-//   B  y-lines forward, write specB transposed so z becomes contiguous
-//   C  z-lines: forward, Green's function multiply, inverse (in place)
-//   D  y-lines inverse, write specA layout
-//   E  x-lines complex->real, write phi
-// Every pass reads and writes each element once; transposes happen through the
-// shared-memory tile, so global accesses are whole lines or 64-128 B segments.
+// Spectrum layout: one buffer of 4x4x4 complex "bricks" (512 B each). The kx
+// axis holds the H+1 = G/2+1 bins of the real transform padded to H+4 (the last
+// brick carries the Nyquist bin and three zero columns). Brick (bx,by,bz) starts
+// at (((bz*NBY + by)*NBX + bx) * 64); inside a brick element (kx_l, y_l, z_l)
+// sits at z_l*16 + y_l*4 + kx_l.
+//
+// Passes (CTA = one 4x4 bundle of 16 lines, held interleaved in shared memory):
+//   A  x-rows real -> complex (input: float grid or int64 fixed-point grid)
+//   B  y-lines forward            (in place)
+//   C  z-lines forward, Green's function, z-lines inverse (in place)
+//   D  y-lines inverse            (in place)
+//   E  x-rows complex -> real, write phi
+// Every global access moves whole 512-byte bricks or whole rows, B/C/D stage
+// their bricks with cp.async, and each pass reads and writes every element once.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -29,232 +31,474 @@ namespace sd {
 namespace {
 
 constexpr int kFftThreads = 256;
+constexpr int kDepositThreads = 512;
 
 template <int G>
-struct Tiles {
+struct Geo {
     static constexpr int H = G / 2;
-    static constexpr int P = H + 1;
-    static constexpr int TY = (G < 16) ? G : 16;  // rows per CTA in passes A and E
-    static constexpr int TZ = (G < 8) ? G : 8;    // lines per CTA in passes B and D
-    static constexpr int LC = (G < 8) ? G : 8;    // lines per CTA in pass C
-    static constexpr int LSH = fft::line_stride(H);
-    static constexpr int LSG = fft::line_stride(G);
+    static constexpr int NBX = H / 4 + 1;  // kx bricks (last: Nyquist + padding)
+    static constexpr int PX = 4 * NBX;     // padded kx positions = H + 4
+    static constexpr int NBY = G / 4;
+    static constexpr int NBZ = G / 4;
+    __device__ __forceinline__ static size_t brick(int bx, int by, int bz) {
+        return ((((size_t)bz * NBY + by) * NBX) + bx) * 64;
+    }
 };
 
-template <int G>
-__global__ void __launch_bounds__(kFftThreads) k_pass_a(const long long* __restrict__ acc, const float* __restrict__ rho,
-                                                        int clear_acc, float* __restrict__ rho_keep,
-                                                        float2* __restrict__ specA, const float2* __restrict__ tw_g) {
-    using T = Tiles<G>;
-    constexpr int H = T::H, P = T::P, TY = T::TY, LS = T::LSH;
+// ---- pass A: rows (y = 4by + y_l, z = 4bz + z_l) -> kx bins -----------------
+// line l = z_l*4 + y_l; positions m < H hold z[m] = x[2m] + i x[2m+1].
+template <int G, int SRC>  // SRC 0: float grid, 1: int64 fixed-point grid (zeroed after reading)
+__global__ void __launch_bounds__(kFftThreads) k_pass_a(const float* __restrict__ rho, long long* __restrict__ acc,
+                                                        float* __restrict__ rho_keep, float2* __restrict__ spec,
+                                                        const float2* __restrict__ tw_g) {
+    using T = Geo<G>;
+    constexpr int H = T::H, NBX = T::NBX;
+    constexpr int ITEMS = 16 * (H / 2);  // (line, pair of positions)
+    constexpr int PER = (ITEMS + kFftThreads - 1) / kFftThreads;
     extern __shared__ float2 sm[];
     float2* tw = sm;
     float2* s = sm + G;
-    const int y0 = blockIdx.x * TY, z = blockIdx.y;
+    const int by = blockIdx.x, bz = blockIdx.y;
     for (int i = threadIdx.x; i < G; i += kFftThreads) tw[i] = tw_g[i];
-    for (int t = threadIdx.x; t < TY * H; t += kFftThreads) {
-        const int yy = t / H, m = t % H;
-        const size_t row = ((size_t)z * G + y0 + yy) * G;
-        float2 v;
-        if (acc) {
-            longlong2* p = reinterpret_cast<longlong2*>(const_cast<long long*>(acc) + row) + m;
-            const longlong2 q = *p;
-            v = make_float2(fixed_to_float(q.x), fixed_to_float(q.y));
-            if (clear_acc) *p = make_longlong2(0, 0);
-            if (rho_keep) reinterpret_cast<float2*>(rho_keep + row)[m] = v;
-        } else {
-            v = reinterpret_cast<const float2*>(rho + row)[m];
+
+    float4 v[PER];
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+        const int u = threadIdx.x + p * kFftThreads;
+        if (ITEMS % kFftThreads == 0 || u < ITEMS) {
+            const int l = u & 15, mp = u >> 4;
+            const size_t row = ((size_t)(bz * 4 + (l >> 2)) * G + by * 4 + (l & 3)) * G;
+            if (SRC == 0) {
+                v[p] = *reinterpret_cast<const float4*>(rho + row + 4 * mp);
+            } else {
+                const longlong2 q0 = *reinterpret_cast<const longlong2*>(acc + row + 4 * mp);
+                const longlong2 q1 = *reinterpret_cast<const longlong2*>(acc + row + 4 * mp + 2);
+                v[p] = make_float4(fixed_to_float(q0.x), fixed_to_float(q0.y), fixed_to_float(q1.x),
+                                   fixed_to_float(q1.y));
+            }
         }
-        s[yy * LS + fft::pad(m)] = v;
+    }
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+        const int u = threadIdx.x + p * kFftThreads;
+        if (ITEMS % kFftThreads == 0 || u < ITEMS) {
+            const int l = u & 15, mp = u >> 4;
+            const size_t row = ((size_t)(bz * 4 + (l >> 2)) * G + by * 4 + (l & 3)) * G;
+            if (SRC == 1) {
+                *reinterpret_cast<longlong2*>(acc + row + 4 * mp) = make_longlong2(0, 0);
+                *reinterpret_cast<longlong2*>(acc + row + 4 * mp + 2) = make_longlong2(0, 0);
+            }
+            if (rho_keep) *reinterpret_cast<float4*>(rho_keep + row + 4 * mp) = v[p];
+            s[(2 * mp) * 16 + l] = make_float2(v[p].x, v[p].y);
+            s[(2 * mp + 1) * 16 + l] = make_float2(v[p].z, v[p].w);
+        }
     }
     __syncthreads();
-    fft::lines<H, TY, LS, kFftThreads, 2, false>(s, tw);
-    // Z -> X:  X[k] = E[k] + W_G^k O[k],  E = (Z[k] + conj Z[H-k])/2,  O = (Z[k] - conj Z[H-k])/(2i)
-    for (int t = threadIdx.x; t < P * TY; t += kFftThreads) {
-        const int kx = t / TY, yy = t % TY;
-        const float2* line = s + yy * LS;
-        const float2 zk = line[fft::pad(kx == H ? 0 : kx)];
-        const float2 zc = line[fft::pad(kx == 0 ? 0 : H - kx)];
+    fft::lines16<H, kFftThreads, 2, false>(s, tw);
+    // Z -> X, pairs (k, H-k):  E = (Z[k] + conj Z[H-k])/2,  O = (Z[k] - conj Z[H-k])/(2i),
+    // X[k] = E + W^k O,  X[H-k] = conj E + W^(H-k) conj O;  X[0], X[H] from Z[0].
+    constexpr int PAIRS = 16 * (H / 2 + 1);
+    for (int u = threadIdx.x; u < PAIRS; u += kFftThreads) {
+        const int l = u & 15, k = u >> 4;
+        if (k == 0) {
+            const float2 z0 = s[l];
+            s[l] = make_float2(z0.x + z0.y, 0.f);
+            s[H * 16 + l] = make_float2(z0.x - z0.y, 0.f);
+            s[(H + 1) * 16 + l] = make_float2(0.f, 0.f);
+            s[(H + 2) * 16 + l] = make_float2(0.f, 0.f);
+            s[(H + 3) * 16 + l] = make_float2(0.f, 0.f);
+            continue;
+        }
+        const float2 zk = s[k * 16 + l], zc = s[(H - k) * 16 + l];
         const float er = 0.5f * (zk.x + zc.x), ei = 0.5f * (zk.y - zc.y);
         const float orr = 0.5f * (zk.y + zc.y), oi = -0.5f * (zk.x - zc.x);
-        const float2 w = tw[kx];
-        specA[((size_t)z * P + kx) * G + y0 + yy] =
-            make_float2(er + (w.x * orr - w.y * oi), ei + (w.x * oi + w.y * orr));
+        const float2 w = tw[k];
+        s[k * 16 + l] = make_float2(er + (w.x * orr - w.y * oi), ei + (w.x * oi + w.y * orr));
+        if (2 * k != H) {
+            const float2 w2 = tw[H - k];  // conj E + W^(H-k) conj O
+            s[(H - k) * 16 + l] = make_float2(er + (w2.x * orr + w2.y * oi), -ei + (w2.y * orr - w2.x * oi));
+        }
+    }
+    __syncthreads();
+    // store bricks (bx, by, bz): brick element e = z_l*16 + y_l*4 + kx_l, two at a time
+    for (int u = threadIdx.x; u < NBX * 32; u += kFftThreads) {
+        const int bx = u >> 5, c = u & 31;
+        const int l = (c >> 3) * 4 + ((c >> 1) & 3), kx = bx * 4 + (c & 1) * 2;
+        const float2 a = s[kx * 16 + l], b = s[(kx + 1) * 16 + l];
+        *reinterpret_cast<float4*>(spec + T::brick(bx, by, bz) + 2 * c) = make_float4(a.x, a.y, b.x, b.y);
     }
 }
 
+// ---- pass A fused with the CIC deposit (particles in SD_ORDER_TILED order) --------
+// The CTA for row bundle (by, bz) owns rows y in [4by, 4by+4), z in [4bz, 4bz+4).
+// Particles are sorted by the row of their CIC base cell, rows grouped in these
+// 4x4 bundles; row_start[r] .. row_start[r+1] is the slice of key-space row r.
+// The CTA reads the 25 base rows whose stencils reach its rows (y and z in
+// [4b-1, 4b+3]), adds each in-bundle corner weight, rounded once to a multiple
+// of 2^-32, into an int64 row buffer in shared memory, then converts and
+// transforms the rows exactly as pass A does. Integer sums make the density
+// independent of the order of the adds; no density grid is written.
 template <int G>
-__global__ void __launch_bounds__(kFftThreads) k_pass_b(const float2* __restrict__ specA, float2* __restrict__ specB,
-                                                        const float2* __restrict__ tw_g) {
-    using T = Tiles<G>;
-    constexpr int P = T::P, TZ = T::TZ, LS = T::LSG;
+__global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4* __restrict__ pos,
+                                                                    const int* __restrict__ row_start,
+                                                                    float* __restrict__ rho_keep,
+                                                                    float2* __restrict__ spec,
+                                                                    const float2* __restrict__ tw_g) {
+    using T = Geo<G>;
+    constexpr int H = T::H, NBX = T::NBX, NT = kDepositThreads;
+    extern __shared__ float2 sm[];
+    float2* tw = sm;
+    // The int64 fixed-point sums, as two 32-bit words per cell (lo[16][G], hi[16][G]),
+    // share their storage with the complex line buffer used after the conversion.
+    unsigned* acc_lo = reinterpret_cast<unsigned*>(sm + G);
+    unsigned* acc_hi = acc_lo + 16 * G;
+    float2* s = sm + G;
+    __shared__ int range_lo[25], range_off[26];
+    const int by = blockIdx.x, bz = blockIdx.y;
+    const int m = G - 1;
+    for (int i = threadIdx.x; i < G; i += NT) tw[i] = tw_g[i];
+    for (int i = threadIdx.x; i < 8 * G; i += NT) reinterpret_cast<uint4*>(acc_lo)[i] = make_uint4(0u, 0u, 0u, 0u);
+    if (threadIdx.x < 32) {
+        // source rows (iy, iz) = (4by - 1 + j % 5, 4bz - 1 + j / 5), j < 25
+        const int j = threadIdx.x;
+        int lo = 0, len = 0;
+        if (j < 25) {
+            const int iy = (4 * by - 1 + j % 5) & m, iz = (4 * bz - 1 + j / 5) & m;
+            const int key = ((iz >> 2) * (G / 4) + (iy >> 2)) * 16 + (iz & 3) * 4 + (iy & 3);
+            lo = row_start[key];
+            len = row_start[key + 1] - lo;
+        }
+        int inc = len;  // inclusive scan of the lengths across the warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (j >= o) inc += t;
+        }
+        if (j < 25) {
+            range_lo[j] = lo;
+            range_off[j + 1] = inc;
+        }
+        if (j == 0) range_off[0] = 0;
+    }
+    __syncthreads();
+    const int total = range_off[25];
+    int r = 0;
+    // Loads are issued kBatch at a time so several particles are in flight per
+    // thread before the shared-memory adds.
+    constexpr int kBatch = 4;
+    for (int f0 = threadIdx.x; f0 < total; f0 += kBatch * NT) {
+        float4 pb[kBatch];
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b) {
+            const int f = f0 + b * NT;
+            if (f < total) {
+                while (f >= range_off[r + 1]) ++r;
+                pb[b] = pos[range_lo[r] + (f - range_off[r])];
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b) {
+            if (f0 + b * NT >= total) break;
+            const float4 p = pb[b];
+            int ix, iy, iz;
+            float fx, fy, fz;
+            cic_axis(p.x, G, ix, fx);
+            cic_axis(p.y, G, iy, fy);
+            cic_axis(p.z, G, iz, fz);
+            const int x0 = ix & m, x1 = (ix + 1) & m;
+#pragma unroll
+            for (int oyz = 0; oyz < 4; ++oyz) {
+                const int oy = oyz & 1, oz = oyz >> 1;
+                const int yl = ((iy + oy) & m) - 4 * by;
+                const int zl = ((iz + oz) & m) - 4 * bz;
+                if ((unsigned)yl >= 4u || (unsigned)zl >= 4u) continue;
+                const int rowc = (zl * 4 + yl) * G;
+#pragma unroll
+                for (int ox = 0; ox < 2; ++ox) {
+                    // q in [0, 2^32]: add the low word and carry into the high word.
+                    // atomicAdd returns the previous low word, so every wrap is seen
+                    // by exactly one add and the 64-bit total is exact.
+                    const unsigned long long q =
+                        (unsigned long long)fixed_weight(cic_weight(ox | (oy << 1) | (oz << 2), fx, fy, fz));
+                    const int c = rowc + (ox ? x1 : x0);
+                    const unsigned lo = (unsigned)q;
+                    const unsigned old = atomicAdd(acc_lo + c, lo);
+                    const unsigned up = (unsigned)(q >> 32) + ((old + lo < old) ? 1u : 0u);
+                    if (up) atomicAdd(acc_hi + c, up);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // int64 rows -> complex positions z[m] = x[2m] + i x[2m+1] on line l = z_l*4 + y_l,
+    // staged through registers because the line buffer overlays the sums.
+    constexpr int CITEMS = 16 * (H / 2);
+    constexpr int CPER = (CITEMS + NT - 1) / NT;
+    float4 cv[CPER];
+#pragma unroll
+    for (int p = 0; p < CPER; ++p) {
+        const int u = threadIdx.x + p * NT;
+        if (CITEMS % NT == 0 || u < CITEMS) {
+            const int l = u & 15, mp = u >> 4;
+            const uint4 lo = *reinterpret_cast<const uint4*>(acc_lo + l * G + 4 * mp);
+            const uint4 hi = *reinterpret_cast<const uint4*>(acc_hi + l * G + 4 * mp);
+            cv[p] = make_float4(fixed_to_float((long long)(((unsigned long long)hi.x << 32) | lo.x)),
+                                fixed_to_float((long long)(((unsigned long long)hi.y << 32) | lo.y)),
+                                fixed_to_float((long long)(((unsigned long long)hi.z << 32) | lo.z)),
+                                fixed_to_float((long long)(((unsigned long long)hi.w << 32) | lo.w)));
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < CPER; ++p) {
+        const int u = threadIdx.x + p * NT;
+        if (CITEMS % NT == 0 || u < CITEMS) {
+            const int l = u & 15, mp = u >> 4;
+            if (rho_keep) {
+                const size_t grow = ((size_t)(bz * 4 + (l >> 2)) * G + by * 4 + (l & 3)) * G;
+                *reinterpret_cast<float4*>(rho_keep + grow + 4 * mp) = cv[p];
+            }
+            s[(2 * mp) * 16 + l] = make_float2(cv[p].x, cv[p].y);
+            s[(2 * mp + 1) * 16 + l] = make_float2(cv[p].z, cv[p].w);
+        }
+    }
+    __syncthreads();
+    fft::lines16<H, NT, 2, false>(s, tw);
+    constexpr int PAIRS = 16 * (H / 2 + 1);
+    for (int u = threadIdx.x; u < PAIRS; u += NT) {
+        const int l = u & 15, k = u >> 4;
+        if (k == 0) {
+            const float2 z0 = s[l];
+            s[l] = make_float2(z0.x + z0.y, 0.f);
+            s[H * 16 + l] = make_float2(z0.x - z0.y, 0.f);
+            s[(H + 1) * 16 + l] = make_float2(0.f, 0.f);
+            s[(H + 2) * 16 + l] = make_float2(0.f, 0.f);
+            s[(H + 3) * 16 + l] = make_float2(0.f, 0.f);
+            continue;
+        }
+        const float2 zk = s[k * 16 + l], zc = s[(H - k) * 16 + l];
+        const float er = 0.5f * (zk.x + zc.x), ei = 0.5f * (zk.y - zc.y);
+        const float orr = 0.5f * (zk.y + zc.y), oi = -0.5f * (zk.x - zc.x);
+        const float2 w = tw[k];
+        s[k * 16 + l] = make_float2(er + (w.x * orr - w.y * oi), ei + (w.x * oi + w.y * orr));
+        if (2 * k != H) {
+            const float2 w2 = tw[H - k];
+            s[(H - k) * 16 + l] = make_float2(er + (w2.x * orr + w2.y * oi), -ei + (w2.y * orr - w2.x * oi));
+        }
+    }
+    __syncthreads();
+    for (int u = threadIdx.x; u < NBX * 32; u += NT) {
+        const int bx = u >> 5, c = u & 31;
+        const int l = (c >> 3) * 4 + ((c >> 1) & 3), kx = bx * 4 + (c & 1) * 2;
+        const float2 a = s[kx * 16 + l], b = s[(kx + 1) * 16 + l];
+        *reinterpret_cast<float4*>(spec + T::brick(bx, by, bz) + 2 * c) = make_float4(a.x, a.y, b.x, b.y);
+    }
+}
+
+// Stage bricks into shared memory with cp.async. DIR 1: y-lines of CTA (bx,bz);
+// DIR 2: z-lines of CTA (bx,by). Lines: DIR 1 -> z_l*4 + kx_l, DIR 2 -> y_l*4 + kx_l.
+template <int G, int DIR>
+__device__ __forceinline__ void load_lines(float2* s, const float2* __restrict__ spec, int b0, int b1) {
+    using T = Geo<G>;
+    constexpr int NB = (DIR == 1) ? T::NBY : T::NBZ;
+    for (int u = threadIdx.x; u < NB * 32; u += kFftThreads) {
+        const int b = u >> 5, c = u & 31;
+        const int e = 2 * c;
+        size_t src;
+        int dst;
+        if (DIR == 1) {  // b = by
+            src = T::brick(b0, b, b1) + e;
+            dst = (b * 4 + ((e >> 2) & 3)) * 16 + (e >> 4) * 4 + (e & 3);
+        } else {  // b = bz: the brick lands contiguously
+            src = T::brick(b0, b1, b) + e;
+            dst = b * 64 + e;
+        }
+        fft::cp_async16(s + dst, spec + src);
+    }
+    fft::cp_async_wait_all();
+    __syncthreads();
+}
+
+template <int G, int DIR>
+__device__ __forceinline__ void store_lines(const float2* s, float2* __restrict__ spec, int b0, int b1) {
+    using T = Geo<G>;
+    constexpr int NB = (DIR == 1) ? T::NBY : T::NBZ;
+    for (int u = threadIdx.x; u < NB * 32; u += kFftThreads) {
+        const int b = u >> 5, c = u & 31;
+        const int e = 2 * c;
+        size_t dst;
+        int src;
+        if (DIR == 1) {
+            dst = T::brick(b0, b, b1) + e;
+            src = (b * 4 + ((e >> 2) & 3)) * 16 + (e >> 4) * 4 + (e & 3);
+        } else {
+            dst = T::brick(b0, b1, b) + e;
+            src = b * 64 + e;
+        }
+        *reinterpret_cast<float4*>(spec + dst) = *reinterpret_cast<const float4*>(s + src);
+    }
+}
+
+// ---- passes B and D: y-lines of CTA (bx, bz), in place -------------------------
+template <int G, bool INV>
+__global__ void __launch_bounds__(kFftThreads) k_pass_y(float2* __restrict__ spec, const float2* __restrict__ tw_g) {
     extern __shared__ float2 sm[];
     float2* tw = sm;
     float2* s = sm + G;
-    const int z0 = blockIdx.x * TZ, kx = blockIdx.y;
+    const int bx = blockIdx.x, bz = blockIdx.y;
     for (int i = threadIdx.x; i < G; i += kFftThreads) tw[i] = tw_g[i];
-    for (int t = threadIdx.x; t < TZ * G; t += kFftThreads) {
-        const int l = t / G, y = t % G;
-        s[l * LS + fft::pad(y)] = specA[((size_t)(z0 + l) * P + kx) * G + y];
-    }
-    __syncthreads();
-    fft::lines<G, TZ, LS, kFftThreads, 1, false>(s, tw);
-    for (int t = threadIdx.x; t < TZ * G; t += kFftThreads) {
-        const int l = t % TZ, ky = t / TZ;
-        specB[((size_t)kx * G + ky) * G + z0 + l] = s[l * LS + fft::pad(ky)];
-    }
+    load_lines<G, 1>(s, spec, bx, bz);
+    fft::lines16<G, kFftThreads, 1, INV>(s, tw);
+    store_lines<G, 1>(s, spec, bx, bz);
 }
 
+// ---- pass C: z-lines of CTA (bx, by): forward, Green's function, inverse ---------
 template <int G>
-__global__ void __launch_bounds__(kFftThreads) k_pass_c(float2* __restrict__ specB, const float2* __restrict__ tw_g,
+__global__ void __launch_bounds__(kFftThreads) k_pass_c(float2* __restrict__ spec, const float2* __restrict__ tw_g,
                                                         const float* __restrict__ gexp_g, float scale) {
-    using T = Tiles<G>;
-    constexpr int LC = T::LC, LS = T::LSG, H = T::H;
+    using T = Geo<G>;
+    constexpr int H = T::H;
     extern __shared__ float2 sm[];
     float2* tw = sm;
     float* gexp = reinterpret_cast<float*>(sm + G);
     float2* s = sm + G + (H + 2) / 2 + 1;
-    const int ky0 = blockIdx.x * LC, kx = blockIdx.y;
-    float2* base = specB + ((size_t)kx * G + ky0) * G;
+    const int bx = blockIdx.x, by = blockIdx.y;
     for (int i = threadIdx.x; i < G; i += kFftThreads) tw[i] = tw_g[i];
     for (int i = threadIdx.x; i <= H; i += kFftThreads) gexp[i] = gexp_g[i];
-    for (int t = threadIdx.x; t < LC * G; t += kFftThreads) {
-        const int l = t / G, z = t % G;
-        s[l * LS + fft::pad(z)] = base[t];
-    }
-    __syncthreads();
-    fft::lines<G, LC, LS, kFftThreads, 1, false>(s, tw);
-    // Green's function: -scale/k^2 * exp(-k^2 s^2/2), k = 0 -> 0 (Sim.cu:536-556).
-    for (int t = threadIdx.x; t < LC * G; t += kFftThreads) {
-        const int l = t / G, kz = t % G;
-        const int ky = ky0 + l;
+    load_lines<G, 2>(s, spec, bx, by);
+    fft::lines16<G, kFftThreads, 1, false>(s, tw);
+    // Green's function: -scale/k^2 * exp(-k^2 s^2/2), k = 0 -> 0 (Sim.cu:536-556);
+    // padding columns kx > H are zeroed.
+    for (int u = threadIdx.x; u < 16 * G; u += kFftThreads) {
+        const int l = u & 15, kz = u >> 4;
+        const int kx = bx * 4 + (l & 3), ky = by * 4 + (l >> 2);
         const int kyf = (ky <= G / 2) ? ky : ky - G;
         const int kzf = (kz <= G / 2) ? kz : kz - G;
         const int k2 = kx * kx + kyf * kyf + kzf * kzf;
         float m = 0.f;
-        if (k2 != 0) m = (-scale / (float)k2) * (gexp[kx] * gexp[abs(kyf)] * gexp[abs(kzf)]);
-        float2& e = s[l * LS + fft::pad(kz)];
+        if (k2 != 0 && kx <= H) m = (-scale / (float)k2) * (gexp[kx] * gexp[abs(kyf)] * gexp[abs(kzf)]);
+        float2& e = s[u];
         e.x *= m;
         e.y *= m;
     }
     __syncthreads();
-    fft::lines<G, LC, LS, kFftThreads, 1, true>(s, tw);
-    for (int t = threadIdx.x; t < LC * G; t += kFftThreads) {
-        const int l = t / G, z = t % G;
-        base[t] = s[l * LS + fft::pad(z)];
-    }
+    fft::lines16<G, kFftThreads, 1, true>(s, tw);
+    store_lines<G, 2>(s, spec, bx, by);
 }
 
+// ---- pass E: kx bins -> real rows (y = 4by + y_l, z = 4bz + z_l) ----------------
 template <int G>
-__global__ void __launch_bounds__(kFftThreads) k_pass_d(const float2* __restrict__ specB, float2* __restrict__ specA,
+__global__ void __launch_bounds__(kFftThreads) k_pass_e(const float2* __restrict__ spec, float* __restrict__ phi,
                                                         const float2* __restrict__ tw_g) {
-    using T = Tiles<G>;
-    constexpr int P = T::P, TZ = T::TZ, LS = T::LSG;
+    using T = Geo<G>;
+    constexpr int H = T::H, NBX = T::NBX;
+    constexpr int ITEMS = NBX * 32;
+    constexpr int PER = (ITEMS + kFftThreads - 1) / kFftThreads;
     extern __shared__ float2 sm[];
     float2* tw = sm;
     float2* s = sm + G;
-    const int z0 = blockIdx.x * TZ, kx = blockIdx.y;
+    const int by = blockIdx.x, bz = blockIdx.y;
     for (int i = threadIdx.x; i < G; i += kFftThreads) tw[i] = tw_g[i];
-    for (int t = threadIdx.x; t < TZ * G; t += kFftThreads) {
-        const int l = t % TZ, ky = t / TZ;
-        s[l * LS + fft::pad(ky)] = specB[((size_t)kx * G + ky) * G + z0 + l];
+    float4 v[PER];
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+        const int u = threadIdx.x + p * kFftThreads;
+        if (ITEMS % kFftThreads == 0 || u < ITEMS)
+            v[p] = *reinterpret_cast<const float4*>(spec + T::brick(u >> 5, by, bz) + 2 * (u & 31));
     }
-    __syncthreads();
-    fft::lines<G, TZ, LS, kFftThreads, 1, true>(s, tw);
-    for (int t = threadIdx.x; t < TZ * G; t += kFftThreads) {
-        const int l = t / G, y = t % G;
-        specA[((size_t)(z0 + l) * P + kx) * G + y] = s[l * LS + fft::pad(y)];
-    }
-}
-
-template <int G>
-__global__ void __launch_bounds__(kFftThreads) k_pass_e(const float2* __restrict__ specA, float* __restrict__ phi,
-                                                        const float2* __restrict__ tw_g) {
-    using T = Tiles<G>;
-    constexpr int H = T::H, P = T::P, TY = T::TY, LS = T::LSH;
-    extern __shared__ float2 sm[];
-    float2* tw = sm;
-    float2* s = sm + G;
-    const int y0 = blockIdx.x * TY, z = blockIdx.y;
-    for (int i = threadIdx.x; i < G; i += kFftThreads) tw[i] = tw_g[i];
-    for (int t = threadIdx.x; t < P * TY; t += kFftThreads) {
-        const int kx = t / TY, yy = t % TY;
-        s[yy * LS + fft::pad(kx)] = specA[((size_t)z * P + kx) * G + y0 + yy];
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+        const int u = threadIdx.x + p * kFftThreads;
+        if (ITEMS % kFftThreads == 0 || u < ITEMS) {
+            const int bx = u >> 5, c = u & 31;
+            const int l = (c >> 3) * 4 + ((c >> 1) & 3), kx = bx * 4 + (c & 1) * 2;
+            s[kx * 16 + l] = make_float2(v[p].x, v[p].y);
+            s[(kx + 1) * 16 + l] = make_float2(v[p].z, v[p].w);
+        }
     }
     __syncthreads();
     // X -> Z, pairs (k, H-k) in place:
     //   Z[k] = E + i O,  E = X[k] + conj X[H-k],  O = (X[k] - conj X[H-k]) * exp(+2 pi i k / G)
     // (imaginary parts of the k = 0 and k = H bins are dropped, as a C2R transform does)
-    constexpr int HP = H / 2 + 1;
-    for (int t = threadIdx.x; t < TY * HP; t += kFftThreads) {
-        const int yy = t / HP, k = t % HP;
-        float2* line = s + yy * LS;
-        float2 a = line[fft::pad(k)], b = line[fft::pad(H - k)];
+    constexpr int PAIRS = 16 * (H / 2 + 1);
+    for (int u = threadIdx.x; u < PAIRS; u += kFftThreads) {
+        const int l = u & 15, k = u >> 4;
+        float2 a = s[k * 16 + l], b = s[(H - k) * 16 + l];
         if (k == 0) { a.y = 0.f; b.y = 0.f; }
         {
             const float2 w = tw[k];
             const float er = a.x + b.x, ei = a.y - b.y, dr = a.x - b.x, di = a.y + b.y;
             const float orr = dr * w.x + di * w.y, oi = di * w.x - dr * w.y;
-            line[fft::pad(k)] = make_float2(er - oi, ei + orr);
+            s[k * 16 + l] = make_float2(er - oi, ei + orr);
         }
         if (k != 0 && 2 * k != H) {
             const float2 w = tw[H - k];
             const float er = b.x + a.x, ei = b.y - a.y, dr = b.x - a.x, di = b.y + a.y;
             const float orr = dr * w.x + di * w.y, oi = di * w.x - dr * w.y;
-            line[fft::pad(H - k)] = make_float2(er - oi, ei + orr);
+            s[(H - k) * 16 + l] = make_float2(er - oi, ei + orr);
         }
     }
     __syncthreads();
-    fft::lines<H, TY, LS, kFftThreads, 2, true>(s, tw);
-    for (int t = threadIdx.x; t < TY * H; t += kFftThreads) {
-        const int yy = t / H, m = t % H;
-        reinterpret_cast<float2*>(phi + ((size_t)z * G + y0 + yy) * G)[m] = s[yy * LS + fft::pad(m)];
+    fft::lines16<H, kFftThreads, 2, true>(s, tw);
+    for (int u = threadIdx.x; u < 16 * (H / 2); u += kFftThreads) {
+        const int l = u & 15, mp = u >> 4;
+        const size_t row = ((size_t)(bz * 4 + (l >> 2)) * G + by * 4 + (l & 3)) * G;
+        const float2 a = s[(2 * mp) * 16 + l], b = s[(2 * mp + 1) * 16 + l];
+        *reinterpret_cast<float4*>(phi + row + 4 * mp) = make_float4(a.x, a.y, b.x, b.y);
     }
 }
 
 template <int G>
 struct Launcher {
-    using T = Tiles<G>;
-    static size_t smem_a() { return sizeof(float2) * ((size_t)G + (size_t)T::TY * T::LSH); }
-    static size_t smem_b() { return sizeof(float2) * ((size_t)G + (size_t)T::TZ * T::LSG); }
-    static size_t smem_c() { return sizeof(float2) * ((size_t)G + (T::H + 2) / 2 + 1 + (size_t)T::LC * T::LSG); }
+    using T = Geo<G>;
+    static size_t smem_ae() { return sizeof(float2) * ((size_t)G + 16 * (size_t)T::PX); }
+    static size_t smem_bd() { return sizeof(float2) * ((size_t)G + 16 * (size_t)G); }
+    static size_t smem_c() { return sizeof(float2) * ((size_t)G + (T::H + 2) / 2 + 1 + 16 * (size_t)G); }
+    // the line buffer (16 * PX float2) overlays the 32-bit sum words (2 * 16 * G)
+    static size_t smem_dep() {
+        const size_t lines = sizeof(float2) * 16 * (size_t)T::PX, sums = 2 * sizeof(unsigned) * 16 * (size_t)G;
+        return sizeof(float2) * (size_t)G + (lines > sums ? lines : sums);
+    }
 
     static int configure() {
-        static bool done = false;
-        if (done) return SD_OK;
         int rc = SD_OK;
-        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a()));
-        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_b<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b()));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a<G, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ae()));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a<G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ae()));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_y<G, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem_bd()));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_y<G, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem_bd()));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_c<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c()));
-        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_d<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b()));
-        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_e<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a()));
-        if (rc == SD_OK) done = true;
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_e<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ae()));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a_deposit<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem_dep()));
         return rc == SD_OK ? SD_OK : SD_E_CUDA;
     }
 
-    static int run(const PoissonPlan& p, const long long* acc, const float* rho, int clear, float* keep, float2* A,
-                   float2* B, float* phi, cudaStream_t s) {
-        int rc = configure();
-        if (rc != SD_OK) return rc;
-        k_pass_a<G><<<dim3(G / T::TY, G), kFftThreads, smem_a(), s>>>(acc, rho, clear, keep, A, p.tw);
+    static int run(const PoissonPlan& p, const long long* acc, const float* rho, const float4* pos,
+                   const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s) {
+        const dim3 grid_rows(T::NBY, T::NBZ), grid_y(T::NBX, T::NBZ), grid_z(T::NBX, T::NBY);
+        if (pos)
+            k_pass_a_deposit<G><<<grid_rows, kDepositThreads, smem_dep(), s>>>(pos, row_start, keep, spec, p.tw);
+        else if (acc)
+            k_pass_a<G, 1><<<grid_rows, kFftThreads, smem_ae(), s>>>(nullptr, const_cast<long long*>(acc), keep, spec,
+                                                                     p.tw);
+        else
+            k_pass_a<G, 0><<<grid_rows, kFftThreads, smem_ae(), s>>>(rho, nullptr, keep, spec, p.tw);
         SD_LAUNCHED(s);
-        k_pass_b<G><<<dim3(G / T::TZ, T::P), kFftThreads, smem_b(), s>>>(A, B, p.tw);
+        k_pass_y<G, false><<<grid_y, kFftThreads, smem_bd(), s>>>(spec, p.tw);
         SD_LAUNCHED(s);
-        k_pass_c<G><<<dim3(G / T::LC, T::P), kFftThreads, smem_c(), s>>>(B, p.tw, p.gexp, p.scale);
+        k_pass_c<G><<<grid_z, kFftThreads, smem_c(), s>>>(spec, p.tw, p.gexp, p.scale);
         SD_LAUNCHED(s);
-        k_pass_d<G><<<dim3(G / T::TZ, T::P), kFftThreads, smem_b(), s>>>(B, A, p.tw);
+        k_pass_y<G, true><<<grid_y, kFftThreads, smem_bd(), s>>>(spec, p.tw);
         SD_LAUNCHED(s);
-        k_pass_e<G><<<dim3(G / T::TY, G), kFftThreads, smem_a(), s>>>(A, phi, p.tw);
+        k_pass_e<G><<<grid_rows, kFftThreads, smem_ae(), s>>>(spec, phi, p.tw);
         SD_LAUNCHED(s);
         return SD_OK;
     }
 };
 
-}  // namespace
-
-size_t poisson_spectrum_elems(int G) { return (size_t)G * G * (size_t)(G / 2 + 1); }
-
-static int poisson_configure(int G) {
+int poisson_configure(int G) {
     switch (G) {
         case 16: return Launcher<16>::configure();
         case 32: return Launcher<32>::configure();
@@ -265,6 +509,10 @@ static int poisson_configure(int G) {
         default: return fail(SD_E_UNSUPPORTED, "poisson: grid size %d not supported", G);
     }
 }
+
+}  // namespace
+
+size_t poisson_spectrum_elems(int G) { return (size_t)G * G * (size_t)(G / 2 + 4); }
 
 int poisson_plan_build(PoissonPlan& p, int G, float soft) {
     if (p.G == G && p.soft == soft && p.tw) return SD_OK;
@@ -299,15 +547,20 @@ void poisson_plan_free(PoissonPlan& p) {
     p.G = 0;
 }
 
-int launch_poisson(const PoissonPlan& p, const long long* acc, const float* rho, int clear, float* keep, float2* A,
-                   float2* B, float* phi, cudaStream_t s) {
+int launch_poisson(const PoissonPlan& p, const long long* acc, const float* rho, float* keep, float2* spec,
+                   float* phi, cudaStream_t s) {
+    return launch_poisson_ex(p, acc, rho, nullptr, nullptr, keep, spec, phi, s);
+}
+
+int launch_poisson_ex(const PoissonPlan& p, const long long* acc, const float* rho, const float4* pos,
+                      const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s) {
     switch (p.G) {
-        case 16: return Launcher<16>::run(p, acc, rho, clear, keep, A, B, phi, s);
-        case 32: return Launcher<32>::run(p, acc, rho, clear, keep, A, B, phi, s);
-        case 64: return Launcher<64>::run(p, acc, rho, clear, keep, A, B, phi, s);
-        case 128: return Launcher<128>::run(p, acc, rho, clear, keep, A, B, phi, s);
-        case 256: return Launcher<256>::run(p, acc, rho, clear, keep, A, B, phi, s);
-        case 512: return Launcher<512>::run(p, acc, rho, clear, keep, A, B, phi, s);
+        case 16: return Launcher<16>::run(p, acc, rho, pos, row_start, keep, spec, phi, s);
+        case 32: return Launcher<32>::run(p, acc, rho, pos, row_start, keep, spec, phi, s);
+        case 64: return Launcher<64>::run(p, acc, rho, pos, row_start, keep, spec, phi, s);
+        case 128: return Launcher<128>::run(p, acc, rho, pos, row_start, keep, spec, phi, s);
+        case 256: return Launcher<256>::run(p, acc, rho, pos, row_start, keep, spec, phi, s);
+        case 512: return Launcher<512>::run(p, acc, rho, pos, row_start, keep, spec, phi, s);
         default: return fail(SD_E_UNSUPPORTED, "poisson: grid size %d not supported", p.G);
     }
 }

@@ -84,7 +84,8 @@ struct sd_sim {
     void* sort_ws = nullptr;
     size_t sort_ws_bytes = 0;
     long long* acc = nullptr;
-    float2 *specA = nullptr, *specB = nullptr;
+    int* row_start = nullptr;    // key-space row starts of the sorted particles (tiled order)
+    float2* spec = nullptr;     // bricked spectrum, transformed in place
     float* phi = nullptr;
     float* rho = nullptr;        // kept density (keep_density)
     double* partials = nullptr;  // gather / energy / reduction partials
@@ -175,7 +176,7 @@ void free_buffers(sd_sim* s) {
     if (s->sort_ws) cudaFree(s->sort_ws);
     s->sort_ws = nullptr;
     s->sort_ws_bytes = 0;
-    free_dev(s->acc); free_dev(s->specA); free_dev(s->specB); free_dev(s->phi); free_dev(s->rho);
+    free_dev(s->acc); free_dev(s->row_start); free_dev(s->spec); free_dev(s->phi); free_dev(s->rho);
     free_dev(s->partials); free_dev(s->mom); free_dev(s->mean);
     poisson_plan_free(s->plan);
     if (s->graph) cudaGraphExecDestroy(s->graph);
@@ -200,7 +201,7 @@ size_t estimate_bytes(int n, int G) {
     b += (sizeof(uint32_t) * 3 + sizeof(int32_t) * 2) * N;
     b += sort_workspace_bytes((int)N);
     b += sizeof(long long) * cells;                    // fixed-point deposit
-    b += 2 * sizeof(float2) * poisson_spectrum_elems(G);
+    b += sizeof(float2) * poisson_spectrum_elems(G);
     b += sizeof(float) * cells * 2;                    // phi, kept density
     b += sizeof(double) * 8 * (gather_partials((int)N) + 1024);
     return b;
@@ -225,8 +226,8 @@ int allocate(sd_sim* s) {
         rc = fail(SD_E_NOMEM, "cudaMalloc of sort workspace failed");
     }
     rc = rc ? rc : alloc_dev(s->acc, cells);
-    rc = rc ? rc : alloc_dev(s->specA, poisson_spectrum_elems(s->G));
-    rc = rc ? rc : alloc_dev(s->specB, poisson_spectrum_elems(s->G));
+    rc = rc ? rc : alloc_dev(s->row_start, (size_t)s->G * s->G + 1);
+    rc = rc ? rc : alloc_dev(s->spec, poisson_spectrum_elems(s->G));
     rc = rc ? rc : alloc_dev(s->phi, cells);
     if (!rc && s->cfg.keep_density) rc = alloc_dev(s->rho, cells);
     s->partials_count = 8 * (gather_partials(s->N) + 1024);
@@ -311,7 +312,7 @@ int do_sort(sd_sim* s, int32_t* perm_out_dev) {
 int do_field(sd_sim* s, bool keep) {
     int rc = launch_deposit_fixed(s->pos, s->N, s->G, s->acc, s->stream);
     if (rc) return rc;
-    rc = launch_poisson(s->plan, s->acc, nullptr, 1, keep ? s->rho : nullptr, s->specA, s->specB, s->phi, s->stream);
+    rc = launch_poisson(s->plan, s->acc, nullptr, keep ? s->rho : nullptr, s->spec, s->phi, s->stream);
     if (rc) return rc;
     if (keep) s->rho_valid = true;
     return SD_OK;
@@ -332,10 +333,17 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     if (sort && (rc = do_sort(s, nullptr))) return sim_error(s, rc);
     if (timed) cudaEventRecord(s->ev[1], s->stream);
     const bool keep = s->cfg.keep_density && s->rho;
-    if ((rc = launch_deposit_fixed(s->pos, s->N, s->G, s->acc, s->stream))) return sim_error(s, rc);
+    // Tiled order right after a sort: the first FFT pass deposits the particles
+    // itself from the row table. Otherwise: int64 atomics, then the FFT.
+    const bool fused = sort && s->cfg.order == SD_ORDER_TILED;
+    if (fused) {
+        if ((rc = launch_row_bounds(s->keys2, s->N, s->G * s->G, s->row_start, s->stream))) return sim_error(s, rc);
+    } else if ((rc = launch_deposit_fixed(s->pos, s->N, s->G, s->acc, s->stream))) {
+        return sim_error(s, rc);
+    }
     if (timed) cudaEventRecord(s->ev[2], s->stream);
-    if ((rc = launch_poisson(s->plan, s->acc, nullptr, 1, keep ? s->rho : nullptr, s->specA, s->specB, s->phi,
-                             s->stream)))
+    if ((rc = launch_poisson_ex(s->plan, fused ? nullptr : s->acc, nullptr, fused ? s->pos : nullptr, s->row_start,
+                                keep ? s->rho : nullptr, s->spec, s->phi, s->stream)))
         return sim_error(s, rc);
     if (keep) s->rho_valid = true;
     if (timed) cudaEventRecord(s->ev[3], s->stream);
@@ -956,7 +964,7 @@ int sd_deposit(const float* pos, int n, int G, float* rho, void* ws, size_t ws_b
     return rc;
 }
 
-size_t sd_poisson_workspace_bytes(int G) { return 2 * align_up(sizeof(float2) * poisson_spectrum_elems(G), 256); }
+size_t sd_poisson_workspace_bytes(int G) { return align_up(sizeof(float2) * poisson_spectrum_elems(G), 256); }
 
 int sd_poisson(const float* rho, int G, float soft, float* phi, void* ws, size_t ws_bytes, void* stream) {
     if (!rho || !phi || !ws || G < 16 || G > 512 || (G & (G - 1))) return fail(SD_E_ARG, "poisson: bad arguments");
@@ -979,9 +987,7 @@ int sd_poisson(const float* rho, int G, float soft, float* phi, void* ws, size_t
             cache.push_back(plan);
         }
     }
-    float2* A = reinterpret_cast<float2*>(ws);
-    float2* B = reinterpret_cast<float2*>((char*)ws + align_up(sizeof(float2) * poisson_spectrum_elems(G), 256));
-    return launch_poisson(*plan, nullptr, rho, 0, nullptr, A, B, phi, (cudaStream_t)stream);
+    return launch_poisson(*plan, nullptr, rho, nullptr, reinterpret_cast<float2*>(ws), phi, (cudaStream_t)stream);
 }
 
 size_t sd_gather_workspace_bytes(int n) { return sizeof(double) * 4 * gather_partials(n); }

@@ -252,7 +252,24 @@ __global__ void k_copy_keys(const uint32_t* __restrict__ kin, const int32_t* __r
     vout[i] = vin ? vin[i] : i;
 }
 
+// Thread i writes row_start[r] = i for every key-space row r in
+// [keys[i-1], keys[i]) (keys are key+1, so empty slots never start a row); the
+// last thread closes the tail up to `rows` with n.
+__global__ void k_row_bounds(const uint32_t* __restrict__ keys, int n, int rows, int* __restrict__ row_start) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    const int lo = (i == 0) ? 0 : (int)min(keys[i - 1], (uint32_t)rows);
+    const int hi = (i == n) ? rows + 1 : (int)min(keys[i], (uint32_t)rows);
+    for (int r = lo; r < hi; ++r) row_start[r] = i;
+}
+
 }  // namespace
+
+int launch_row_bounds(const uint32_t* keys, int n, int rows, int* row_start, cudaStream_t s) {
+    k_row_bounds<<<(n + 1 + 255) / 256, 256, 0, s>>>(keys, n, rows, row_start);
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
 
 int launch_cell_keys(const float4* pos, int n, int G, int order, uint32_t* keys, cudaStream_t s) {
     if (n <= 0) return SD_OK;

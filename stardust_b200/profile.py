@@ -22,7 +22,7 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--stage", choices=["step", "poisson"], default="step")
     ap.add_argument("--grid", type=int, default=512)
-    ap.add_argument("--order", type=int, default=0)
+    ap.add_argument("--order", type=int, default=2)
     a = ap.parse_args(argv)
 
     import torch
