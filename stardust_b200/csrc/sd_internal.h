@@ -54,14 +54,19 @@ int launch_poisson(const PoissonPlan& p, const long long* rho_fixed, const float
 // pos != nullptr: the first pass deposits the particles itself (SD_ORDER_TILED
 // order, row_start from launch_row_bounds) instead of reading a density grid.
 int launch_poisson_ex(const PoissonPlan& p, const long long* rho_fixed, const float* rho_float, const float4* pos,
-                      const int* row_start, float* rho_keep, float2* spec, float* phi, cudaStream_t s);
+                      const int* perm, const int* row_start, float* rho_keep, float2* spec, float* phi,
+                      cudaStream_t s);
 // row_start[r] = first index i with sorted keys_plus1[i] > r, for r in [0, rows]
 int launch_row_bounds(const uint32_t* keys_plus1, int n, int rows, int* row_start, cudaStream_t s);
 
 size_t gather_partials(int n);
-int launch_gather_kick_drift(const float* phi, int G, float pot_scale, float4* pos, float4* vel, int n,
-                             float dt_kick, float dt_drift, float c2, const float* mean_vel,
-                             double* partials, double* mom_out, float* mean_out, cudaStream_t s);
+// perm != nullptr: slot i takes input particle perm[i] (fused reorder) and the
+// outputs must be separate arrays; otherwise pos_out/vel_out may alias the inputs.
+// keys_out (optional) receives the next step's order keys (key + 1).
+int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const float4* pos_in, const float4* vel_in,
+                             const int* perm, float4* pos_out, float4* vel_out, uint32_t* keys_out, int order, int n,
+                             float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
+                             double* mom_out, float* mean_out, cudaStream_t s);
 int launch_interpolate_accel(const float* phi, int G, float pot_scale, const float4* pos, float4* acc, int n,
                              cudaStream_t s);
 int launch_apply_mean(float4* vel, const float4* pos, int n, const float* mean_vel, cudaStream_t s);

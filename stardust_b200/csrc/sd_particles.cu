@@ -150,18 +150,30 @@ __device__ __forceinline__ void block_sum4(double v0, double v1, double v2, doub
 // One thread per particle, grid-stride over at most kGatherMaxBlocks blocks so the
 // per-block FP64 partials stay few; the block-to-particle assignment depends only
 // on n, so the sums are deterministic.
-__global__ void __launch_bounds__(kGatherThreads) k_gather_kick_drift(const float* __restrict__ phi, int G, float h,
-                                                                      float4* __restrict__ pos, float4* __restrict__ vel,
-                                                                      int n, float dt_kick, float dt_drift, float c2,
-                                                                      const float* __restrict__ mean_vel,
-                                                                      double* __restrict__ partials) {
+//
+// With perm != nullptr the kernel also performs the sort's reorder
+// (kReorder, Sim.cu:2488-2495): slot i takes particle perm[i] of the input
+// arrays and the results go to separate output arrays. keys_out (optional)
+// receives the order key of each new position for the next step's sort.
+__global__ void __launch_bounds__(kGatherThreads) k_gather_kick_drift(
+    const float* __restrict__ phi, int G, float h, const float4* pos_in, const float4* vel_in,
+    const int* __restrict__ perm, float4* pos_out, float4* vel_out, uint32_t* __restrict__ keys_out, int order, int n,
+    float dt_kick, float dt_drift, float c2, const float* __restrict__ mean_vel, double* __restrict__ partials) {
     double sx = 0.0, sy = 0.0, sz = 0.0, cnt = 0.0;
     const float mx = mean_vel ? mean_vel[0] : 0.f, my = mean_vel ? mean_vel[1] : 0.f,
                 mz = mean_vel ? mean_vel[2] : 0.f;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float4 p = pos[i];
-        if (p.x < 0.f) continue;
-        float4 v = vel[i];
+        const int j = perm ? perm[i] : i;
+        float4 p = pos_in[j];
+        float4 v = vel_in[j];
+        if (p.x < 0.f) {
+            if (perm) {
+                pos_out[i] = p;
+                vel_out[i] = v;
+            }
+            if (keys_out) keys_out[i] = 0u;
+            continue;
+        }
         if (mean_vel) {
             v.x = __fsub_rn(v.x, mx);
             v.y = __fsub_rn(v.y, my);
@@ -185,15 +197,17 @@ __global__ void __launch_bounds__(kGatherThreads) k_gather_kick_drift(const floa
         p.z = __fmaf_rn(v.z, dt_drift, p.z);
         if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z) || !isfinite(v.x) || !isfinite(v.y) ||
             !isfinite(v.z)) {
-            pos[i] = make_float4(-1.f, -1.f, -1.f, 0.f);
-            vel[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            pos_out[i] = make_float4(-1.f, -1.f, -1.f, 0.f);
+            vel_out[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (keys_out) keys_out[i] = 0u;
             continue;
         }
         p.x = __fsub_rn(p.x, floorf(p.x));
         p.y = __fsub_rn(p.y, floorf(p.y));
         p.z = __fsub_rn(p.z, floorf(p.z));
-        pos[i] = p;
-        vel[i] = v;
+        pos_out[i] = p;
+        vel_out[i] = v;
+        if (keys_out) keys_out[i] = order_key_plus1(p, G, order);
         sx += v.x;
         sy += v.y;
         sz += v.z;
@@ -411,14 +425,15 @@ size_t gather_partials(int n) {
     return (size_t)(b < 1 ? 1 : (b > kGatherMaxBlocks ? kGatherMaxBlocks : b));
 }
 
-int launch_gather_kick_drift(const float* phi, int G, float pot_scale, float4* pos, float4* vel, int n,
+int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const float4* pos_in, const float4* vel_in,
+                             const int* perm, float4* pos_out, float4* vel_out, uint32_t* keys_out, int order, int n,
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
                              double* mom_out, float* mean_out, cudaStream_t s) {
     if (n <= 0) return SD_OK;
     const float h = (0.5f * (float)G) * pot_scale;  // Sim.cu:604
     const int blocks = (int)gather_partials(n);
-    k_gather_kick_drift<<<blocks, kGatherThreads, 0, s>>>(phi, G, h, pos, vel, n, dt_kick, dt_drift, c2, mean_vel,
-                                                          partials);
+    k_gather_kick_drift<<<blocks, kGatherThreads, 0, s>>>(phi, G, h, pos_in, vel_in, perm, pos_out, vel_out, keys_out,
+                                                          order, n, dt_kick, dt_drift, c2, mean_vel, partials);
     SD_LAUNCHED(s);
     if (partials && (mom_out || mean_out)) {
         k_finalize_mean<<<1, 256, 0, s>>>(partials, blocks, mom_out, mean_out);

@@ -140,6 +140,7 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_a(const float* __restrict_
 // independent of the order of the adds; no density grid is written.
 template <int G>
 __global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4* __restrict__ pos,
+                                                                    const int* __restrict__ perm,
                                                                     const int* __restrict__ row_start,
                                                                     float* __restrict__ rho_keep,
                                                                     float2* __restrict__ spec,
@@ -182,6 +183,7 @@ __global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4
     }
     __syncthreads();
     const int total = range_off[25];
+    const bool split16 = total < 65536;
     int r = 0;
     // Loads are issued kBatch at a time so several particles are in flight per
     // thread before the shared-memory adds.
@@ -193,7 +195,8 @@ __global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4
             const int f = f0 + b * NT;
             if (f < total) {
                 while (f >= range_off[r + 1]) ++r;
-                pb[b] = pos[range_lo[r] + (f - range_off[r])];
+                const int idx = range_lo[r] + (f - range_off[r]);
+                pb[b] = pos[perm ? perm[idx] : idx];
             }
         }
 #pragma unroll
@@ -215,16 +218,23 @@ __global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4
                 const int rowc = (zl * 4 + yl) * G;
 #pragma unroll
                 for (int ox = 0; ox < 2; ++ox) {
-                    // q in [0, 2^32]: add the low word and carry into the high word.
-                    // atomicAdd returns the previous low word, so every wrap is seen
-                    // by exactly one add and the 64-bit total is exact.
                     const unsigned long long q =
                         (unsigned long long)fixed_weight(cic_weight(ox | (oy << 1) | (oz << 2), fx, fy, fz));
                     const int c = rowc + (ox ? x1 : x0);
-                    const unsigned lo = (unsigned)q;
-                    const unsigned old = atomicAdd(acc_lo + c, lo);
-                    const unsigned up = (unsigned)(q >> 32) + ((old + lo < old) ? 1u : 0u);
-                    if (up) atomicAdd(acc_hi + c, up);
+                    if (split16) {
+                        // q in [0, 2^32] as (q >> 16) * 2^16 + (q & 0xffff): with fewer than
+                        // 2^16 particles in the tile neither 32-bit sum can overflow, so two
+                        // plain adds (no returned value) keep the 64-bit total exact.
+                        atomicAdd(acc_hi + c, (unsigned)(q >> 16));
+                        atomicAdd(acc_lo + c, (unsigned)(q & 0xffffu));
+                    } else {
+                        // add the low word and carry into the high word; atomicAdd returns the
+                        // previous low word, so every wrap is seen by exactly one add
+                        const unsigned lo = (unsigned)q;
+                        const unsigned old = atomicAdd(acc_lo + c, lo);
+                        const unsigned up = (unsigned)(q >> 32) + ((old + lo < old) ? 1u : 0u);
+                        if (up) atomicAdd(acc_hi + c, up);
+                    }
                 }
             }
         }
@@ -242,10 +252,11 @@ __global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4
             const int l = u & 15, mp = u >> 4;
             const uint4 lo = *reinterpret_cast<const uint4*>(acc_lo + l * G + 4 * mp);
             const uint4 hi = *reinterpret_cast<const uint4*>(acc_hi + l * G + 4 * mp);
-            cv[p] = make_float4(fixed_to_float((long long)(((unsigned long long)hi.x << 32) | lo.x)),
-                                fixed_to_float((long long)(((unsigned long long)hi.y << 32) | lo.y)),
-                                fixed_to_float((long long)(((unsigned long long)hi.z << 32) | lo.z)),
-                                fixed_to_float((long long)(((unsigned long long)hi.w << 32) | lo.w)));
+            const int sh = split16 ? 16 : 32;
+            cv[p] = make_float4(fixed_to_float((long long)(((unsigned long long)hi.x << sh) + lo.x)),
+                                fixed_to_float((long long)(((unsigned long long)hi.y << sh) + lo.y)),
+                                fixed_to_float((long long)(((unsigned long long)hi.z << sh) + lo.z)),
+                                fixed_to_float((long long)(((unsigned long long)hi.w << sh) + lo.w)));
         }
     }
     __syncthreads();
@@ -462,6 +473,15 @@ struct Launcher {
 
     static int configure() {
         int rc = SD_OK;
+        // prefer the largest shared-memory carveout so several 70 KB CTAs fit per SM
+        const int carve = (int)cudaSharedmemCarveoutMaxShared;
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a<G, 0>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a<G, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_y<G, false>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_y<G, true>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_c<G>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_e<G>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a_deposit<G>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a<G, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ae()));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a<G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ae()));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_y<G, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -475,11 +495,11 @@ struct Launcher {
         return rc == SD_OK ? SD_OK : SD_E_CUDA;
     }
 
-    static int run(const PoissonPlan& p, const long long* acc, const float* rho, const float4* pos,
+    static int run(const PoissonPlan& p, const long long* acc, const float* rho, const float4* pos, const int* perm,
                    const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s) {
         const dim3 grid_rows(T::NBY, T::NBZ), grid_y(T::NBX, T::NBZ), grid_z(T::NBX, T::NBY);
         if (pos)
-            k_pass_a_deposit<G><<<grid_rows, kDepositThreads, smem_dep(), s>>>(pos, row_start, keep, spec, p.tw);
+            k_pass_a_deposit<G><<<grid_rows, kDepositThreads, smem_dep(), s>>>(pos, perm, row_start, keep, spec, p.tw);
         else if (acc)
             k_pass_a<G, 1><<<grid_rows, kFftThreads, smem_ae(), s>>>(nullptr, const_cast<long long*>(acc), keep, spec,
                                                                      p.tw);
@@ -549,18 +569,18 @@ void poisson_plan_free(PoissonPlan& p) {
 
 int launch_poisson(const PoissonPlan& p, const long long* acc, const float* rho, float* keep, float2* spec,
                    float* phi, cudaStream_t s) {
-    return launch_poisson_ex(p, acc, rho, nullptr, nullptr, keep, spec, phi, s);
+    return launch_poisson_ex(p, acc, rho, nullptr, nullptr, nullptr, keep, spec, phi, s);
 }
 
 int launch_poisson_ex(const PoissonPlan& p, const long long* acc, const float* rho, const float4* pos,
-                      const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s) {
+                      const int* perm, const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s) {
     switch (p.G) {
-        case 16: return Launcher<16>::run(p, acc, rho, pos, row_start, keep, spec, phi, s);
-        case 32: return Launcher<32>::run(p, acc, rho, pos, row_start, keep, spec, phi, s);
-        case 64: return Launcher<64>::run(p, acc, rho, pos, row_start, keep, spec, phi, s);
-        case 128: return Launcher<128>::run(p, acc, rho, pos, row_start, keep, spec, phi, s);
-        case 256: return Launcher<256>::run(p, acc, rho, pos, row_start, keep, spec, phi, s);
-        case 512: return Launcher<512>::run(p, acc, rho, pos, row_start, keep, spec, phi, s);
+        case 16: return Launcher<16>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s);
+        case 32: return Launcher<32>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s);
+        case 64: return Launcher<64>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s);
+        case 128: return Launcher<128>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s);
+        case 256: return Launcher<256>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s);
+        case 512: return Launcher<512>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s);
         default: return fail(SD_E_UNSUPPORTED, "poisson: grid size %d not supported", p.G);
     }
 }

@@ -21,6 +21,7 @@
 
 #include <atomic>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "sd_internal.h"
@@ -94,6 +95,7 @@ struct sd_sim {
     float* mean = nullptr;       // 4 floats: pending mean velocity; [3] = max speed scratch
     bool mean_pending = false;
     bool rho_valid = false;
+    bool keys_valid = false;     // keys hold the order keys of the current pos order
     PoissonPlan plan;
 
     // leapfrog
@@ -110,7 +112,8 @@ struct sd_sim {
     // captured steps for sd_steps
     cudaGraphExec_t graph = nullptr;
     float graph_dt = 0.f;
-    long long graph_launches = 0;  // kernels inside one replay
+    const float4* graph_pos = nullptr;  // particle buffer the graph's first step reads
+    long long graph_launches = 0;       // kernels inside one replay
 };
 
 namespace {
@@ -303,8 +306,9 @@ int do_sort(sd_sim* s, int32_t* perm_out_dev) {
     if (perm_out_dev &&
         SD_CUDA(cudaMemcpyAsync(perm_out_dev, s->vals, sizeof(int32_t) * s->N, cudaMemcpyDeviceToDevice, s->stream)))
         return SD_E_CUDA;
-    float4* t = s->pos; s->pos = s->pos2; s->pos2 = t;
-    t = s->vel; s->vel = s->vel2; s->vel2 = t;
+    std::swap(s->pos, s->pos2);
+    std::swap(s->vel, s->vel2);
+    s->keys_valid = false;
     return SD_OK;
 }
 
@@ -330,11 +334,22 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     int rc = SD_OK;
     if (timed && (rc = ensure_events(s))) return sim_error(s, rc);
     if (timed) cudaEventRecord(s->ev[0], s->stream);
-    if (sort && (rc = do_sort(s, nullptr))) return sim_error(s, rc);
+    // Sort (sortParticles, Sim.cu:3656-3671): keys come from the previous step's
+    // gather; the permutation is applied by the deposit and gather reads, so no
+    // separate reorder pass runs.
+    const int32_t* perm = nullptr;
+    if (sort) {
+        if (!s->keys_valid && (rc = launch_cell_keys(s->pos, s->N, s->G, s->cfg.order, s->keys, s->stream)))
+            return sim_error(s, rc);
+        rc = launch_sort_pairs(s->keys, nullptr, s->keys2, s->vals, s->keys3, s->vals2, s->N,
+                               key_bits_for(s->G, s->cfg.order), s->sort_ws, s->sort_ws_bytes, s->stream);
+        if (rc) return sim_error(s, rc);
+        perm = s->vals;
+    }
     if (timed) cudaEventRecord(s->ev[1], s->stream);
     const bool keep = s->cfg.keep_density && s->rho;
     // Tiled order right after a sort: the first FFT pass deposits the particles
-    // itself from the row table. Otherwise: int64 atomics, then the FFT.
+    // itself from the row table. Otherwise: int64 atomics (any particle order).
     const bool fused = sort && s->cfg.order == SD_ORDER_TILED;
     if (fused) {
         if ((rc = launch_row_bounds(s->keys2, s->N, s->G * s->G, s->row_start, s->stream))) return sim_error(s, rc);
@@ -342,17 +357,25 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
         return sim_error(s, rc);
     }
     if (timed) cudaEventRecord(s->ev[2], s->stream);
-    if ((rc = launch_poisson_ex(s->plan, fused ? nullptr : s->acc, nullptr, fused ? s->pos : nullptr, s->row_start,
-                                keep ? s->rho : nullptr, s->spec, s->phi, s->stream)))
+    if ((rc = launch_poisson_ex(s->plan, fused ? nullptr : s->acc, nullptr, fused ? s->pos : nullptr, perm,
+                                s->row_start, keep ? s->rho : nullptr, s->spec, s->phi, s->stream)))
         return sim_error(s, rc);
     if (keep) s->rho_valid = true;
     if (timed) cudaEventRecord(s->ev[3], s->stream);
     const float c2 = light_speed_sq(s->cfg.length_scale, s->cfg.time_unit_scale);
     // The mean written last step is read here as the correction for the loaded
     // velocities; the finalize kernel then overwrites it with this step's mean.
-    rc = launch_gather_kick_drift(s->phi, s->G, pot_scale_of(s), s->pos, s->vel, s->N, dt_kick, dt_drift, c2,
-                                  s->mean, s->partials, s->mom, s->mean, s->stream);
+    float4* pos_out = perm ? s->pos2 : s->pos;
+    float4* vel_out = perm ? s->vel2 : s->vel;
+    rc = launch_gather_kick_drift(s->phi, s->G, pot_scale_of(s), s->pos, s->vel, perm, pos_out, vel_out, s->keys,
+                                  s->cfg.order, s->N, dt_kick, dt_drift, c2, s->mean, s->partials, s->mom, s->mean,
+                                  s->stream);
     if (rc) return sim_error(s, rc);
+    if (perm) {
+        std::swap(s->pos, s->pos2);
+        std::swap(s->vel, s->vel2);
+    }
+    s->keys_valid = true;
     s->mean_pending = true;
     if (timed) cudaEventRecord(s->ev[4], s->stream);
     s->ev_valid = timed;
@@ -390,6 +413,7 @@ int reconfigure(sd_sim* s, const sd_config* c) {
     const bool structural = !s->configured || c->particle_count != s->N || G != s->G ||
                             c->boundary != s->cfg.boundary || (c->keep_density && !s->rho);
     const bool soft_changed = c->softening_cells != s->cfg.softening_cells;
+    if (c->order != s->cfg.order) s->keys_valid = false;
     s->cfg = *c;
     s->cfg.grid_size = G;
     if (!structural) {
@@ -407,6 +431,7 @@ int reconfigure(sd_sim* s, const sd_config* c) {
     s->mean_pending = false;
     s->lf_open = false;
     s->rho_valid = false;
+    s->keys_valid = false;
     s->cuda_failed = false;
     return SD_OK;
 }
@@ -553,6 +578,7 @@ int sd_reset(sd_sim* s) {
     s->mean_pending = false;
     s->lf_open = false;
     s->rho_valid = false;
+    s->keys_valid = false;
     if (SD_CUDA(cudaMemsetAsync(s->mean, 0, sizeof(float) * 4, s->stream))) return SD_E_CUDA;
     return launch_hide_range(s->pos, s->vel, 0, s->N, s->stream);
 }
@@ -577,6 +603,7 @@ int sd_set_particles(sd_sim* s, const float* pos, const float* vel, int n, int w
     s->mean_pending = false;
     s->lf_open = false;
     s->rho_valid = false;
+    s->keys_valid = false;
     return SD_OK;
 }
 
@@ -687,9 +714,16 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
     }
     if (done >= nsteps) return SD_OK;
     const bool sort = s->cfg.sort_interval == 1;
+    // Keys are computed outside the graph, so replays never depend on them being stale.
+    if (sort && !s->keys_valid) {
+        int rc = launch_cell_keys(s->pos, s->N, s->G, s->cfg.order, s->keys, s->stream);
+        if (rc) return sim_error(s, rc);
+        s->keys_valid = true;
+    }
     // A captured graph covers two steps so the pos/pos2 ping-pong returns to the
-    // same buffers; it is rebuilt when dt changes.
-    if (!s->graph || s->graph_dt != dt) {
+    // same buffers; it is rebuilt when dt changes or the particles sit in the
+    // other buffer of the pair.
+    if (!s->graph || s->graph_dt != dt || s->graph_pos != s->pos) {
         if (s->graph) cudaGraphExecDestroy(s->graph);
         s->graph = nullptr;
         cudaGraph_t graph = nullptr;
@@ -699,6 +733,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
         const bool lf0 = s->lf_open;
         const float lfd = s->lf_dt_prev;
         const bool mp0 = s->mean_pending;
+        const bool kv0 = s->keys_valid;
         const long long l0 = launches();
         int rc = do_step(s, dt, sort, false);
         if (!rc) rc = do_step(s, dt, sort, false);
@@ -712,6 +747,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
         s->lf_open = lf0;
         s->lf_dt_prev = lfd;
         s->mean_pending = mp0;
+        s->keys_valid = kv0;
         if (rc) {
             if (graph) cudaGraphDestroy(graph);
             return rc;
@@ -721,6 +757,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
         cudaGraphDestroy(graph);
         if (SD_CUDA(e)) return sim_error(s, SD_E_CUDA);
         s->graph_dt = dt;
+        s->graph_pos = s->pos;
     }
     while (nsteps - done >= 2) {
         if (SD_CUDA(cudaGraphLaunch(s->graph, s->stream))) return sim_error(s, SD_E_CUDA);
@@ -728,6 +765,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
         s->sim_time += 2.0 * dt;
         s->step_count += 2;
         s->mean_pending = true;
+        s->keys_valid = true;
         if (s->cfg.integrator == SD_INT_KDK) {
             s->lf_open = true;
             s->lf_dt_prev = dt;
@@ -749,8 +787,9 @@ int sd_synchronize(sd_sim* s) {
     int rc = do_field(s, false);
     if (rc) return sim_error(s, rc);
     const float c2 = light_speed_sq(s->cfg.length_scale, s->cfg.time_unit_scale);
-    rc = launch_gather_kick_drift(s->phi, s->G, pot_scale_of(s), s->pos, s->vel, s->N, 0.5f * s->lf_dt_prev, 0.f,
-                                  c2, s->mean, s->partials, s->mom, s->mean, s->stream);
+    rc = launch_gather_kick_drift(s->phi, s->G, pot_scale_of(s), s->pos, s->vel, nullptr, s->pos, s->vel, s->keys,
+                                  s->cfg.order, s->N, 0.5f * s->lf_dt_prev, 0.f, c2, s->mean, s->partials, s->mom,
+                                  s->mean, s->stream);
     if (rc) return sim_error(s, rc);
     s->mean_pending = true;
     s->lf_open = false;
@@ -997,9 +1036,10 @@ int sd_gather_kick_drift(const float* phi, int G, float pot_scale, float* pos, f
                          void* stream) {
     if (!phi || !pos || !vel || n < 0 || G < 16 || (G & (G - 1))) return fail(SD_E_ARG, "gather: bad arguments");
     if (mom_out && (!ws || ws_bytes < sd_gather_workspace_bytes(n))) return fail(SD_E_ARG, "gather: workspace too small");
-    return launch_gather_kick_drift(phi, G, pot_scale, reinterpret_cast<float4*>(pos), reinterpret_cast<float4*>(vel),
-                                    n, dt_kick, dt_drift, c2, mean_vel, mom_out ? (double*)ws : nullptr, mom_out,
-                                    nullptr, (cudaStream_t)stream);
+    float4* p4 = reinterpret_cast<float4*>(pos);
+    float4* v4 = reinterpret_cast<float4*>(vel);
+    return launch_gather_kick_drift(phi, G, pot_scale, p4, v4, nullptr, p4, v4, nullptr, 0, n, dt_kick, dt_drift, c2,
+                                    mean_vel, mom_out ? (double*)ws : nullptr, mom_out, nullptr, (cudaStream_t)stream);
 }
 
 int sd_interpolate_accel(const float* phi, int G, float pot_scale, const float* pos, float* acc, int n, void* stream) {

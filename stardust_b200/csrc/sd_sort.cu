@@ -3,7 +3,8 @@
 // Replaces kCellKey (Sim.cu:2476-2486), cub::DeviceRadixSort::SortPairs
 // (Sim.cu:3659-3667) and kReorder (Sim.cu:2488-2495).
 //
-// The sort is a classic stable LSD radix sort with 8-bit digits, written for
+// The sort is a classic stable LSD radix sort with 8- to 10-bit digits (the key
+// width is split into the fewest passes of at most 10 bits), written for
 // sm_100a, in three kernels per digit pass:
 //   1. k_digit_counts: each 2048-key tile counts its digits in shared memory and
 //      writes them digit-major (count[d * tiles + t]);
@@ -29,8 +30,7 @@ namespace {
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per tile
-constexpr int kRadixBits = 8;
-constexpr int kRadix = 1 << kRadixBits;
+constexpr int kMaxRadixBits = 10;
 constexpr int kWarps = kSortThreads / 32;
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
@@ -73,9 +73,11 @@ __device__ __forceinline__ unsigned block_exclusive(unsigned v, unsigned* warp_s
     return r;
 }
 
+template <int BITS>
 __global__ void __launch_bounds__(kSortThreads) k_digit_counts(const uint32_t* __restrict__ keys, int n, int shift,
-                                                               unsigned mask, unsigned* __restrict__ counts,
-                                                               int tiles) {
+                                                               unsigned* __restrict__ counts, int tiles) {
+    constexpr int kRadix = 1 << BITS;
+    constexpr unsigned mask = kRadix - 1;
     __shared__ unsigned hist[kRadix];
     for (int d = threadIdx.x; d < kRadix; d += kSortThreads) hist[d] = 0u;
     __syncthreads();
@@ -89,20 +91,24 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_counts(const uint32_t* _
     for (int d = threadIdx.x; d < kRadix; d += kSortThreads) counts[(size_t)d * tiles + blockIdx.x] = hist[d];
 }
 
+template <int BITS>
 __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* __restrict__ keys_in,
                                                                 const int32_t* __restrict__ vals_in,
                                                                 uint32_t* __restrict__ keys_out,
                                                                 int32_t* __restrict__ vals_out, int n, int shift,
-                                                                unsigned mask, const unsigned* __restrict__ offsets,
-                                                                int tiles) {
-    __shared__ unsigned warp_cnt[kWarps][kRadix];
+                                                                const unsigned* __restrict__ offsets, int tiles) {
+    constexpr int kRadix = 1 << BITS;
+    constexpr unsigned mask = kRadix - 1;
+    constexpr int DPT = (kRadix + kSortThreads - 1) / kSortThreads;  // digits per thread
+    // per-warp digit counts fit 16 bits (a warp ranks at most 32 * kSortItems keys)
+    __shared__ unsigned short warp_cnt[kWarps][kRadix];
     __shared__ unsigned local_start[kRadix];
     __shared__ unsigned scan_tmp[33];
     __shared__ uint32_t skeys[kSortTile];
     __shared__ int32_t svals[kSortTile];
 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortThreads) (&warp_cnt[0][0])[i] = 0u;
+    for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortThreads) (&warp_cnt[0][0])[i] = 0;
     __syncthreads();
 
     const int tile0 = blockIdx.x * kSortTile;
@@ -127,29 +133,40 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* 
         __syncwarp();
         if (valid) {
             rank[it] = before + __popc(peers & lt);
-            if ((peers & lt) == 0u) warp_cnt[w][d] = before + __popc(peers);
+            if ((peers & lt) == 0u) warp_cnt[w][d] = (unsigned short)(before + __popc(peers));
         }
         __syncwarp();
     }
     __syncthreads();
 
     // Per digit: exclusive scan over warps, then the block-local digit starts.
-    unsigned dtotal = 0u;
-    for (int d = threadIdx.x; d < kRadix; d += kSortThreads) {
-        unsigned run = 0u;
+    unsigned dtot[DPT];
+    unsigned tsum = 0u;
 #pragma unroll
-        for (int ww = 0; ww < kWarps; ++ww) {
-            const unsigned c = warp_cnt[ww][d];
-            warp_cnt[ww][d] = run;
-            run += c;
+    for (int j = 0; j < DPT; ++j) {
+        const int d = threadIdx.x * DPT + j;
+        unsigned run = 0u;
+        if (d < kRadix) {
+#pragma unroll
+            for (int ww = 0; ww < kWarps; ++ww) {
+                const unsigned c = warp_cnt[ww][d];
+                warp_cnt[ww][d] = (unsigned short)run;
+                run += c;
+            }
         }
-        dtotal = run;
+        dtot[j] = run;
+        tsum += run;
     }
     __syncthreads();
     {
         unsigned tot;
-        const unsigned ex = block_exclusive(threadIdx.x < kRadix ? dtotal : 0u, scan_tmp, &tot);
-        if (threadIdx.x < kRadix) local_start[threadIdx.x] = ex;
+        unsigned ex = block_exclusive(tsum, scan_tmp, &tot);
+#pragma unroll
+        for (int j = 0; j < DPT; ++j) {
+            const int d = threadIdx.x * DPT + j;
+            if (d < kRadix) local_start[d] = ex;
+            ex += dtot[j];
+        }
     }
     __syncthreads();
 
@@ -282,7 +299,7 @@ static int scan_tiles_for(size_t m) { return (int)((m + kScanTile - 1) / kScanTi
 
 size_t sort_workspace_bytes(int n) {
     const int tiles = (n + kSortTile - 1) / kSortTile;
-    const size_t m = (size_t)kRadix * (size_t)(tiles > 0 ? tiles : 1);
+    const size_t m = (size_t)(1 << kMaxRadixBits) * (size_t)(tiles > 0 ? tiles : 1);
     return align_up(m * sizeof(unsigned), 256) + align_up((size_t)scan_tiles_for(m) * sizeof(unsigned), 256);
 }
 
@@ -308,32 +325,47 @@ int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t*
     if (ws_bytes < sort_workspace_bytes(n)) return fail(SD_E_ARG, "sort: workspace too small");
     if (keys_in == keys_out || (vals_in && vals_in == vals_out))
         return fail(SD_E_ARG, "sort: input and output buffers must differ");
-    const int passes = (key_bits + kRadixBits - 1) / kRadixBits;
+    // fewest passes of at most kMaxRadixBits bits
+    const int passes = (key_bits + kMaxRadixBits - 1) / kMaxRadixBits;
     if (passes == 0) {
         k_copy_keys<<<(n + 255) / 256, 256, 0, s>>>(keys_in, vals_in, keys_out, vals_out, n);
         SD_LAUNCHED(s);
         return SD_OK;
     }
+    const int even = (key_bits + passes - 1) / passes;  // <= kMaxRadixBits
+    const int bits = even <= 8 ? 8 : even;               // digit width of the kernels (8, 9 or 10)
     const int tiles = (n + kSortTile - 1) / kSortTile;
-    const size_t m = (size_t)kRadix * tiles;
     unsigned* counts = (unsigned*)ws;
-    unsigned* sums = (unsigned*)((char*)ws + align_up(m * sizeof(unsigned), 256));
+    unsigned* sums = (unsigned*)((char*)ws + align_up((size_t)(1 << kMaxRadixBits) * tiles * sizeof(unsigned), 256));
 
     const uint32_t* kin = keys_in;
     const int32_t* vin = vals_in;
     for (int p = 0; p < passes; ++p) {
-        const int shift = p * kRadixBits;
-        const int bits = (key_bits - shift) < kRadixBits ? (key_bits - shift) : kRadixBits;
-        const unsigned mask = (1u << bits) - 1u;
+        const int shift = p * bits;  // passes * bits >= key_bits
         // the last pass lands in *_out; earlier passes alternate so that holds
         const bool to_out = ((passes - 1 - p) % 2) == 0;
         uint32_t* kout = to_out ? keys_out : keys_tmp;
         int32_t* vout = to_out ? vals_out : vals_tmp;
-        k_digit_counts<<<tiles, kSortThreads, 0, s>>>(kin, n, shift, mask, counts, tiles);
+        // key bits above key_bits are zero, so a last digit reaching past them is exact
+        switch (bits) {
+            case 8: k_digit_counts<8><<<tiles, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles); break;
+            case 9: k_digit_counts<9><<<tiles, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles); break;
+            default: k_digit_counts<10><<<tiles, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles); break;
+        }
         SD_LAUNCHED(s);
-        int rc = scan_exclusive(counts, m, sums, s);
+        int rc = scan_exclusive(counts, (size_t)(1 << bits) * tiles, sums, s);
         if (rc != SD_OK) return rc;
-        k_digit_scatter<<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, mask, counts, tiles);
+        switch (bits) {
+            case 8:
+                k_digit_scatter<8><<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, tiles);
+                break;
+            case 9:
+                k_digit_scatter<9><<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, tiles);
+                break;
+            default:
+                k_digit_scatter<10><<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, tiles);
+                break;
+        }
         SD_LAUNCHED(s);
         kin = kout;
         vin = vout;

@@ -233,3 +233,25 @@ def test_tiled_graph_replay_matches_eager(cuda):
             outs.append(s.get_particles())
     assert np.array_equal(outs[0][0].view(np.int32), outs[1][0].view(np.int32))
     assert np.array_equal(outs[0][1].view(np.int32), outs[1][1].view(np.int32))
+
+
+def test_graph_replay_across_calls_and_parity(cuda):
+    """Odd step counts and interleaved eager steps leave the particles in either
+    ping-pong buffer; later graph replays must still match plain stepping."""
+    G, n = 32, 60_000
+    pos, vel = random_particles(n, 21, clustered=True)
+    outs = []
+    for mode in ("eager", "mixed"):
+        with make_sim(cuda, n, G, gravity=200.0, softening_cells=1.0, order=L.SD_ORDER_TILED) as s:
+            s.set_particles(pos, vel)
+            if mode == "eager":
+                for _ in range(12):
+                    s.step(1e-3)
+            else:
+                s.steps(1e-3, 3)
+                s.step(1e-3)
+                s.steps(1e-3, 5)
+                s.steps(1e-3, 3)
+            outs.append(s.get_particles())
+    assert np.array_equal(outs[0][0].view(np.int32), outs[1][0].view(np.int32))
+    assert np.array_equal(outs[0][1].view(np.int32), outs[1][1].view(np.int32))
