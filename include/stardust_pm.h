@@ -227,6 +227,20 @@ int sd_deposit(const float* pos, int n, int grid_size, float* rho, void* workspa
 size_t sd_poisson_workspace_bytes(int grid_size);
 int sd_poisson(const float* rho, int grid_size, float softening_cells, float* phi, void* workspace,
                size_t workspace_bytes, void* stream);
+/* The same Poisson solve for callers that cannot allocate device memory: no
+ * counterpart in the reference. Some callers cannot call cudaMalloc, or be handed
+ * a workspace, on this path: code inside another component's allocation-free
+ * hot loop, under a fixed memory budget that forbids growth after start-up, or
+ * enqueuing work on a stream that someone else is capturing. This entry point
+ * allocates nothing: its spectrum and tables live in fixed device storage of
+ * the library, which every GPU that loads the library holds (about 9 MB) until
+ * the process exits. grid_size must be a power of two in [16, 128]; larger
+ * grids are rejected with SD_E_ARG. The first call on a device resolves that
+ * storage and uploads the twiddle tables (synchronously), so make it before any
+ * stream capture. All calls on a device share the storage: calls that overlap
+ * on the GPU (different streams, no ordering between them) race and give wrong
+ * results. rho and phi are caller device buffers of grid_size^3 floats. */
+int sd_poisson_noalloc(const float* rho, int grid_size, float softening_cells, float* phi, void* stream);
 /* Gather + kick + drift (kGridAccel Sim.cu:589-611 folded into sampleAcc /
  * kIntegrate Sim.cu:614-629, 685-906). pot_scale = gravity/N. mean_vel (3
  * floats, device, may be NULL) is subtracted from each loaded velocity (the

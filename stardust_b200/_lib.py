@@ -117,6 +117,7 @@ SIGNATURES = [
     ("sd_deposit", _I, [_P, _I, _I, _P, _P, _S, _P]),
     ("sd_poisson_workspace_bytes", _S, [_I]),
     ("sd_poisson", _I, [_P, _I, _F, _P, _P, _S, _P]),
+    ("sd_poisson_noalloc", _I, [_P, _I, _F, _P, _P]),
     ("sd_gather_kick_drift", _I, [_P, _I, _F, _P, _P, _I, _F, _F, _F, _P, _P, _P, _S, _P]),
     ("sd_gather_workspace_bytes", _S, [_I]),
     ("sd_interpolate_accel", _I, [_P, _I, _F, _P, _P, _I, _P]),

@@ -20,6 +20,7 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <mutex>
 #include <vector>
 
 #include "sd_common.cuh"
@@ -585,4 +586,114 @@ int launch_poisson_ex(const PoissonPlan& p, const long long* acc, const float* r
     }
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free Poisson solve (sd_poisson_noalloc).
+//
+// For callers that must not allocate device memory: code running where
+// cudaMalloc is not allowed, such as inside another library's allocator-free
+// hot loop, under a strict memory budget that forbids growth after start-up,
+// or on a stream being captured by someone else's graph. Its working memory
+// is file-scope device storage of fixed size, so grids are limited to
+// kNoAllocMaxGrid^3. Every GPU that loads this library holds that storage
+// (about 9 MB) until the process exits, and all calls on a device share it:
+// calls that overlap on the GPU race on it.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocMaxGrid = 128;
+constexpr size_t kNoAllocSpecElems =
+    (size_t)kNoAllocMaxGrid * kNoAllocMaxGrid * (size_t)(kNoAllocMaxGrid / 2 + 4);
+constexpr int kNoAllocMaxDevices = 64;
+
+// The bricked spectrum of the largest supported grid, the twiddle tables of
+// G = 16, 32, 64, 128 (one row of kNoAllocMaxGrid entries each) and the
+// Green's-function exponent table of the current call.
+static __device__ __align__(256) float2 g_noalloc_spec[kNoAllocSpecElems];
+static __device__ __align__(256) float2 g_noalloc_tw[4 * kNoAllocMaxGrid];
+static __device__ __align__(256) float g_noalloc_gexp[kNoAllocMaxGrid / 2 + 1];
+
+struct NoAllocDevice {
+    bool ready = false;
+    float2* spec = nullptr;
+    float2* tw = nullptr;
+    float* gexp = nullptr;
+};
+NoAllocDevice g_noalloc[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+// exp(-(2 pi soft / G)^2 k^2 / 2) in FP64, k = 0..G/2 (the table poisson_plan_build
+// makes on the host).
+__global__ void k_fill_gexp(float* __restrict__ gexp, int G, float soft) {
+    const int k = threadIdx.x;
+    if (k > G / 2) return;
+    const double s = 6.283185307179586476925286766559 * (double)(soft > 0.f ? soft : 0.f) / (double)G;
+    gexp[k] = (float)exp(-0.5 * s * s * (double)k * (double)k);
+}
+
+int noalloc_slot(int G) { return G == 16 ? 0 : (G == 32 ? 1 : (G == 64 ? 2 : 3)); }
+
+// Once per device, with that device current: resolve the device addresses of
+// the file-scope arrays (their names are host-side stand-ins in host code),
+// upload the twiddle tables and set the kernels' shared-memory attributes.
+int noalloc_setup(int dev) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    NoAllocDevice& d = g_noalloc[dev];
+    if (d.ready) return SD_OK;
+    void* p = nullptr;
+    if (SD_CUDA(cudaGetSymbolAddress(&p, g_noalloc_spec))) return SD_E_CUDA;
+    d.spec = static_cast<float2*>(p);
+    if (SD_CUDA(cudaGetSymbolAddress(&p, g_noalloc_tw))) return SD_E_CUDA;
+    d.tw = static_cast<float2*>(p);
+    if (SD_CUDA(cudaGetSymbolAddress(&p, g_noalloc_gexp))) return SD_E_CUDA;
+    d.gexp = static_cast<float*>(p);
+    std::vector<float2> tw((size_t)4 * kNoAllocMaxGrid, make_float2(0.f, 0.f));
+    const double two_pi = 6.283185307179586476925286766559;
+    for (int G = 16; G <= kNoAllocMaxGrid; G *= 2) {
+        float2* row = tw.data() + (size_t)noalloc_slot(G) * kNoAllocMaxGrid;
+        for (int m = 0; m < G; ++m) {
+            const double a = -two_pi * (double)m / (double)G;
+            row[m] = make_float2((float)cos(a), (float)sin(a));
+        }
+        if (int rc = poisson_configure(G)) return rc;
+    }
+    if (SD_CUDA(cudaMemcpy(d.tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice))) return SD_E_CUDA;
+    d.ready = true;
+    return SD_OK;
+}
+
+}  // namespace
+
 }  // namespace sd
+
+extern "C" int sd_poisson_noalloc(const float* rho, int grid_size, float softening_cells, float* phi, void* stream) {
+    using namespace sd;
+    const int G = grid_size;
+    if (!rho || !phi) return fail(SD_E_ARG, "sd_poisson_noalloc: null rho or phi");
+    if (G < 16 || G > kNoAllocMaxGrid || (G & (G - 1)))
+        return fail(SD_E_ARG,
+                    "sd_poisson_noalloc: grid_size %d is not a power of two in [16, %d]; its fixed workspace holds "
+                    "the spectrum of a %d^3 grid at most (use sd_poisson with a caller workspace for larger grids)",
+                    G, kNoAllocMaxGrid, kNoAllocMaxGrid);
+    int dev = 0;
+    if (SD_CUDA(cudaGetDevice(&dev))) return SD_E_CUDA;
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(SD_E_ARG, "sd_poisson_noalloc: device %d unsupported", dev);
+    if (int rc = noalloc_setup(dev)) return rc;
+    const NoAllocDevice& d = g_noalloc[dev];
+    cudaStream_t st = (cudaStream_t)stream;
+    // the exponent table depends on the softening: rebuilt by every call
+    k_fill_gexp<<<1, kNoAllocMaxGrid, 0, st>>>(d.gexp, G, softening_cells);
+    SD_LAUNCHED(st);
+    PoissonPlan plan;
+    plan.G = G;
+    plan.soft = softening_cells;
+    plan.tw = d.tw + (size_t)noalloc_slot(G) * kNoAllocMaxGrid;
+    plan.gexp = d.gexp;
+    plan.scale = (float)(1.0 / (4.0 * 3.14159265358979323846 * 3.14159265358979323846 * (double)G * G * G));
+    // pass A writes every spectrum element (padding columns as zeros), so the
+    // shared workspace needs no clearing between calls
+    const int rc = launch_poisson(plan, nullptr, rho, nullptr, d.spec, phi, st);
+    plan.tw = nullptr;  // static storage: the plan does not own it
+    plan.gexp = nullptr;
+    return rc;
+}
+
