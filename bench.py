@@ -44,6 +44,40 @@ def model_bytes(n: int, G: int) -> float:
     return 184.0 * n + 40.0 * G ** 3
 
 
+# kernels of one timed step, in the order of sd_timings.kernel_ms
+KERNELS = ["sort", "row_table", "pass_a_deposit", "pass_b", "pass_c", "pass_d", "pass_e", "gather"]
+
+
+def kernel_bytes(n: int, G: int) -> dict:
+    """Algorithmic bytes per launch of each kernel of the tiled-order step."""
+    spec = 8.0 * G * G * (G // 2 + 4)  # bricked half spectrum, complex64
+    cells = float(G) ** 3
+    return {
+        "sort": 2 * (4 + 16) * n,                 # two 10-bit passes: count keys, move key + value
+        "row_table": 4 * n + 4 * (G * G + 1),
+        "pass_a_deposit": 20 * n + spec,          # perm + pos once; spectrum written
+        "pass_b": 2 * spec,
+        "pass_c": 2 * spec,
+        "pass_d": 2 * spec,
+        "pass_e": spec + 4 * cells,
+        "gather": 72 * n + 4 * cells,             # perm, pos+vel in/out, keys, potential
+    }
+
+
+def measured_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 3 and parts[0] == workload and parts[1] == kernel:
+                    return float(parts[2])
+    except OSError:
+        pass
+    return None
+
+
 def hbm_peak():
     try:
         with open(MEASURED_PEAKS) as f:
@@ -80,7 +114,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -162,14 +196,17 @@ def run_ours(args, rank, world):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
     ms = float(t.item())
 
-    # --- per-phase times (eager steps with phase events) for the roofline ---
+    # --- per-kernel times (eager steps with events between kernels) for the roofline ---
+    kms = []
     phases = {"sort_ms": [], "deposit_ms": [], "poisson_ms": [], "gather_ms": [], "total_ms": []}
     for _ in range(3):
         sim.step(dt)
         tm = sim.timings()
+        kms.append(tm["kernel_ms"])
         for k in phases:
             phases[k].append(tm[k])
     phase_ms = {k: float(np.median(v)) for k, v in phases.items()}
+    kernel_ms = dict(zip(KERNELS, np.median(np.array(kms), axis=0).tolist()))
 
     # --- end to end through the C ABI with pinned host buffers, every step ---
     hp = torch.from_numpy(pos).pin_memory()
@@ -202,15 +239,10 @@ def run_ours(args, rank, world):
     peak, peak_kind = hbm_peak()
     B = model_bytes(n, G)
     achieved_step = B / (ms * 1e-3) / 1e9
-    # dominant phase and its algorithmic bytes
-    phase_bytes = {
-        "sort_ms": (4 + 16) * n + 2 * ((28 + 7) // 8) * 16 * n + 68 * n,  # keys, LSD passes, reorder
-        "deposit_ms": 16 * n + 8 * G ** 3 + 8 * G ** 3,                    # pos read, int64 RMW
-        "poisson_ms": 36 * G ** 3,                                          # 5 passes over ~4 B/cell spectra
-        "gather_ms": 64 * n + 4 * G ** 3,                                   # pos+vel r/w, phi read
-    }
-    dom = max((k for k in phase_bytes), key=lambda k: phase_ms[k])
-    dom_achieved = phase_bytes[dom] / (phase_ms[dom] * 1e-3) / 1e9
+    kbytes = kernel_bytes(n, G)
+    dom = max(KERNELS, key=lambda k: kernel_ms[k])
+    dom_achieved = kbytes[dom] / (kernel_ms[dom] * 1e-3) / 1e9
+    traffic = measured_traffic(dom, args.workload)
     value = world * n / (ms * 1e-3)
     out = {
         "metric": "particle-steps/s at 16M/512^3",
@@ -230,9 +262,13 @@ def run_ours(args, rank, world):
                    "units": "newton G=1 M=1", "softening_cells": 1.0, "parallelism": f"replicas x{world}",
                    "l2": "inputs exceed L2 (no flush)", "timed_path": "sd_steps (CUDA graph, 2 steps/replay)"},
         "roofline": {"bound": "hbm", "achieved": dom_achieved, "peak": peak, "unit": "GB/s",
-                     "frac": dom_achieved / peak, "traffic": None, "kernel": dom.replace("_ms", ""),
-                     "peak_source": peak_kind},
-        "step_roofline": {"model_bytes": B, "achieved_gbs": achieved_step, "frac": achieved_step / peak},
+                     "frac": dom_achieved / peak, "traffic": traffic, "kernel": dom,
+                     "algorithmic_bytes": kbytes[dom], "kernel_ms": kernel_ms[dom],
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                     else "fallback 6650 GB/s"},
+        "step_roofline": {"model_bytes": B, "model": "184 N + 40 G^3", "achieved_gbs": achieved_step,
+                          "frac": achieved_step / peak},
+        "kernel_ms": kernel_ms,
         "phase_ms": phase_ms,
         "e2e": {"value": world * n / (e2e_ms * 1e-3), "unit": "particle-steps/s",
                 "h2d_bytes_per_step": 2 * 16 * n, "d2h_bytes_per_step": 2 * 16 * n,
@@ -252,7 +288,9 @@ def run_reference(args, rank, world):
     grav = float(4 * np.pi * G ** 3)
     # warm-up on a small sample, then time whole steps at the full size
     O.step(pos[:4096], vel[:4096], 16, grav, 1.0, dt, dt)
-    steps = max(1, min(args.steps, 2))
+    # each timed step is one full step of the workload (about 1 s on 16 cores);
+    # at most 20 of them keep the arm within a few minutes
+    steps = max(1, min(args.steps, 20))
     t0 = time.perf_counter()
     p, v = pos, vel
     for _ in range(steps):
@@ -281,24 +319,27 @@ def run_reference(args, rank, world):
     }
 
 
-def cpu_baseline_sample(workload: str):
-    """One full step of the CPU restatement (oracle/), all host threads."""
+def cpu_baseline_sample(workload: str, steps: int = 8):
+    """Full steps of the CPU restatement (oracle/), all host threads: a bounded
+    sample of about 10 s on a 16-core host."""
     from oracle import oracle as O
 
     pos, vel, G, dt = make_workload(workload)
     grav = float(4 * np.pi * G ** 3)
     O.step(pos[:4096], vel[:4096], 16, grav, 1.0, dt, dt)
     t0 = time.perf_counter()
-    O.step(pos, vel, G, grav, 1.0, dt, dt)
-    sec = time.perf_counter() - t0
+    p, v = pos, vel
+    for _ in range(steps):
+        p, v, _, _ = O.step(p, v, G, grav, 1.0, dt, dt)
+    sec = (time.perf_counter() - t0) / steps
     return {"value": len(pos) / sec, "unit": "particle-steps/s", "cores": O.num_threads(), "kind": "port",
-            "sample": f"1 full step of {len(pos)} particles on a {G}^3 grid ({sec:.1f} s)"}
+            "sample": f"{steps} full steps of {len(pos)} particles on a {G}^3 grid ({sec:.2f} s each)"}
 
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cosmic_web_512")

@@ -97,6 +97,12 @@ typedef struct sd_timings {
     float dt_used;
     float max_speed;
     int32_t steps;     /* steps covered by these numbers */
+    /* per-kernel device time of the last eager step: [0] keys + sort,
+     * [1] row table or atomic deposit, [2] pass A (fused deposit + x real FFT),
+     * [3] pass B (y forward), [4] pass C (z forward, Green's function, z
+     * inverse), [5] pass D (y inverse), [6] pass E (x complex-to-real),
+     * [7] gather + kick + drift (+ momentum sums) */
+    float kernel_ms[8];
 } sd_timings;
 
 /* FP64 diagnostics of the last step (computed on the device). */

@@ -50,6 +50,7 @@ class SdTimings(ctypes.Structure):
         ("dt_used", ctypes.c_float),
         ("max_speed", ctypes.c_float),
         ("steps", ctypes.c_int32),
+        ("kernel_ms", ctypes.c_float * 8),
     ]
 
 

@@ -53,9 +53,10 @@ int launch_poisson(const PoissonPlan& p, const long long* rho_fixed, const float
                    float2* spec, float* phi, cudaStream_t s);
 // pos != nullptr: the first pass deposits the particles itself (SD_ORDER_TILED
 // order, row_start from launch_row_bounds) instead of reading a density grid.
+// ev (optional): 4 events recorded after passes A, B, C and D.
 int launch_poisson_ex(const PoissonPlan& p, const long long* rho_fixed, const float* rho_float, const float4* pos,
                       const int* perm, const int* row_start, float* rho_keep, float2* spec, float* phi,
-                      cudaStream_t s);
+                      cudaStream_t s, cudaEvent_t* ev = nullptr);
 // row_start[r] = first index i with sorted keys_plus1[i] > r, for r in [0, rows]
 int launch_row_bounds(const uint32_t* keys_plus1, int n, int rows, int* row_start, cudaStream_t s);
 

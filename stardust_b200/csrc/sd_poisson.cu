@@ -497,7 +497,7 @@ struct Launcher {
     }
 
     static int run(const PoissonPlan& p, const long long* acc, const float* rho, const float4* pos, const int* perm,
-                   const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s) {
+                   const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s, cudaEvent_t* ev) {
         const dim3 grid_rows(T::NBY, T::NBZ), grid_y(T::NBX, T::NBZ), grid_z(T::NBX, T::NBY);
         if (pos)
             k_pass_a_deposit<G><<<grid_rows, kDepositThreads, smem_dep(), s>>>(pos, perm, row_start, keep, spec, p.tw);
@@ -507,12 +507,16 @@ struct Launcher {
         else
             k_pass_a<G, 0><<<grid_rows, kFftThreads, smem_ae(), s>>>(rho, nullptr, keep, spec, p.tw);
         SD_LAUNCHED(s);
+        if (ev) cudaEventRecord(ev[0], s);
         k_pass_y<G, false><<<grid_y, kFftThreads, smem_bd(), s>>>(spec, p.tw);
         SD_LAUNCHED(s);
+        if (ev) cudaEventRecord(ev[1], s);
         k_pass_c<G><<<grid_z, kFftThreads, smem_c(), s>>>(spec, p.tw, p.gexp, p.scale);
         SD_LAUNCHED(s);
+        if (ev) cudaEventRecord(ev[2], s);
         k_pass_y<G, true><<<grid_y, kFftThreads, smem_bd(), s>>>(spec, p.tw);
         SD_LAUNCHED(s);
+        if (ev) cudaEventRecord(ev[3], s);
         k_pass_e<G><<<grid_rows, kFftThreads, smem_ae(), s>>>(spec, phi, p.tw);
         SD_LAUNCHED(s);
         return SD_OK;
@@ -574,14 +578,15 @@ int launch_poisson(const PoissonPlan& p, const long long* acc, const float* rho,
 }
 
 int launch_poisson_ex(const PoissonPlan& p, const long long* acc, const float* rho, const float4* pos,
-                      const int* perm, const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s) {
+                      const int* perm, const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s,
+                      cudaEvent_t* ev) {
     switch (p.G) {
-        case 16: return Launcher<16>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s);
-        case 32: return Launcher<32>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s);
-        case 64: return Launcher<64>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s);
-        case 128: return Launcher<128>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s);
-        case 256: return Launcher<256>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s);
-        case 512: return Launcher<512>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s);
+        case 16: return Launcher<16>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev);
+        case 32: return Launcher<32>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev);
+        case 64: return Launcher<64>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev);
+        case 128: return Launcher<128>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev);
+        case 256: return Launcher<256>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev);
+        case 512: return Launcher<512>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev);
         default: return fail(SD_E_UNSUPPORTED, "poisson: grid size %d not supported", p.G);
     }
 }

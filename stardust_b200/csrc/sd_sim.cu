@@ -102,8 +102,9 @@ struct sd_sim {
     bool lf_open = false;
     float lf_dt_prev = 0.f;
 
-    // timings of the last eager step
+    // timings of the last eager step: ev[0..4] phase bounds, pev[0..3] after Poisson passes A-D
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t pev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool ev_valid = false;
     sd_timings tm{};
     sd_diagnostics diag{};
@@ -291,6 +292,8 @@ int ensure_events(sd_sim* s) {
     if (s->ev[0]) return SD_OK;
     for (auto& e : s->ev)
         if (SD_CUDA(cudaEventCreate(&e))) return SD_E_CUDA;
+    for (auto& e : s->pev)
+        if (SD_CUDA(cudaEventCreate(&e))) return SD_E_CUDA;
     return SD_OK;
 }
 
@@ -358,7 +361,8 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     }
     if (timed) cudaEventRecord(s->ev[2], s->stream);
     if ((rc = launch_poisson_ex(s->plan, fused ? nullptr : s->acc, nullptr, fused ? s->pos : nullptr, perm,
-                                s->row_start, keep ? s->rho : nullptr, s->spec, s->phi, s->stream)))
+                                s->row_start, keep ? s->rho : nullptr, s->spec, s->phi, s->stream,
+                                timed ? s->pev : nullptr)))
         return sim_error(s, rc);
     if (keep) s->rho_valid = true;
     if (timed) cudaEventRecord(s->ev[3], s->stream);
@@ -538,6 +542,8 @@ int sd_destroy(sd_sim* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     free_buffers(s);
     for (auto& e : s->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : s->pev)
         if (e) cudaEventDestroy(e);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -898,6 +904,14 @@ int sd_timings_get(const sd_sim* s, sd_timings* out) {
         out->poisson_ms = ms[2];
         out->gather_ms = ms[3];
         out->total_ms = tot;
+        // kernels: sort, row table / deposit, passes A-E, gather
+        cudaEvent_t seq[9] = {s->ev[0], s->ev[1], s->ev[2], s->pev[0], s->pev[1], s->pev[2], s->pev[3], s->ev[3],
+                              s->ev[4]};
+        for (int i = 0; i < 8; ++i) {
+            float k = 0.f;
+            cudaEventElapsedTime(&k, seq[i], seq[i + 1]);
+            out->kernel_ms[i] = k;
+        }
     }
     return SD_OK;
 }

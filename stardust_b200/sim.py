@@ -214,7 +214,9 @@ class Sim:
     def timings(self) -> dict:
         t = L.SdTimings()
         L.check(L.lib().sd_timings_get(self._h, ctypes.byref(t)), "sd_timings_get")
-        return {f[0]: getattr(t, f[0]) for f in L.SdTimings._fields_}
+        out = {f[0]: getattr(t, f[0]) for f in L.SdTimings._fields_ if f[0] != "kernel_ms"}
+        out["kernel_ms"] = list(t.kernel_ms)
+        return out
 
     def sim_time(self) -> float:
         return float(L.lib().sd_sim_time(self._h))

@@ -30,7 +30,7 @@ def test_every_declared_symbol_is_exported(lib):
 
 def test_struct_sizes_match_header(lib):
     assert ctypes.sizeof(L.SdConfig) == 20 * 4
-    assert ctypes.sizeof(L.SdTimings) == 8 * 4
+    assert ctypes.sizeof(L.SdTimings) == 16 * 4
 
 
 def test_defaults_follow_reference_simconfig(lib):
