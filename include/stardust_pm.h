@@ -261,6 +261,49 @@ size_t sd_gather_workspace_bytes(int n);
 int sd_interpolate_accel(const float* phi, int grid_size, float pot_scale, const float* pos, float* acc_out,
                          int n, void* stream);
 
+/* ---- learned sub-grid force correction (no counterpart in the reference) ----
+ * An MLP 30 -> 64 -> 64 -> 3 (SiLU) maps a particle's coarse-grid features (the
+ * 3x3x3 CIC density stencil around its cell as log(1 + rho/rho_bar) - log 2, and
+ * its sub-cell offset) to a residual acceleration that is added to the PM
+ * acceleration before the kick. BF16 weights and activations, FP32 accumulation
+ * on the tensor cores. params: FP32 vector of sd_mlp_param_count() floats
+ * (W1[32][64], b1[64], W2[64][64], b2[64], W3[64][8], b3[8]). inv_mean =
+ * grid_size^3 / particle count. Outputs are scaled by out_scale. */
+int sd_mlp_param_count(void);
+/* features (bf16[n][32]) of pos[perm[i]] (perm may be NULL) from the density rho[G^3] */
+int sd_mlp_features(const float* pos, const int32_t* perm, int n, const float* rho, int grid_size, float inv_mean,
+                    void* features_bf16, void* stream);
+/* residual accelerations float4[n] (w = 0; empty slots get 0) */
+int sd_mlp_infer(const float* params, const float* pos, const int32_t* perm, int n, const float* rho,
+                 int grid_size, float inv_mean, float out_scale, float* out, void* stream);
+/* gradient (FP32 [params]) of the mean squared error over rows and the 3 outputs
+ * of one batch (rows a multiple of 16); *sse = sum of squared errors (device) */
+size_t sd_mlp_train_workspace_bytes(int rows);
+int sd_mlp_loss_grad(const float* params, const void* features_bf16, const float* targets, int rows, float* grad,
+                     float* sse, void* workspace, size_t workspace_bytes, void* stream);
+/* one Adam step on the FP32 master parameters (device arrays m, v of the same size) */
+int sd_mlp_adam(float* params, float* m, float* v, const float* grad, int step, float lr, float beta1, float beta2,
+                float eps, void* stream);
+/* Enable (params != NULL) or disable the correction in sd_step / sd_steps of a
+ * handle; params are copied. Needs keep_density (the correction reads the
+ * step-start density), which this call switches on. */
+int sd_set_mlp(sd_sim* sim, const float* params_device, float out_scale);
+
+/* ---- FP64 reference forces (force-error judge; not on the step) ------------
+ * Periodic Newtonian accelerations (G = 1, each source of mass 1/n_src, mean
+ * density removed) of Gaussian-smoothed masses of width `softening` (box units;
+ * the PM step's softening_cells / grid_size), by Ewald summation in FP64:
+ * structure factors over modes 0 < |n| <= nmax and the erf-difference pair
+ * kernel over all sources at their nearest image. split_b is the Ewald
+ * smoothing length (b^2 > 2 softening^2, b <= 0.1); choose nmax >= 1.75 / split_b
+ * so the dropped modes carry weights below 1e-12. acc_out: double[3 * n_tgt], device.
+ * The reference has no force-accuracy code (its test was deleted); the metric
+ * is .drive/nbody-simulator/method-search/scoring.md:38. Synchronises `stream`. */
+int sd_ewald_modes(int nmax);
+size_t sd_ewald_workspace_bytes(int nmax);
+int sd_ewald_forces(const float* src, int n_src, const float* tgt, int n_tgt, double softening, double split_b,
+                    int nmax, double* acc_out, void* workspace, size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

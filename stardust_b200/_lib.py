@@ -122,6 +122,16 @@ SIGNATURES = [
     ("sd_gather_kick_drift", _I, [_P, _I, _F, _P, _P, _I, _F, _F, _F, _P, _P, _P, _S, _P]),
     ("sd_gather_workspace_bytes", _S, [_I]),
     ("sd_interpolate_accel", _I, [_P, _I, _F, _P, _P, _I, _P]),
+    ("sd_mlp_param_count", _I, []),
+    ("sd_mlp_features", _I, [_P, _P, _I, _P, _I, _F, _P, _P]),
+    ("sd_mlp_infer", _I, [_P, _P, _P, _I, _P, _I, _F, _F, _P, _P]),
+    ("sd_mlp_train_workspace_bytes", _S, [_I]),
+    ("sd_mlp_loss_grad", _I, [_P, _P, _P, _I, _P, _P, _P, _S, _P]),
+    ("sd_mlp_adam", _I, [_P, _P, _P, _P, _I, _F, _F, _F, _F, _P]),
+    ("sd_set_mlp", _I, [_P, _P, _F]),
+    ("sd_ewald_modes", _I, [_I]),
+    ("sd_ewald_workspace_bytes", _S, [_I]),
+    ("sd_ewald_forces", _I, [_P, _I, _P, _I, _D, _D, _I, _P, _P, _S, _P]),
 ]
 
 _lib = None

@@ -64,12 +64,17 @@ size_t gather_partials(int n);
 // perm != nullptr: slot i takes input particle perm[i] (fused reorder) and the
 // outputs must be separate arrays; otherwise pos_out/vel_out may alias the inputs.
 // keys_out (optional) receives the next step's order keys (key + 1).
+// extra (optional) is an acceleration added to the PM one, indexed like the outputs.
 int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const float4* pos_in, const float4* vel_in,
                              const int* perm, float4* pos_out, float4* vel_out, uint32_t* keys_out, int order, int n,
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
-                             double* mom_out, float* mean_out, cudaStream_t s);
+                             double* mom_out, float* mean_out, cudaStream_t s, const float4* extra = nullptr);
 int launch_interpolate_accel(const float* phi, int G, float pot_scale, const float4* pos, float4* acc, int n,
-                             cudaStream_t s);
+                             cudaStream_t s, const float4* extra = nullptr);
+// learned correction (sd_mlp.cu): out[i] = out_scale * MLP(features of pos[perm ? perm[i] : i])
+size_t mlp_param_count();
+int launch_mlp_infer(const float* params, const float4* pos, const int* perm, int n, const float* rho, int G,
+                     float inv_mean, float out_scale, float4* out, cudaStream_t s);
 int launch_apply_mean(float4* vel, const float4* pos, int n, const float* mean_vel, cudaStream_t s);
 int launch_max_speed(const float4* pos, const float4* vel, int n, const float* mean_vel, float* out,
                      cudaStream_t s);

@@ -158,7 +158,8 @@ __device__ __forceinline__ void block_sum4(double v0, double v1, double v2, doub
 __global__ void __launch_bounds__(kGatherThreads) k_gather_kick_drift(
     const float* __restrict__ phi, int G, float h, const float4* pos_in, const float4* vel_in,
     const int* __restrict__ perm, float4* pos_out, float4* vel_out, uint32_t* __restrict__ keys_out, int order, int n,
-    float dt_kick, float dt_drift, float c2, const float* __restrict__ mean_vel, double* __restrict__ partials) {
+    float dt_kick, float dt_drift, float c2, const float* __restrict__ mean_vel, double* __restrict__ partials,
+    const float4* __restrict__ extra) {
     double sx = 0.0, sy = 0.0, sz = 0.0, cnt = 0.0;
     const float mx = mean_vel ? mean_vel[0] : 0.f, my = mean_vel ? mean_vel[1] : 0.f,
                 mz = mean_vel ? mean_vel[2] : 0.f;
@@ -179,7 +180,13 @@ __global__ void __launch_bounds__(kGatherThreads) k_gather_kick_drift(
             v.y = __fsub_rn(v.y, my);
             v.z = __fsub_rn(v.z, mz);
         }
-        const float3 a = gather_accel(phi, G, h, p);
+        float3 a = gather_accel(phi, G, h, p);
+        if (extra) {  // learned correction, indexed like the outputs
+            const float4 e = extra[i];
+            a.x = __fadd_rn(a.x, e.x);
+            a.y = __fadd_rn(a.y, e.y);
+            a.z = __fadd_rn(a.z, e.z);
+        }
         v.x = __fmaf_rn(a.x, dt_kick, v.x);
         v.y = __fmaf_rn(a.y, dt_kick, v.y);
         v.z = __fmaf_rn(a.z, dt_kick, v.z);
@@ -245,7 +252,7 @@ __global__ void __launch_bounds__(256) k_finalize_mean(const double* __restrict_
 
 __global__ void __launch_bounds__(256) k_interpolate_accel(const float* __restrict__ phi, int G, float h,
                                                            const float4* __restrict__ pos, float4* __restrict__ acc,
-                                                           int n) {
+                                                           int n, const float4* __restrict__ extra) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 p = pos[i];
@@ -253,7 +260,13 @@ __global__ void __launch_bounds__(256) k_interpolate_accel(const float* __restri
         acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         return;
     }
-    const float3 a = gather_accel(phi, G, h, p);
+    float3 a = gather_accel(phi, G, h, p);
+    if (extra) {
+        const float4 e = extra[i];
+        a.x = __fadd_rn(a.x, e.x);
+        a.y = __fadd_rn(a.y, e.y);
+        a.z = __fadd_rn(a.z, e.z);
+    }
     acc[i] = make_float4(a.x, a.y, a.z, 0.f);
 }
 
@@ -428,12 +441,12 @@ size_t gather_partials(int n) {
 int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const float4* pos_in, const float4* vel_in,
                              const int* perm, float4* pos_out, float4* vel_out, uint32_t* keys_out, int order, int n,
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
-                             double* mom_out, float* mean_out, cudaStream_t s) {
+                             double* mom_out, float* mean_out, cudaStream_t s, const float4* extra) {
     if (n <= 0) return SD_OK;
     const float h = (0.5f * (float)G) * pot_scale;  // Sim.cu:604
     const int blocks = (int)gather_partials(n);
     k_gather_kick_drift<<<blocks, kGatherThreads, 0, s>>>(phi, G, h, pos_in, vel_in, perm, pos_out, vel_out, keys_out,
-                                                          order, n, dt_kick, dt_drift, c2, mean_vel, partials);
+                                                          order, n, dt_kick, dt_drift, c2, mean_vel, partials, extra);
     SD_LAUNCHED(s);
     if (partials && (mom_out || mean_out)) {
         k_finalize_mean<<<1, 256, 0, s>>>(partials, blocks, mom_out, mean_out);
@@ -443,10 +456,10 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
 }
 
 int launch_interpolate_accel(const float* phi, int G, float pot_scale, const float4* pos, float4* acc, int n,
-                             cudaStream_t s) {
+                             cudaStream_t s, const float4* extra) {
     if (n <= 0) return SD_OK;
     const float h = (0.5f * (float)G) * pot_scale;
-    k_interpolate_accel<<<(n + 255) / 256, 256, 0, s>>>(phi, G, h, pos, acc, n);
+    k_interpolate_accel<<<(n + 255) / 256, 256, 0, s>>>(phi, G, h, pos, acc, n, extra);
     SD_LAUNCHED(s);
     return SD_OK;
 }

@@ -110,6 +110,12 @@ struct sd_sim {
     sd_diagnostics diag{};
     bool diag_valid = false;
 
+    // learned correction (sd_set_mlp): device copy of the parameters, per-slot output
+    float* mlp_params = nullptr;
+    float4* mlp_out = nullptr;
+    float mlp_scale = 0.f;
+    bool mlp_on = false;
+
     // captured steps for sd_steps
     cudaGraphExec_t graph = nullptr;
     float graph_dt = 0.f;
@@ -182,6 +188,7 @@ void free_buffers(sd_sim* s) {
     s->sort_ws_bytes = 0;
     free_dev(s->acc); free_dev(s->row_start); free_dev(s->spec); free_dev(s->phi); free_dev(s->rho);
     free_dev(s->partials); free_dev(s->mom); free_dev(s->mean);
+    free_dev(s->mlp_out);
     poisson_plan_free(s->plan);
     if (s->graph) cudaGraphExecDestroy(s->graph);
     s->graph = nullptr;
@@ -233,7 +240,8 @@ int allocate(sd_sim* s) {
     rc = rc ? rc : alloc_dev(s->row_start, (size_t)s->G * s->G + 1);
     rc = rc ? rc : alloc_dev(s->spec, poisson_spectrum_elems(s->G));
     rc = rc ? rc : alloc_dev(s->phi, cells);
-    if (!rc && s->cfg.keep_density) rc = alloc_dev(s->rho, cells);
+    if (!rc && (s->cfg.keep_density || s->mlp_on)) rc = alloc_dev(s->rho, cells);
+    if (!rc && s->mlp_on) rc = alloc_dev(s->mlp_out, N);
     s->partials_count = 8 * (gather_partials(s->N) + 1024);
     rc = rc ? rc : alloc_dev(s->partials, s->partials_count);
     rc = rc ? rc : alloc_dev(s->mom, 8);
@@ -297,6 +305,15 @@ int ensure_events(sd_sim* s) {
     return SD_OK;
 }
 
+bool keeps_rho(const sd_sim* s) { return s->rho && (s->cfg.keep_density || s->mlp_on); }
+
+// Learned correction of the particles pos[perm[i]] from the density just kept.
+int mlp_correction(sd_sim* s, const int32_t* perm) {
+    const float inv_mean = (float)((double)s->G * s->G * s->G / (double)(s->N > 0 ? s->N : 1));
+    return launch_mlp_infer(s->mlp_params, s->pos, perm, s->N, s->rho, s->G, inv_mean, s->mlp_scale, s->mlp_out,
+                            s->stream);
+}
+
 // Sort + reorder (sortParticles, Sim.cu:3656-3671).
 int do_sort(sd_sim* s, int32_t* perm_out_dev) {
     int rc = launch_cell_keys(s->pos, s->N, s->G, s->cfg.order, s->keys, s->stream);
@@ -350,7 +367,7 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
         perm = s->vals;
     }
     if (timed) cudaEventRecord(s->ev[1], s->stream);
-    const bool keep = s->cfg.keep_density && s->rho;
+    const bool keep = keeps_rho(s);
     // Tiled order right after a sort: the first FFT pass deposits the particles
     // itself from the row table. Otherwise: int64 atomics (any particle order).
     const bool fused = sort && s->cfg.order == SD_ORDER_TILED;
@@ -366,6 +383,7 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
         return sim_error(s, rc);
     if (keep) s->rho_valid = true;
     if (timed) cudaEventRecord(s->ev[3], s->stream);
+    if (s->mlp_on && (rc = mlp_correction(s, perm))) return sim_error(s, rc);
     const float c2 = light_speed_sq(s->cfg.length_scale, s->cfg.time_unit_scale);
     // The mean written last step is read here as the correction for the loaded
     // velocities; the finalize kernel then overwrites it with this step's mean.
@@ -373,7 +391,7 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     float4* vel_out = perm ? s->vel2 : s->vel;
     rc = launch_gather_kick_drift(s->phi, s->G, pot_scale_of(s), s->pos, s->vel, perm, pos_out, vel_out, s->keys,
                                   s->cfg.order, s->N, dt_kick, dt_drift, c2, s->mean, s->partials, s->mom, s->mean,
-                                  s->stream);
+                                  s->stream, s->mlp_on ? s->mlp_out : nullptr);
     if (rc) return sim_error(s, rc);
     if (perm) {
         std::swap(s->pos, s->pos2);
@@ -541,6 +559,7 @@ int sd_destroy(sd_sim* s) {
     DeviceGuard g(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     free_buffers(s);
+    free_dev(s->mlp_params);
     for (auto& e : s->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : s->pev)
@@ -663,14 +682,39 @@ int sd_get_accel(sd_sim* s, float* out, int n, int where) {
     if (!s || !s->configured || !out) return fail(SD_E_STATE, "get_accel: not initialised");
     if (n < 0 || n > s->N) return fail(SD_E_ARG, "get_accel: bad n=%d", n);
     DeviceGuard g(s->device);
-    int rc = do_field(s, s->cfg.keep_density && s->rho);
+    int rc = do_field(s, keeps_rho(s));
     if (rc) return sim_error(s, rc);
+    if (s->mlp_on && (rc = mlp_correction(s, nullptr))) return sim_error(s, rc);
     float4* dst = reinterpret_cast<float4*>(out);
     float4* tmp = nullptr;
     if (where == SD_HOST) tmp = s->pos2;  // scratch: pos2 is free between steps
-    rc = launch_interpolate_accel(s->phi, s->G, pot_scale_of(s), s->pos, tmp ? tmp : dst, n, s->stream);
+    rc = launch_interpolate_accel(s->phi, s->G, pot_scale_of(s), s->pos, tmp ? tmp : dst, n, s->stream,
+                                  s->mlp_on ? s->mlp_out : nullptr);
     if (rc) return sim_error(s, rc);
     if (tmp) return copy_out(out, tmp, sizeof(float4) * (size_t)n, SD_HOST, s->stream);
+    return SD_OK;
+}
+
+int sd_set_mlp(sd_sim* s, const float* params_device, float out_scale) {
+    if (!s || !s->configured) return fail(SD_E_STATE, "set_mlp: not initialised");
+    DeviceGuard g(s->device);
+    if (s->graph) cudaGraphExecDestroy(s->graph);  // replays must see the new setting
+    s->graph = nullptr;
+    if (!params_device) {
+        s->mlp_on = false;
+        return SD_OK;
+    }
+    if (!std::isfinite(out_scale)) return fail(SD_E_ARG, "set_mlp: out_scale is not finite");
+    int rc = SD_OK;
+    if (!s->mlp_params) rc = alloc_dev(s->mlp_params, mlp_param_count());
+    if (!rc && !s->mlp_out) rc = alloc_dev(s->mlp_out, (size_t)s->N);
+    if (!rc && !s->rho) rc = alloc_dev(s->rho, (size_t)s->G * s->G * s->G);
+    if (rc) return rc;
+    if (SD_CUDA(cudaMemcpyAsync(s->mlp_params, params_device, sizeof(float) * mlp_param_count(),
+                                cudaMemcpyDeviceToDevice, s->stream)))
+        return sim_error(s, SD_E_CUDA);
+    s->mlp_scale = out_scale;
+    s->mlp_on = true;
     return SD_OK;
 }
 
@@ -790,12 +834,13 @@ int sd_synchronize(sd_sim* s) {
     if (!s || !s->configured) return fail(SD_E_STATE, "synchronize: not initialised");
     if (s->cfg.integrator != SD_INT_KDK || !s->lf_open) return SD_OK;
     DeviceGuard g(s->device);
-    int rc = do_field(s, false);
+    int rc = do_field(s, keeps_rho(s));
     if (rc) return sim_error(s, rc);
+    if (s->mlp_on && (rc = mlp_correction(s, nullptr))) return sim_error(s, rc);
     const float c2 = light_speed_sq(s->cfg.length_scale, s->cfg.time_unit_scale);
     rc = launch_gather_kick_drift(s->phi, s->G, pot_scale_of(s), s->pos, s->vel, nullptr, s->pos, s->vel, s->keys,
                                   s->cfg.order, s->N, 0.5f * s->lf_dt_prev, 0.f, c2, s->mean, s->partials, s->mom,
-                                  s->mean, s->stream);
+                                  s->mean, s->stream, s->mlp_on ? s->mlp_out : nullptr);
     if (rc) return sim_error(s, rc);
     s->mean_pending = true;
     s->lf_open = false;

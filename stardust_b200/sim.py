@@ -184,6 +184,13 @@ class Sim:
         L.check(L.lib().sd_get_accel(self._h, out.ctypes.data, n, L.SD_HOST), "sd_get_accel")
         return out
 
+    def set_correction(self, correction) -> None:
+        """Add a learned sub-grid correction (``learned.Correction``) to every
+        step's acceleration; ``None`` restores the plain PM step."""
+        from .learned import set_correction
+
+        set_correction(self, correction)
+
     # ---- stepping -----------------------------------------------------------------
     def step(self, dt: float | None = None) -> None:
         """``step()`` is the reference's CFL-clamped step; ``step(dt)`` advances by dt."""
