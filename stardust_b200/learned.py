@@ -99,6 +99,9 @@ class PMField:
         self.n = int(pos_dev.shape[0])
         self.grid = grid
         self.sim = Sim(0)
+        # the library's calls below return before their kernels finish: order
+        # them with the torch tensors that receive the results
+        self.sim.set_stream(torch.cuda.current_stream())
         self.sim.init(pm_config(self.n, grid, softening))
         vel = torch.zeros_like(pos_dev)
         self.sim.set_particles(pos_dev, vel)

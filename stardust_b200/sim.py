@@ -95,6 +95,12 @@ class Sim:
     def handle(self) -> ctypes.c_void_p:
         return self._h
 
+    def set_stream(self, stream) -> None:
+        """Run this simulation's work on ``stream`` (a CUDA stream handle as an
+        int, or a torch stream), so that it is ordered with other work there."""
+        ptr = getattr(stream, "cuda_stream", stream)
+        L.check(L.lib().sd_set_stream(self._h, ctypes.c_void_p(int(ptr))), "sd_set_stream")
+
     # ---- static queries --------------------------------------------------------
     @staticmethod
     def device_available() -> bool:
