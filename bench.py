@@ -245,7 +245,7 @@ def run_ours(args, rank, world):
     traffic = measured_traffic(dom, args.workload)
     value = world * n / (ms * 1e-3)
     out = {
-        "metric": "particle-steps/s at 16M/512^3",
+        "metric": "particle-steps/s at 16M/512^3; learned vs plain PM at equal force error vs FP64",
         "value": value,
         "unit": "particle-steps/s",
         "n_gpus": world,
@@ -279,6 +279,59 @@ def run_ours(args, rank, world):
     return out
 
 
+def run_ensemble(rank, world, steps: int = 100, warmup: int = 3, dt: float = 1e-3) -> dict:
+    """The batched ensemble: 64 seeded scenes (disk or Zel'dovich recipe, N
+    log-uniform in [16K, 1M], grids 32/64/128 matched to N), split across ranks
+    by LPT on step bytes; each rank advances its scenes with one graph launch per
+    step after autotuning. Value = all scenes' particle-steps / max-over-ranks time."""
+    import torch
+
+    from stardust_b200.ensemble import Ensemble, member_config, partition
+    from stardust_b200.scenes import ensemble_members, make_member
+
+    members = ensemble_members(64, 4)
+    mine = partition(members, world)[rank]
+    ens = Ensemble(torch.cuda.current_device())
+    n_local = 0
+    for i in mine:
+        p, v = make_member(members[i])
+        ens.add(member_config(members[i]), p, v)
+        n_local += len(p)
+    t0 = time.perf_counter()
+    tuning = ens.autotune(dt)
+    tune_s = time.perf_counter() - t0
+    ens.steps(dt, warmup)
+    ens.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    stream = torch.cuda.ExternalStream(ens.stream_handle)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ens.steps(dt, steps)
+    e1.record(stream)
+    ens.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    t = torch.tensor([ms, float(n_local)], device="cuda", dtype=torch.float64)
+    if world > 1:
+        tm = t[:1].clone()
+        torch.distributed.all_reduce(tm, op=torch.distributed.ReduceOp.MAX)
+        nt = t[1:].clone()
+        torch.distributed.all_reduce(nt, op=torch.distributed.ReduceOp.SUM)
+        ms, n_total = float(tm.item()), float(nt.item())
+    else:
+        n_total = float(n_local)
+    kernels = ens.graph_kernels()
+    ens.close()
+    tiled = sum(1 for tt in tuning if tt["order"] == "tiled")
+    return {"value": n_total / (ms * 1e-3), "unit": "particle-steps/s", "ms_per_step": ms, "steps": steps,
+            "scenes": len(members), "particles": int(n_total),
+            "grids": {str(g): sum(1 for m in members if m["grid"] == g) for g in (32, 64, 128)},
+            "graph_launches_per_step": 1, "kernels_per_graph_rank0": kernels,
+            "autotune": {"seconds": tune_s, "tiled_deposit_scenes": tiled, "atomic_deposit_scenes": len(tuning) - tiled},
+            "partition": f"LPT over {world} rank(s)"}
+
+
 def run_reference(args, rank, world):
     from oracle import oracle as O
 
@@ -298,7 +351,7 @@ def run_reference(args, rank, world):
     sec = (time.perf_counter() - t0) / steps
     value = n / sec
     return {
-        "metric": "particle-steps/s at 16M/512^3",
+        "metric": "particle-steps/s at 16M/512^3; learned vs plain PM at equal force error vs FP64",
         "value": value,
         "unit": "particle-steps/s",
         "n_gpus": world,
@@ -316,7 +369,54 @@ def run_reference(args, rank, world):
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
                          "sample": f"{steps} full step(s) of {n} particles on a {G}^3 grid"},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": reference_gpu_sample(pos, vel, G, dt),
     }
+
+
+def reference_gpu_sample(pos, vel, G: int, dt: float, steps: int = 10, warmup: int = 3) -> dict:
+    """The reference's own GPU step (its Sim class, cuFFT + CUB, built from its
+    sources for sm_100a into oracle/_ref by oracle/ref/Makefile) on the same
+    workload: a second baseline beside the CPU one. Its stock step() sizes dt by
+    the CFL rule (timeScale = dt / 0.0016) and reads vmax back every step."""
+    import ctypes
+    import tempfile
+
+    so = os.path.join(ROOT, "oracle", "_ref", "libsimref.so")
+    if not os.path.exists(so):
+        return {"unavailable": "oracle/_ref/libsimref.so was not built (the reference sources were absent)"}
+    import torch
+
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    lib = ctypes.CDLL(so)
+    lib.ref_create.restype = ctypes.c_void_p
+    lib.ref_destroy.argtypes = [ctypes.c_void_p]
+    lib.ref_load.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                             ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_char_p]
+    lib.ref_steps.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.ref_timings.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    n = len(pos)
+    h = lib.ref_create()
+    try:
+        with tempfile.TemporaryDirectory() as d:
+            rc = lib.ref_load(h, pos.ctypes.data, vel.ctypes.data, n, G, float(4 * np.pi * G ** 3), 1.0,
+                              float(dt / 0.0016), 1, os.path.join(d, "state.bin").encode())
+        if rc != 0:
+            return {"unavailable": f"reference load failed ({rc})"}
+        if lib.ref_steps(h, warmup) != 0:
+            return {"unavailable": "reference step failed"}
+        t0 = time.perf_counter()
+        if lib.ref_steps(h, steps) != 0:
+            return {"unavailable": "reference step failed"}
+        sec = (time.perf_counter() - t0) / steps
+        tm = np.zeros(6, np.float32)
+        lib.ref_timings(h, tm.ctypes.data)
+    finally:
+        lib.ref_destroy(h)
+    return {"value": n / sec, "unit": "particle-steps/s", "ms_per_step": sec * 1e3, "steps": steps,
+            "dt_used": float(tm[4]), "kind": "reference Sim (cuFFT + CUB) built for sm_100a, wall clock per step",
+            "phase_ms": {"scatter": float(tm[0]), "poisson": float(tm[1]), "gather": float(tm[2]),
+                         "total": float(tm[3])}}
 
 
 def cpu_baseline_sample(workload: str, steps: int = 8):
@@ -345,6 +445,9 @@ def main(argv=None) -> int:
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cosmic_web_512")
     ap.add_argument("--order", type=int, default=2, help="0 row-major (reference), 1 Morton, 2 tiled (fused deposit)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-scene batched ensemble")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned-correction comparison (2M particles, 128^3 + MLP vs 128..512^3)")
     args = ap.parse_args(argv)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -362,6 +465,12 @@ def main(argv=None) -> int:
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     out = run_ours(args, rank, world)
+    if not args.no_ensemble:
+        out["ensemble"] = run_ensemble(rank, world)
+    if world == 1 and not args.no_learned:
+        from stardust_b200.learned import compare
+
+        out["learned"] = compare()
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_sample(args.workload)
     if world > 1:

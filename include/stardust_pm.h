@@ -289,6 +289,35 @@ int sd_mlp_adam(float* params, float* m, float* v, const float* grad, int step, 
  * step-start density), which this call switches on. */
 int sd_set_mlp(sd_sim* sim, const float* params_device, float out_scale);
 
+/* ---- batched ensemble (no counterpart in the reference: one Sim per scene) --
+ * Independent periodic scenes of any particle count and grid size, advanced
+ * together. One step of the ensemble is one CUDA graph launch: a fork, one
+ * branch per scene holding that scene's whole step, a join; scenes run side by
+ * side on the GPU. Scenes are ordinary sd_sim handles owned by the ensemble
+ * (sd_ensemble_scene), so every per-scene query works on them. Each scene's
+ * density is the same fixed-point sum as when it runs alone (bit-exact). */
+typedef struct sd_ensemble sd_ensemble;
+typedef struct sd_scene_tuning {
+    int order;          /* SD_ORDER_TILED (fused deposit) or SD_ORDER_ROWMAJOR (atomic deposit) */
+    int gather_blocks;  /* gather grid cap in CTAs (0: one CTA per 256 particles, at most 4096) */
+    float step_ms;      /* median step time of the chosen variant alone; -1 before tuning */
+    int reserved;
+} sd_scene_tuning;
+int sd_ensemble_create(sd_ensemble** out, int device);
+int sd_ensemble_destroy(sd_ensemble* ens);
+/* adds a scene (sort_interval 0 or 1, diagnostics off); returns its index or a negative status */
+int sd_ensemble_add(sd_ensemble* ens, const sd_config* cfg, const float* pos, const float* vel, int n, int where);
+int sd_ensemble_size(const sd_ensemble* ens);
+sd_sim* sd_ensemble_scene(sd_ensemble* ens, int index);
+/* times each scene's deposit path and gather grid on a snapshot (restored) and keeps the fastest */
+int sd_ensemble_autotune(sd_ensemble* ens, float dt, int reps);
+int sd_ensemble_get_tuning(const sd_ensemble* ens, int index, sd_scene_tuning* out);
+/* nsteps steps of every scene: one graph launch per step, no host synchronisation */
+int sd_ensemble_steps(sd_ensemble* ens, float dt, int nsteps);
+int sd_ensemble_synchronize(sd_ensemble* ens);
+void* sd_ensemble_stream(const sd_ensemble* ens);
+long long sd_ensemble_graph_kernels(const sd_ensemble* ens);
+
 /* ---- FP64 reference forces (force-error judge; not on the step) ------------
  * Periodic Newtonian accelerations (G = 1, each source of mass 1/n_src, mean
  * density removed) of Gaussian-smoothed masses of width `softening` (box units;

@@ -54,6 +54,11 @@ class SdTimings(ctypes.Structure):
     ]
 
 
+class SdSceneTuning(ctypes.Structure):
+    _fields_ = [("order", ctypes.c_int32), ("gather_blocks", ctypes.c_int32), ("step_ms", ctypes.c_float),
+                ("reserved", ctypes.c_int32)]
+
+
 class SdDiagnostics(ctypes.Structure):
     _fields_ = [
         ("kinetic", ctypes.c_double),
@@ -129,6 +134,17 @@ SIGNATURES = [
     ("sd_mlp_loss_grad", _I, [_P, _P, _P, _I, _P, _P, _P, _S, _P]),
     ("sd_mlp_adam", _I, [_P, _P, _P, _P, _I, _F, _F, _F, _F, _P]),
     ("sd_set_mlp", _I, [_P, _P, _F]),
+    ("sd_ensemble_create", _I, [_P, _I]),
+    ("sd_ensemble_destroy", _I, [_P]),
+    ("sd_ensemble_add", _I, [_P, _P, _P, _P, _I, _I]),
+    ("sd_ensemble_size", _I, [_P]),
+    ("sd_ensemble_scene", _P, [_P, _I]),
+    ("sd_ensemble_autotune", _I, [_P, _F, _I]),
+    ("sd_ensemble_get_tuning", _I, [_P, _I, _P]),
+    ("sd_ensemble_steps", _I, [_P, _F, _I]),
+    ("sd_ensemble_synchronize", _I, [_P]),
+    ("sd_ensemble_stream", _P, [_P]),
+    ("sd_ensemble_graph_kernels", _LL, [_P]),
     ("sd_ewald_modes", _I, [_I]),
     ("sd_ewald_workspace_bytes", _S, [_I]),
     ("sd_ewald_forces", _I, [_P, _I, _P, _I, _D, _D, _I, _P, _P, _S, _P]),

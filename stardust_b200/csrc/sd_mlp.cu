@@ -66,7 +66,7 @@ __device__ __forceinline__ void particle_features(const float* __restrict__ rho,
             for (int dx = -1; dx <= 1; ++dx) {
                 const float r =
                     __ldg(rho + ((size_t)((cz + dz) & m) * G + ((cy + dy) & m)) * G + ((cx + dx) & m));
-                f[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] = log1pf(r * inv_mean) - ln2;
+                f[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] = __logf(1.f + r * inv_mean) - ln2;
             }
     f[27] = p.x * (float)G - (float)cx - 0.5f;
     f[28] = p.y * (float)G - (float)cy - 0.5f;
@@ -108,7 +108,71 @@ __device__ __forceinline__ uint2 b_frag(const float* W, int N, int kc, int nt, i
 }
 
 constexpr int kInferWarps = 8;
+constexpr int kXPad = kIn + 8;  // bf16 row stride of the feature tile: 80 B, conflict-light fragment loads
 
+// Output rows [r0, r0 + 16) of the warp's feature tile through the three layers;
+// y[] receives rows r0 + g and r0 + g + 8, columns 2t, 2t + 1 (no bias).
+__device__ __forceinline__ void mlp_tile(const __nv_bfloat16 (*xs)[kXPad], int r0, const uint2* f1, const uint2* f2,
+                                         const uint2* f3, const float* bias, int lane, float (&y)[4]) {
+    const int g = lane >> 2, t = lane & 3;
+    float acc[kH / 8][4];
+#pragma unroll
+    for (int nt = 0; nt < kH / 8; ++nt)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[nt][q] = 0.f;
+#pragma unroll
+    for (int kc = 0; kc < kIn / 16; ++kc) {
+        unsigned a[4];
+        a[0] = *reinterpret_cast<const unsigned*>(&xs[r0 + g][16 * kc + 2 * t]);
+        a[1] = *reinterpret_cast<const unsigned*>(&xs[r0 + g + 8][16 * kc + 2 * t]);
+        a[2] = *reinterpret_cast<const unsigned*>(&xs[r0 + g][16 * kc + 2 * t + 8]);
+        a[3] = *reinterpret_cast<const unsigned*>(&xs[r0 + g + 8][16 * kc + 2 * t + 8]);
+#pragma unroll
+        for (int nt = 0; nt < kH / 8; ++nt) {
+            const uint2 b = f1[(kc * (kH / 8) + nt) * 32 + lane];
+            mma16816(acc[nt], a, b.x, b.y);
+        }
+    }
+    // bias + SiLU; the C fragments of n-tiles (2j, 2j+1) are the A fragment of k-chunk j
+    unsigned h[kH / 16][4];
+#pragma unroll
+    for (int j = 0; j < kH / 16; ++j) {
+        const int c0 = 16 * j + 2 * t, c1 = c0 + 8;
+        h[j][0] = pack_bf16(silu(acc[2 * j][0] + bias[c0]), silu(acc[2 * j][1] + bias[c0 + 1]));
+        h[j][1] = pack_bf16(silu(acc[2 * j][2] + bias[c0]), silu(acc[2 * j][3] + bias[c0 + 1]));
+        h[j][2] = pack_bf16(silu(acc[2 * j + 1][0] + bias[c1]), silu(acc[2 * j + 1][1] + bias[c1 + 1]));
+        h[j][3] = pack_bf16(silu(acc[2 * j + 1][2] + bias[c1]), silu(acc[2 * j + 1][3] + bias[c1 + 1]));
+    }
+#pragma unroll
+    for (int nt = 0; nt < kH / 8; ++nt)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[nt][q] = 0.f;
+#pragma unroll
+    for (int kc = 0; kc < kH / 16; ++kc)
+#pragma unroll
+        for (int nt = 0; nt < kH / 8; ++nt) {
+            const uint2 b = f2[(kc * (kH / 8) + nt) * 32 + lane];
+            mma16816(acc[nt], h[kc], b.x, b.y);
+        }
+#pragma unroll
+    for (int j = 0; j < kH / 16; ++j) {
+        const int c0 = 16 * j + 2 * t, c1 = c0 + 8;
+        h[j][0] = pack_bf16(silu(acc[2 * j][0] + bias[kH + c0]), silu(acc[2 * j][1] + bias[kH + c0 + 1]));
+        h[j][1] = pack_bf16(silu(acc[2 * j][2] + bias[kH + c0]), silu(acc[2 * j][3] + bias[kH + c0 + 1]));
+        h[j][2] = pack_bf16(silu(acc[2 * j + 1][0] + bias[kH + c1]), silu(acc[2 * j + 1][1] + bias[kH + c1 + 1]));
+        h[j][3] = pack_bf16(silu(acc[2 * j + 1][2] + bias[kH + c1]), silu(acc[2 * j + 1][3] + bias[kH + c1 + 1]));
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) y[q] = 0.f;
+#pragma unroll
+    for (int kc = 0; kc < kH / 16; ++kc) {
+        const uint2 b = f3[kc * 32 + lane];
+        mma16816(y, h[kc], b.x, b.y);
+    }
+}
+
+// 32 particles per warp pass: every lane builds one particle's features, then
+// the warp runs two 16-row tiles through the network on the tensor cores.
 __global__ void __launch_bounds__(kInferWarps * 32) k_mlp_infer(const float* __restrict__ params,
                                                                const float4* __restrict__ pos,
                                                                const int* __restrict__ perm, int n,
@@ -116,8 +180,8 @@ __global__ void __launch_bounds__(kInferWarps * 32) k_mlp_infer(const float* __r
                                                                float out_scale, float4* __restrict__ out) {
     __shared__ uint2 f1[kFragW1], f2[kFragW2], f3[kFragW3];
     __shared__ float bias[kH + kH + kOut];
-    __shared__ __nv_bfloat16 xs[kInferWarps][16][kIn + 8];  // +8: rows 80 B apart, conflict-light
-    __shared__ float ys[kInferWarps][16][4];
+    __shared__ __nv_bfloat16 xs[kInferWarps][32][kXPad];
+    __shared__ float ys[kInferWarps][32][4];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < kFragW1; i += blockDim.x) {
         const int l = i & 31, nt = (i >> 5) % (kH / 8), kc = (i >> 5) / (kH / 8);
@@ -139,14 +203,13 @@ __global__ void __launch_bounds__(kInferWarps * 32) k_mlp_infer(const float* __r
     __syncthreads();
 
     const int g = lane >> 2, t = lane & 3;
-    const int tiles = (n + 15) / 16;
-    for (int tile = blockIdx.x * kInferWarps + w; tile < tiles; tile += gridDim.x * kInferWarps) {
-        const int i0 = tile * 16;
-        if (lane < 16) {
-            const int i = i0 + lane;
+    const int passes = (n + 31) / 32;
+    for (int ps = blockIdx.x * kInferWarps + w; ps < passes; ps += gridDim.x * kInferWarps) {
+        const int i = ps * 32 + lane;
+        float4 p = make_float4(-1.f, -1.f, -1.f, 0.f);
+        if (i < n) p = pos[perm ? perm[i] : i];
+        {
             float f[32];
-            float4 p = make_float4(-1.f, -1.f, -1.f, 0.f);
-            if (i < n) p = pos[perm ? perm[i] : i];
             if (p.x < 0.f) {
 #pragma unroll
                 for (int j = 0; j < 32; ++j) f[j] = 0.f;
@@ -154,83 +217,30 @@ __global__ void __launch_bounds__(kInferWarps * 32) k_mlp_infer(const float* __r
                 particle_features(rho, G, inv_mean, p, f);
             }
 #pragma unroll
-            for (int j = 0; j < 32; j += 2)
-                *reinterpret_cast<unsigned*>(&xs[w][lane][j]) = pack_bf16(f[j], f[j + 1]);
+            for (int j = 0; j < 32; j += 8)
+                *reinterpret_cast<uint4*>(&xs[w][lane][j]) =
+                    make_uint4(pack_bf16(f[j], f[j + 1]), pack_bf16(f[j + 2], f[j + 3]),
+                               pack_bf16(f[j + 4], f[j + 5]), pack_bf16(f[j + 6], f[j + 7]));
         }
         __syncwarp();
-        // layer 1: A fragments of X (rows g, g+8; cols 2t, 2t+1 and +8 within each k-chunk)
-        float acc1[kH / 8][4];
-#pragma unroll
-        for (int nt = 0; nt < kH / 8; ++nt)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc1[nt][q] = 0.f;
-#pragma unroll
-        for (int kc = 0; kc < kIn / 16; ++kc) {
-            unsigned a[4];
-            a[0] = *reinterpret_cast<const unsigned*>(&xs[w][g][16 * kc + 2 * t]);
-            a[1] = *reinterpret_cast<const unsigned*>(&xs[w][g + 8][16 * kc + 2 * t]);
-            a[2] = *reinterpret_cast<const unsigned*>(&xs[w][g][16 * kc + 2 * t + 8]);
-            a[3] = *reinterpret_cast<const unsigned*>(&xs[w][g + 8][16 * kc + 2 * t + 8]);
-#pragma unroll
-            for (int nt = 0; nt < kH / 8; ++nt) {
-                const uint2 b = f1[(kc * (kH / 8) + nt) * 32 + lane];
-                mma16816(acc1[nt], a, b.x, b.y);
-            }
-        }
-        // bias + SiLU; the C fragments of n-tiles (2j, 2j+1) are the A fragment of k-chunk j
-        unsigned h1[kH / 16][4];
-#pragma unroll
-        for (int j = 0; j < kH / 16; ++j) {
-            const int c0 = 16 * j + 2 * t, c1 = c0 + 8;
-            h1[j][0] = pack_bf16(silu(acc1[2 * j][0] + bias[c0]), silu(acc1[2 * j][1] + bias[c0 + 1]));
-            h1[j][1] = pack_bf16(silu(acc1[2 * j][2] + bias[c0]), silu(acc1[2 * j][3] + bias[c0 + 1]));
-            h1[j][2] = pack_bf16(silu(acc1[2 * j + 1][0] + bias[c1]), silu(acc1[2 * j + 1][1] + bias[c1 + 1]));
-            h1[j][3] = pack_bf16(silu(acc1[2 * j + 1][2] + bias[c1]), silu(acc1[2 * j + 1][3] + bias[c1 + 1]));
-        }
-        float acc2[kH / 8][4];
-#pragma unroll
-        for (int nt = 0; nt < kH / 8; ++nt)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc2[nt][q] = 0.f;
-#pragma unroll
-        for (int kc = 0; kc < kH / 16; ++kc)
-#pragma unroll
-            for (int nt = 0; nt < kH / 8; ++nt) {
-                const uint2 b = f2[(kc * (kH / 8) + nt) * 32 + lane];
-                mma16816(acc2[nt], h1[kc], b.x, b.y);
-            }
-        unsigned h2[kH / 16][4];
-#pragma unroll
-        for (int j = 0; j < kH / 16; ++j) {
-            const int c0 = 16 * j + 2 * t, c1 = c0 + 8;
-            h2[j][0] = pack_bf16(silu(acc2[2 * j][0] + bias[kH + c0]), silu(acc2[2 * j][1] + bias[kH + c0 + 1]));
-            h2[j][1] = pack_bf16(silu(acc2[2 * j][2] + bias[kH + c0]), silu(acc2[2 * j][3] + bias[kH + c0 + 1]));
-            h2[j][2] = pack_bf16(silu(acc2[2 * j + 1][0] + bias[kH + c1]), silu(acc2[2 * j + 1][1] + bias[kH + c1 + 1]));
-            h2[j][3] = pack_bf16(silu(acc2[2 * j + 1][2] + bias[kH + c1]), silu(acc2[2 * j + 1][3] + bias[kH + c1 + 1]));
-        }
-        float y[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-        for (int kc = 0; kc < kH / 16; ++kc) {
-            const uint2 b = f3[kc * 32 + lane];
-            mma16816(y, h2[kc], b.x, b.y);
-        }
-        // y: rows g, g+8; cols 2t, 2t+1 (outputs 0..2 are meaningful)
-        if (t < 2) {
-            ys[w][g][2 * t] = y[0] + bias[2 * kH + 2 * t];
-            ys[w][g + 8][2 * t] = y[2] + bias[2 * kH + 2 * t];
-            if (2 * t + 1 < 4) {
-                ys[w][g][2 * t + 1] = y[1] + bias[2 * kH + 2 * t + 1];
-                ys[w][g + 8][2 * t + 1] = y[3] + bias[2 * kH + 2 * t + 1];
+#pragma unroll 1
+        for (int half = 0; half < 2; ++half) {
+            float y[4];
+            mlp_tile(xs[w], 16 * half, f1, f2, f3, bias, lane, y);
+            // y: rows g, g+8 of this half; cols 2t, 2t+1 (outputs 0..2 are meaningful)
+            if (t < 2) {
+                const int r = 16 * half + g;
+                ys[w][r][2 * t] = y[0] + bias[2 * kH + 2 * t];
+                ys[w][r][2 * t + 1] = y[1] + bias[2 * kH + 2 * t + 1];
+                ys[w][r + 8][2 * t] = y[2] + bias[2 * kH + 2 * t];
+                ys[w][r + 8][2 * t + 1] = y[3] + bias[2 * kH + 2 * t + 1];
             }
         }
         __syncwarp();
-        if (lane < 16 && i0 + lane < n) {
-            const int i = i0 + lane;
-            const bool live = pos[perm ? perm[i] : i].x >= 0.f;
-            out[i] = live ? make_float4(ys[w][lane][0] * out_scale, ys[w][lane][1] * out_scale,
-                                        ys[w][lane][2] * out_scale, 0.f)
-                          : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
+        if (i < n)
+            out[i] = (p.x >= 0.f) ? make_float4(ys[w][lane][0] * out_scale, ys[w][lane][1] * out_scale,
+                                                ys[w][lane][2] * out_scale, 0.f)
+                                  : make_float4(0.f, 0.f, 0.f, 0.f);
         __syncwarp();
     }
 }
@@ -382,8 +392,8 @@ size_t mlp_param_count() { return kParams; }
 int launch_mlp_infer(const float* params, const float4* pos, const int* perm, int n, const float* rho, int G,
                      float inv_mean, float out_scale, float4* out, cudaStream_t s) {
     if (n <= 0) return SD_OK;
-    const int tiles = (n + 15) / 16;
-    int blocks = (tiles + kInferWarps - 1) / kInferWarps;
+    const int passes = (n + 31) / 32;
+    int blocks = (passes + kInferWarps - 1) / kInferWarps;
     if (blocks > 148 * 8) blocks = 148 * 8;
     k_mlp_infer<<<blocks, kInferWarps * 32, 0, s>>>(params, pos, perm, n, rho, G, inv_mean, out_scale, out);
     SD_LAUNCHED(s);

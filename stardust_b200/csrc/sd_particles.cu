@@ -441,10 +441,12 @@ size_t gather_partials(int n) {
 int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const float4* pos_in, const float4* vel_in,
                              const int* perm, float4* pos_out, float4* vel_out, uint32_t* keys_out, int order, int n,
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
-                             double* mom_out, float* mean_out, cudaStream_t s, const float4* extra) {
+                             double* mom_out, float* mean_out, cudaStream_t s, const float4* extra,
+                             int max_blocks) {
     if (n <= 0) return SD_OK;
     const float h = (0.5f * (float)G) * pot_scale;  // Sim.cu:604
-    const int blocks = (int)gather_partials(n);
+    int blocks = (int)gather_partials(n);
+    if (max_blocks > 0 && blocks > max_blocks) blocks = max_blocks;
     k_gather_kick_drift<<<blocks, kGatherThreads, 0, s>>>(phi, G, h, pos_in, vel_in, perm, pos_out, vel_out, keys_out,
                                                           order, n, dt_kick, dt_drift, c2, mean_vel, partials, extra);
     SD_LAUNCHED(s);

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "sd_internal.h"
+#include "sd_sim_impl.h"
 
 // ---------------------------------------------------------------------------
 // sticky error record and launch accounting
@@ -63,79 +64,16 @@ long long launches() { return g_launches.load(std::memory_order_relaxed); }
 
 using namespace sd;
 
-// ---------------------------------------------------------------------------
-// handle
-// ---------------------------------------------------------------------------
-struct sd_sim {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    bool configured = false;
-    bool cuda_failed = false;
-    sd_config cfg{};
-    int N = 0;          // slots (allocN)
-    int G = 0;
-    int active = 0;     // slots loaded by the last set_particles / load_state
-    double sim_time = 0.0;
-    int step_count = 0;
+namespace sdsim {
 
-    float4 *pos = nullptr, *vel = nullptr, *pos2 = nullptr, *vel2 = nullptr;
-    uint32_t *keys = nullptr, *keys2 = nullptr, *keys3 = nullptr;
-    int32_t *vals = nullptr, *vals2 = nullptr;
-    void* sort_ws = nullptr;
-    size_t sort_ws_bytes = 0;
-    long long* acc = nullptr;
-    int* row_start = nullptr;    // key-space row starts of the sorted particles (tiled order)
-    float2* spec = nullptr;     // bricked spectrum, transformed in place
-    float* phi = nullptr;
-    float* rho = nullptr;        // kept density (keep_density)
-    double* partials = nullptr;  // gather / energy / reduction partials
-    size_t partials_count = 0;
-    double* mom = nullptr;       // 8 doubles: momentum sums of the last step, energy results
-    float* mean = nullptr;       // 4 floats: pending mean velocity; [3] = max speed scratch
-    bool mean_pending = false;
-    bool rho_valid = false;
-    bool keys_valid = false;     // keys hold the order keys of the current pos order
-    PoissonPlan plan;
-
-    // leapfrog
-    bool lf_open = false;
-    float lf_dt_prev = 0.f;
-
-    // timings of the last eager step: ev[0..4] phase bounds, pev[0..3] after Poisson passes A-D
-    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    cudaEvent_t pev[4] = {nullptr, nullptr, nullptr, nullptr};
-    bool ev_valid = false;
-    sd_timings tm{};
-    sd_diagnostics diag{};
-    bool diag_valid = false;
-
-    // learned correction (sd_set_mlp): device copy of the parameters, per-slot output
-    float* mlp_params = nullptr;
-    float4* mlp_out = nullptr;
-    float mlp_scale = 0.f;
-    bool mlp_on = false;
-
-    // captured steps for sd_steps
-    cudaGraphExec_t graph = nullptr;
-    float graph_dt = 0.f;
-    const float4* graph_pos = nullptr;  // particle buffer the graph's first step reads
-    long long graph_launches = 0;       // kernels inside one replay
-};
-
-namespace {
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-    }
-};
+DeviceGuard::DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+}
+DeviceGuard::~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+}
 
 int ceil_pow2_clamp(int g, int cap) {
     if (g <= 0) g = 64;
@@ -391,7 +329,7 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     float4* vel_out = perm ? s->vel2 : s->vel;
     rc = launch_gather_kick_drift(s->phi, s->G, pot_scale_of(s), s->pos, s->vel, perm, pos_out, vel_out, s->keys,
                                   s->cfg.order, s->N, dt_kick, dt_drift, c2, s->mean, s->partials, s->mom, s->mean,
-                                  s->stream, s->mlp_on ? s->mlp_out : nullptr);
+                                  s->stream, s->mlp_on ? s->mlp_out : nullptr, s->gather_blocks);
     if (rc) return sim_error(s, rc);
     if (perm) {
         std::swap(s->pos, s->pos2);
@@ -475,7 +413,9 @@ struct StateHeader {
 static_assert(sizeof(StateHeader) == 76, "STARDUST header layout");
 constexpr size_t kBlackHoleRecord = 48;  // sizeof(BlackHoleState) (Sim.h:813-825)
 
-}  // namespace
+}  // namespace sdsim
+
+using namespace sdsim;
 
 // ---------------------------------------------------------------------------
 // C ABI

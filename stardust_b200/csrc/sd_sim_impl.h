@@ -1,0 +1,84 @@
+// sd_sim_impl.h -- the simulation handle's state, shared by sd_sim.cu (the
+// single-scene C ABI) and sd_ensemble.cu (many scenes in one graph).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "sd_internal.h"
+#include "stardust_pm.h"
+
+struct sd_sim {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    bool configured = false;
+    bool cuda_failed = false;
+    sd_config cfg{};
+    int N = 0;          // slots (allocN)
+    int G = 0;
+    int active = 0;     // slots loaded by the last set_particles / load_state
+    double sim_time = 0.0;
+    int step_count = 0;
+
+    float4 *pos = nullptr, *vel = nullptr, *pos2 = nullptr, *vel2 = nullptr;
+    uint32_t *keys = nullptr, *keys2 = nullptr, *keys3 = nullptr;
+    int32_t *vals = nullptr, *vals2 = nullptr;
+    void* sort_ws = nullptr;
+    size_t sort_ws_bytes = 0;
+    long long* acc = nullptr;
+    int* row_start = nullptr;    // key-space row starts of the sorted particles (tiled order)
+    float2* spec = nullptr;     // bricked spectrum, transformed in place
+    float* phi = nullptr;
+    float* rho = nullptr;        // kept density (keep_density)
+    double* partials = nullptr;  // gather / energy / reduction partials
+    size_t partials_count = 0;
+    double* mom = nullptr;       // 8 doubles: momentum sums of the last step, energy results
+    float* mean = nullptr;       // 4 floats: pending mean velocity; [3] = max speed scratch
+    bool mean_pending = false;
+    bool rho_valid = false;
+    bool keys_valid = false;     // keys hold the order keys of the current pos order
+    sd::PoissonPlan plan;
+
+    // leapfrog
+    bool lf_open = false;
+    float lf_dt_prev = 0.f;
+
+    // timings of the last eager step: ev[0..4] phase bounds, pev[0..3] after Poisson passes A-D
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t pev[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool ev_valid = false;
+    sd_timings tm{};
+    sd_diagnostics diag{};
+    bool diag_valid = false;
+
+    // learned correction (sd_set_mlp): device copy of the parameters, per-slot output
+    float* mlp_params = nullptr;
+    float4* mlp_out = nullptr;
+    float mlp_scale = 0.f;
+    bool mlp_on = false;
+
+    int gather_blocks = 0;   // cap of the gather grid (0: the default); set by the ensemble autotuner
+
+    // captured steps for sd_steps
+    cudaGraphExec_t graph = nullptr;
+    float graph_dt = 0.f;
+    const float4* graph_pos = nullptr;  // particle buffer the graph's first step reads
+    long long graph_launches = 0;       // kernels inside one replay
+};
+
+
+namespace sdsim {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev);
+    ~DeviceGuard();
+};
+
+int sim_error(sd_sim* s, int rc);
+bool sort_due(const sd_sim* s);
+int key_bits_for(int G, int order);
+// One step of one scene on s->stream (no host synchronisation; capturable).
+int do_step(sd_sim* s, float dt, bool sort, bool timed);
+
+}  // namespace sdsim

@@ -22,6 +22,7 @@ is the exact answer both approximate.
 from __future__ import annotations
 
 import ctypes
+import json
 import math
 import time
 from dataclasses import dataclass
@@ -87,8 +88,9 @@ def _torch():
 
 def pm_config(n: int, grid: int, softening: float, **kw) -> SimConfig:
     """Newtonian PM configuration of the periodic unit box (G = 1, total mass 1)."""
+    kw.setdefault("keep_density", 1)
     return SimConfig(particle_count=n, grid_size=grid, gravity=1.0, softening_cells=softening * grid,
-                     units=L.SD_UNITS_NEWTON, order=L.SD_ORDER_TILED, keep_density=1, **kw)
+                     units=L.SD_UNITS_NEWTON, order=L.SD_ORDER_TILED, **kw)
 
 
 class PMField:
@@ -215,3 +217,90 @@ def train(X, T, epochs: int = 12, batch: int = 16384, lr: float = 2e-3, seed: in
         if log:
             log(f"epoch {ep}: rms residual left {rel:.4f}")
     return p.cpu().numpy(), out_scale, history
+
+
+def step_rate(pos, vel, grid: int, softening: float, correction: Correction | None = None, dt: float = 1e-3,
+              steps: int = 20, warmup: int = 4) -> float:
+    """Particle-steps/s of the full step (sort, deposit, Poisson, [correction],
+    gather) through the captured-graph path, timed with CUDA events."""
+    torch = _torch()
+    n = len(pos)
+    stream = torch.cuda.Stream()
+    with Sim(0) as sim:
+        sim.set_stream(stream)
+        sim.init(pm_config(n, grid, softening, sort_interval=1, keep_density=0 if correction is None else 1))
+        sim.set_particles(pos, vel)
+        if correction is not None:
+            sim.set_correction(correction)
+        sim.steps(dt, warmup)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.steps(dt, steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return n / (e0.elapsed_time(e1) * 1e-3 / steps)
+
+
+def equal_error_rate(err: float, plain: dict) -> float | None:
+    """Particle-steps/s plain PM would need for force error `err`: log-log
+    interpolation between the grids that bracket it (None outside them)."""
+    gs = sorted(plain)
+    for a, b in zip(gs, gs[1:]):
+        ea, eb = plain[a]["error"], plain[b]["error"]
+        if eb <= err <= ea:
+            t = (math.log(ea) - math.log(err)) / (math.log(ea) - math.log(eb))
+            return math.exp((1 - t) * math.log(plain[a]["rate"]) + t * math.log(plain[b]["rate"]))
+    return None
+
+
+def compare(train_seeds=range(8), eval_seed: int = 1000, n_side: int = 128, coarse: int = 128, fine: int = 512,
+            softening: float = 1.0 / 128, n_targets: int = 65_536, epochs: int = 10, steps: int = 20,
+            log=None) -> dict:
+    """Train on (coarse, fine) pairs of `train_seeds`, then judge plain PM on
+    coarse..fine grids and coarse + correction on a held-out scene against FP64
+    Ewald forces at `n_targets` particles, and time each step."""
+    torch = _torch()
+    from .ewald import ewald_forces, force_error
+
+    t0 = time.time()
+    X, T = training_pairs(train_seeds, n_side, coarse, fine, softening)
+    params, scale, hist = train(X, T, epochs=epochs)
+    del X, T
+    corr = Correction(params, scale, softening, coarse, fine)
+    t_train = time.time() - t0
+    pos, vel = zeldovich(n_side, eval_seed)
+    pd = torch.from_numpy(pos).cuda()
+    tgt = np.sort(np.random.default_rng(eval_seed).choice(len(pos), n_targets, replace=False))
+    ref = ewald_forces(pd, pd[torch.from_numpy(tgt).cuda()].contiguous(), softening)
+    plain = {}
+    g = coarse
+    while g <= fine:
+        f = PMField(pd, g, softening)
+        e = force_error(f.accel().cpu().numpy()[tgt], ref)
+        f.close()
+        plain[g] = {"error": e["rms_rel"], "max_error": e["max_rel"], "rate": step_rate(pos, vel, g, softening,
+                                                                                          steps=steps)}
+        g *= 2
+    f = PMField(pd, coarse, softening, corr)
+    e = force_error(f.accel().cpu().numpy()[tgt], ref)
+    f.close()
+    learned = {"error": e["rms_rel"], "max_error": e["max_rel"],
+               "rate": step_rate(pos, vel, coarse, softening, corr, steps=steps)}
+    eq = equal_error_rate(learned["error"], plain)
+    out = {
+        "scene": f"Zel'dovich {n_side}^3 lattice (seed {eval_seed}), softening {softening:.6g} box",
+        "judge": f"FP64 Ewald, {n_targets} targets, all {len(pos)} sources",
+        "plain": {str(k): v for k, v in plain.items()},
+        "learned": learned,
+        "train": {"seeds": list(train_seeds), "pairs": f"{coarse}^3 vs {fine}^3", "epochs": epochs,
+                  "rms_residual_left": hist[-1], "seconds": t_train, "out_scale": scale},
+        "error_gain": plain[coarse]["error"] / learned["error"],
+        "speed_vs_fine": learned["rate"] / plain[fine]["rate"],
+        "reaches_fine_error": learned["error"] <= plain[fine]["error"],
+        "speed_vs_plain_at_equal_error": (learned["rate"] / eq) if eq else None,
+    }
+    if log:
+        log(json.dumps(out))
+    return out
