@@ -150,16 +150,19 @@ __global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4
     constexpr int H = T::H, NBX = T::NBX, NT = kDepositThreads;
     extern __shared__ float2 sm[];
     float2* tw = sm;
-    // The int64 fixed-point sums, as two 32-bit words per cell (lo[16][G], hi[16][G]),
+    // The int64 fixed-point sums, as two 32-bit words per cell (lo[16][RS], hi[16][RS]),
     // share their storage with the complex line buffer used after the conversion.
+    // Rows are RS = G + 4 words apart, so the row-parallel 16-byte reads of the
+    // conversion fall in different banks.
+    constexpr int RS = G + 4;
     unsigned* acc_lo = reinterpret_cast<unsigned*>(sm + G);
-    unsigned* acc_hi = acc_lo + 16 * G;
+    unsigned* acc_hi = acc_lo + 16 * RS;
     float2* s = sm + G;
     __shared__ int range_lo[25], range_off[26];
     const int by = blockIdx.x, bz = blockIdx.y;
     const int m = G - 1;
     for (int i = threadIdx.x; i < G; i += NT) tw[i] = tw_g[i];
-    for (int i = threadIdx.x; i < 8 * G; i += NT) reinterpret_cast<uint4*>(acc_lo)[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (int i = threadIdx.x; i < 8 * RS; i += NT) reinterpret_cast<uint4*>(acc_lo)[i] = make_uint4(0u, 0u, 0u, 0u);
     if (threadIdx.x < 32) {
         // source rows (iy, iz) = (4by - 1 + j % 5, 4bz - 1 + j / 5), j < 25
         const int j = threadIdx.x;
@@ -216,7 +219,7 @@ __global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4
                 const int yl = ((iy + oy) & m) - 4 * by;
                 const int zl = ((iz + oz) & m) - 4 * bz;
                 if ((unsigned)yl >= 4u || (unsigned)zl >= 4u) continue;
-                const int rowc = (zl * 4 + yl) * G;
+                const int rowc = (zl * 4 + yl) * RS;
 #pragma unroll
                 for (int ox = 0; ox < 2; ++ox) {
                     const unsigned long long q =
@@ -251,8 +254,8 @@ __global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4
         const int u = threadIdx.x + p * NT;
         if (CITEMS % NT == 0 || u < CITEMS) {
             const int l = u & 15, mp = u >> 4;
-            const uint4 lo = *reinterpret_cast<const uint4*>(acc_lo + l * G + 4 * mp);
-            const uint4 hi = *reinterpret_cast<const uint4*>(acc_hi + l * G + 4 * mp);
+            const uint4 lo = *reinterpret_cast<const uint4*>(acc_lo + l * RS + 4 * mp);
+            const uint4 hi = *reinterpret_cast<const uint4*>(acc_hi + l * RS + 4 * mp);
             const int sh = split16 ? 16 : 32;
             cv[p] = make_float4(fixed_to_float((long long)(((unsigned long long)hi.x << sh) + lo.x)),
                                 fixed_to_float((long long)(((unsigned long long)hi.y << sh) + lo.y)),
@@ -366,7 +369,7 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_y(float2* __restrict__ spe
 
 // ---- pass C: z-lines of CTA (bx, by): forward, Green's function, inverse ---------
 template <int G>
-__global__ void __launch_bounds__(kFftThreads) k_pass_c(float2* __restrict__ spec, const float2* __restrict__ tw_g,
+__global__ void __launch_bounds__(kFftThreads, 3) k_pass_c(float2* __restrict__ spec, const float2* __restrict__ tw_g,
                                                         const float* __restrict__ gexp_g, float scale) {
     using T = Geo<G>;
     constexpr int H = T::H;
@@ -466,9 +469,9 @@ struct Launcher {
     static size_t smem_ae() { return sizeof(float2) * ((size_t)G + 16 * (size_t)T::PX); }
     static size_t smem_bd() { return sizeof(float2) * ((size_t)G + 16 * (size_t)G); }
     static size_t smem_c() { return sizeof(float2) * ((size_t)G + (T::H + 2) / 2 + 1 + 16 * (size_t)G); }
-    // the line buffer (16 * PX float2) overlays the 32-bit sum words (2 * 16 * G)
+    // the line buffer (16 * PX float2) overlays the 32-bit sum words (2 * 16 * (G + 4))
     static size_t smem_dep() {
-        const size_t lines = sizeof(float2) * 16 * (size_t)T::PX, sums = 2 * sizeof(unsigned) * 16 * (size_t)G;
+        const size_t lines = sizeof(float2) * 16 * (size_t)T::PX, sums = 2 * sizeof(unsigned) * 16 * (size_t)(G + 4);
         return sizeof(float2) * (size_t)G + (lines > sums ? lines : sums);
     }
 

@@ -7,10 +7,12 @@
 // width is split into the fewest passes of at most 10 bits), written for
 // sm_100a, in three kernels per digit pass:
 //   1. k_digit_counts: each 2048-key tile counts its digits in shared memory and
-//      writes them digit-major (count[d * tiles + t]);
-//   2. an exclusive scan of that digit-major array gives, for every (digit,tile),
-//      the global output offset -- digit-major order is what makes the result
-//      stable across tiles;
+//      writes them as one coalesced row (count[t][d]);
+//   2. a column scan over tiles (chunk sums, a per-digit scan of the chunk sums
+//      plus the digit bases, a rescan of each chunk) turns the rows into, for
+//      every (tile, digit), the global output offset: all keys of smaller digits
+//      plus the same digit's keys in earlier tiles, which is what makes the
+//      result stable across tiles;
 //   3. k_digit_scatter: each tile ranks its keys stably (per warp, in input order,
 //      with __match_any_sync on the digit), stages them digit-sorted in shared
 //      memory and writes each digit run contiguously.
@@ -19,6 +21,8 @@
 // reference's signed keys.
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <algorithm>
 
 #include "sd_common.cuh"
 #include "sd_internal.h"
@@ -32,9 +36,6 @@ constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per tile
 constexpr int kMaxRadixBits = 10;
 constexpr int kWarps = kSortThreads / 32;
-constexpr int kScanThreads = 256;
-constexpr int kScanItems = 8;
-constexpr int kScanTile = kScanThreads * kScanItems;
 
 __global__ void __launch_bounds__(256) k_cell_keys(const float4* __restrict__ pos, int n, int G, int order,
                                                    uint32_t* __restrict__ keys) {
@@ -88,7 +89,8 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_counts(const uint32_t* _
         if (idx < n) atomicAdd(&hist[(keys[idx] >> shift) & mask], 1u);
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < kRadix; d += kSortThreads) counts[(size_t)d * tiles + blockIdx.x] = hist[d];
+    // tile-major rows: one coalesced row of kRadix counts per tile
+    for (int d = threadIdx.x; d < kRadix; d += kSortThreads) counts[(size_t)blockIdx.x * kRadix + d] = hist[d];
 }
 
 template <int BITS>
@@ -103,6 +105,7 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* 
     // per-warp digit counts fit 16 bits (a warp ranks at most 32 * kSortItems keys)
     __shared__ unsigned short warp_cnt[kWarps][kRadix];
     __shared__ unsigned local_start[kRadix];
+    __shared__ unsigned dst_base[kRadix];  // global start of the digit's run minus its local start
     __shared__ unsigned scan_tmp[33];
     __shared__ uint32_t skeys[kSortTile];
     __shared__ int32_t svals[kSortTile];
@@ -164,7 +167,10 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* 
 #pragma unroll
         for (int j = 0; j < DPT; ++j) {
             const int d = threadIdx.x * DPT + j;
-            if (d < kRadix) local_start[d] = ex;
+            if (d < kRadix) {
+                local_start[d] = ex;
+                dst_base[d] = offsets[(size_t)blockIdx.x * kRadix + d] - ex;
+            }
             ex += dtot[j];
         }
     }
@@ -186,68 +192,70 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* 
     for (int i = threadIdx.x; i < count; i += kSortThreads) {
         const uint32_t key = skeys[i];
         const unsigned d = (key >> shift) & mask;
-        const unsigned dst = offsets[(size_t)d * tiles + blockIdx.x] + ((unsigned)i - local_start[d]);
+        const unsigned dst = dst_base[d] + (unsigned)i;
         keys_out[dst] = key;
         vals_out[dst] = svals[i];
     }
 }
 
-// Exclusive scan of a uint32 array in place: tile sums, scan of sums, rescan.
-__global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(const unsigned* __restrict__ a, size_t m,
-                                                                 unsigned* __restrict__ sums) {
-    __shared__ unsigned tmp[33];
-    const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+// Exclusive offsets of the tile-major digit counts counts[tile][digit]:
+//   offset(t, d) = sum_{d' < d} total(d') + sum_{t' < t} counts[t'][d],
+// computed over chunks of kColChunk tiles so every access is a coalesced row.
+constexpr int kColChunk = 64;
+constexpr int kColThreads = 256;
+constexpr int kColBatch = 8;
+
+// S[c][d] = sum of counts[t][d] over the tiles t of chunk c
+__global__ void __launch_bounds__(kColThreads) k_col_sums(const unsigned* __restrict__ counts, int tiles, int radix,
+                                                          unsigned* __restrict__ S) {
+    const int c = blockIdx.x, d = blockIdx.y * kColThreads + threadIdx.x;
+    if (d >= radix) return;
+    const int t0 = c * kColChunk, t1 = min(tiles, t0 + kColChunk);
     unsigned s = 0u;
-#pragma unroll
-    for (int j = 0; j < kScanItems; ++j)
-        if (base + j < m) s += a[base + j];
-    unsigned tot;
-    block_exclusive(s, tmp, &tot);
-    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+#pragma unroll 8
+    for (int t = t0; t < t1; ++t) s += counts[(size_t)t * radix + d];
+    S[(size_t)c * radix + d] = s;
 }
 
-__global__ void __launch_bounds__(1024) k_scan_sums(unsigned* __restrict__ sums, int m) {
-    __shared__ unsigned warp_tot[32];
-    __shared__ unsigned carry;
-    if (threadIdx.x == 0) carry = 0u;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int base = 0; base < m; base += 1024) {
-        const int i = base + threadIdx.x;
-        const unsigned v = (i < m) ? sums[i] : 0u;
-        const unsigned inc = warp_inclusive(v);
-        if (lane == 31) warp_tot[w] = inc;
-        __syncthreads();
-        if (w == 0) {
-            const unsigned t = warp_tot[lane];
-            const unsigned ti = warp_inclusive(t);
-            warp_tot[lane] = ti - t;
+// One CTA, thread per digit: S[c][d] <- base(d) + sum_{c' < c} S[c'][d], where
+// base is the exclusive scan of the digit totals.
+__global__ void __launch_bounds__(1024) k_col_bases(unsigned* __restrict__ S, int chunks, int radix) {
+    __shared__ unsigned tmp[33];
+    const int d = threadIdx.x;
+    unsigned run = 0u;
+    if (d < radix) {
+        for (int c0 = 0; c0 < chunks; c0 += kColBatch) {
+            unsigned v[kColBatch];
+#pragma unroll
+            for (int j = 0; j < kColBatch; ++j) v[j] = (c0 + j < chunks) ? S[(size_t)(c0 + j) * radix + d] : 0u;
+#pragma unroll
+            for (int j = 0; j < kColBatch; ++j) {
+                if (c0 + j < chunks) S[(size_t)(c0 + j) * radix + d] = run;
+                run += v[j];
+            }
         }
-        __syncthreads();
-        const unsigned ex = carry + warp_tot[w] + inc - v;
-        if (i < m) sums[i] = ex;
-        __syncthreads();
-        if (threadIdx.x == 1023) carry = ex + v;
-        __syncthreads();
     }
+    const unsigned base = block_exclusive(d < radix ? run : 0u, tmp, nullptr);
+    if (d < radix)
+        for (int c = 0; c < chunks; ++c) S[(size_t)c * radix + d] += base;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_apply(unsigned* __restrict__ a, size_t m,
-                                                             const unsigned* __restrict__ sums) {
-    __shared__ unsigned tmp[33];
-    const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
-    unsigned x[kScanItems];
-    unsigned s = 0u;
+// counts[t][d] <- offset(t, d), running through the chunk's tiles from S[c][d]
+__global__ void __launch_bounds__(kColThreads) k_col_apply(unsigned* __restrict__ counts, int tiles, int radix,
+                                                           const unsigned* __restrict__ S) {
+    const int c = blockIdx.x, d = blockIdx.y * kColThreads + threadIdx.x;
+    if (d >= radix) return;
+    const int t0 = c * kColChunk, t1 = min(tiles, t0 + kColChunk);
+    unsigned run = S[(size_t)c * radix + d];
+    for (int tb = t0; tb < t1; tb += kColBatch) {
+        unsigned v[kColBatch];
 #pragma unroll
-    for (int j = 0; j < kScanItems; ++j) {
-        x[j] = (base + j < m) ? a[base + j] : 0u;
-        s += x[j];
-    }
-    unsigned run = block_exclusive(s, tmp, nullptr) + sums[blockIdx.x];
+        for (int j = 0; j < kColBatch; ++j) v[j] = (tb + j < t1) ? counts[(size_t)(tb + j) * radix + d] : 0u;
 #pragma unroll
-    for (int j = 0; j < kScanItems; ++j) {
-        if (base + j < m) a[base + j] = run;
-        run += x[j];
+        for (int j = 0; j < kColBatch; ++j) {
+            if (tb + j < t1) counts[(size_t)(tb + j) * radix + d] = run;
+            run += v[j];
+        }
     }
 }
 
@@ -295,22 +303,23 @@ int launch_cell_keys(const float4* pos, int n, int G, int order, uint32_t* keys,
     return SD_OK;
 }
 
-static int scan_tiles_for(size_t m) { return (int)((m + kScanTile - 1) / kScanTile); }
+static int col_chunks(int tiles) { return (tiles + kColChunk - 1) / kColChunk; }
 
 size_t sort_workspace_bytes(int n) {
-    const int tiles = (n + kSortTile - 1) / kSortTile;
-    const size_t m = (size_t)(1 << kMaxRadixBits) * (size_t)(tiles > 0 ? tiles : 1);
-    return align_up(m * sizeof(unsigned), 256) + align_up((size_t)scan_tiles_for(m) * sizeof(unsigned), 256);
+    const int tiles = std::max(1, (n + kSortTile - 1) / kSortTile);
+    const size_t radix = (size_t)1 << kMaxRadixBits;
+    return align_up(radix * tiles * sizeof(unsigned), 256) + align_up(radix * col_chunks(tiles) * sizeof(unsigned), 256);
 }
 
-// Exclusive scan of counts[m] in place, with sums[] from the workspace.
-static int scan_exclusive(unsigned* a, size_t m, unsigned* sums, cudaStream_t s) {
-    const int nt = scan_tiles_for(m);
-    k_scan_tile_sums<<<nt, kScanThreads, 0, s>>>(a, m, sums);
+// counts[tiles][radix] (tile-major) -> exclusive global offsets, in place
+static int scan_offsets(unsigned* counts, int tiles, int radix, unsigned* S, cudaStream_t s) {
+    const int chunks = col_chunks(tiles);
+    const dim3 grid(chunks, (radix + kColThreads - 1) / kColThreads);
+    k_col_sums<<<grid, kColThreads, 0, s>>>(counts, tiles, radix, S);
     SD_LAUNCHED(s);
-    k_scan_sums<<<1, 1024, 0, s>>>(sums, nt);
+    k_col_bases<<<1, 1024, 0, s>>>(S, chunks, radix);
     SD_LAUNCHED(s);
-    k_scan_apply<<<nt, kScanThreads, 0, s>>>(a, m, sums);
+    k_col_apply<<<grid, kColThreads, 0, s>>>(counts, tiles, radix, S);
     SD_LAUNCHED(s);
     return SD_OK;
 }
@@ -353,7 +362,7 @@ int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t*
             default: k_digit_counts<10><<<tiles, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles); break;
         }
         SD_LAUNCHED(s);
-        int rc = scan_exclusive(counts, (size_t)(1 << bits) * tiles, sums, s);
+        int rc = scan_offsets(counts, tiles, 1 << bits, sums, s);
         if (rc != SD_OK) return rc;
         switch (bits) {
             case 8:
