@@ -205,9 +205,12 @@ long long sd_kernel_launches(const sd_sim* sim);
  * stages can be checked one at a time. Workspace sizes come from the *_bytes
  * queries; workspaces must be 256-byte aligned. */
 
-/* kCellKey (Sim.cu:2476-2486) for order SD_ORDER_*: keys_plus1[i] = key + 1
- * (empty slot -> 0), so an unsigned sort puts empty slots first as CUB does with
- * the reference's signed -1. */
+/* kCellKey (Sim.cu:2476-2486) for order SD_ORDER_ROWMAJOR / SD_ORDER_MORTON:
+ * keys_plus1[i] = key + 1 (empty slot -> 0), so an unsigned sort puts empty slots
+ * first as CUB does with the reference's signed -1. SD_ORDER_TILED (no reference
+ * counterpart): keys_plus1[i] = the row index of the CIC base cell in 4x4 row
+ * tiles, (tile_z * G/4 + tile_y) * 16 + (iz & 3) * 4 + (iy & 3), in log2(G^2)
+ * bits; empty slots get 0 and share row 0. */
 int sd_cell_keys(const float* pos, int n, int grid_size, int order, uint32_t* keys_plus1, void* stream);
 /* Bits a stable sort of keys_plus1 must cover for this grid and order. */
 int sd_key_bits(int grid_size, int order);

@@ -47,8 +47,10 @@ __device__ __forceinline__ uint32_t part1by2(uint32_t v) {
     return v;
 }
 
-// Order keys (see sd_cell_keys in stardust_pm.h). Returns key + 1; 0 = empty slot.
-__device__ __forceinline__ uint32_t order_key_plus1(float4 p, int G, int order) {
+// Order keys (see sd_cell_keys in stardust_pm.h). Row-major and Morton: key + 1,
+// 0 = empty slot. Tiled: the row index itself (G^2 values, log2(G^2) bits), with
+// empty slots sharing row 0 (the fused deposit skips them).
+__device__ __forceinline__ uint32_t order_key(float4 p, int G, int order) {
     if (p.x < 0.f) return 0u;
     if (order == 2) {  // tile rows of the CIC base cell
         int iy, iz; float f;
@@ -57,7 +59,7 @@ __device__ __forceinline__ uint32_t order_key_plus1(float4 p, int G, int order) 
         iy &= (G - 1); iz &= (G - 1);
         const int tiles = G >> 2;
         const int tile = (iz >> 2) * tiles + (iy >> 2);
-        return (uint32_t)(tile * 16 + (iz & 3) * 4 + (iy & 3)) + 1u;
+        return (uint32_t)(tile * 16 + (iz & 3) * 4 + (iy & 3));
     }
     // containing cell, clamped (kCellKey, Sim.cu:2482-2485)
     const int cx = min(max((int)__fmul_rn(p.x, (float)G), 0), G - 1);

@@ -57,8 +57,8 @@ int launch_poisson(const PoissonPlan& p, const long long* rho_fixed, const float
 int launch_poisson_ex(const PoissonPlan& p, const long long* rho_fixed, const float* rho_float, const float4* pos,
                       const int* perm, const int* row_start, float* rho_keep, float2* spec, float* phi,
                       cudaStream_t s, cudaEvent_t* ev = nullptr);
-// row_start[r] = first index i with sorted keys_plus1[i] > r, for r in [0, rows]
-int launch_row_bounds(const uint32_t* keys_plus1, int n, int rows, int* row_start, cudaStream_t s);
+// row_start[r] = first index i with sorted row keys[i] >= r, for r in [0, rows]
+int launch_row_bounds(const uint32_t* keys, int n, int rows, int* row_start, cudaStream_t s);
 
 size_t gather_partials(int n);
 // perm != nullptr: slot i takes input particle perm[i] (fused reorder) and the

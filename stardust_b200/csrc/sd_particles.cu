@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kGatherThreads) k_gather_kick_drift(
         p.z = __fsub_rn(p.z, floorf(p.z));
         pos_out[i] = p;
         vel_out[i] = v;
-        if (keys_out) keys_out[i] = order_key_plus1(p, G, order);
+        if (keys_out) keys_out[i] = order_key(p, G, order);
         sx += v.x;
         sy += v.y;
         sz += v.z;

@@ -207,6 +207,7 @@ __global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4
         for (int b = 0; b < kBatch; ++b) {
             if (f0 + b * NT >= total) break;
             const float4 p = pb[b];
+            if (p.x < 0.f) continue;  // empty slots sort into row 0
             int ix, iy, iz;
             float fx, fy, fz;
             cic_axis(p.x, G, ix, fx);

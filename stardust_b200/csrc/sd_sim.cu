@@ -98,7 +98,8 @@ float dt_scale_for(float ts) {  // dtScaleFor (Sim.h:89-93)
 }
 
 int key_bits_for(int G, int order) {
-    const long long top = (order == SD_ORDER_TILED) ? (long long)G * G : (long long)G * G * G;
+    // largest key: G^2 - 1 (tiled rows) or G^3 (row-major / Morton key + 1)
+    const long long top = (order == SD_ORDER_TILED) ? (long long)G * G - 1 : (long long)G * G * G;
     int b = 0;
     while ((1ll << b) < top + 1) ++b;
     return b;

@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(256) k_cell_keys(const float4* __restrict__ po
                                                    uint32_t* __restrict__ keys) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    keys[i] = order_key_plus1(pos[i], G, order);
+    keys[i] = order_key(pos[i], G, order);
 }
 
 // Inclusive warp scan.
@@ -199,13 +199,17 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* 
 }
 
 // Exclusive offsets of the tile-major digit counts counts[tile][digit]:
-//   offset(t, d) = sum_{d' < d} total(d') + sum_{t' < t} counts[t'][d],
-// computed over chunks of kColChunk tiles so every access is a coalesced row.
+//   offset(t, d) = base(d) + sum_{t' < t} counts[t'][d],  base(d) = sum_{d' < d} total(d'),
+// over chunks of kColChunk tiles and slabs of 32 digits, so every global access
+// is a coalesced 128-byte row piece and every chain of dependent adds is short:
+//   k_col_sums   S[c][d] = chunk sums
+//   k_col_prefix S[c][d] -> exclusive prefix over chunks, T[d] = digit totals
+//   k_col_bases  T[d] -> base(d) (one CTA)
+//   k_col_apply  counts[t][d] -> base(d) + S[c][d] + prefix within the chunk
 constexpr int kColChunk = 64;
 constexpr int kColThreads = 256;
-constexpr int kColBatch = 8;
+constexpr int kColSegs = kColThreads / 32;  // 8 segments of a column per CTA
 
-// S[c][d] = sum of counts[t][d] over the tiles t of chunk c
 __global__ void __launch_bounds__(kColThreads) k_col_sums(const unsigned* __restrict__ counts, int tiles, int radix,
                                                           unsigned* __restrict__ S) {
     const int c = blockIdx.x, d = blockIdx.y * kColThreads + threadIdx.x;
@@ -217,45 +221,87 @@ __global__ void __launch_bounds__(kColThreads) k_col_sums(const unsigned* __rest
     S[(size_t)c * radix + d] = s;
 }
 
-// One CTA, thread per digit: S[c][d] <- base(d) + sum_{c' < c} S[c'][d], where
-// base is the exclusive scan of the digit totals.
-__global__ void __launch_bounds__(1024) k_col_bases(unsigned* __restrict__ S, int chunks, int radix) {
-    __shared__ unsigned tmp[33];
-    const int d = threadIdx.x;
-    unsigned run = 0u;
+// CTA per 32-digit slab: thread (seg, lane) owns digit slab*32 + lane and a
+// contiguous run of chunks; two sweeps (sum, rewrite) around a scan of the runs.
+__global__ void __launch_bounds__(kColThreads) k_col_prefix(unsigned* __restrict__ S, int chunks, int radix,
+                                                            unsigned* __restrict__ T) {
+    __shared__ unsigned seg_sum[kColSegs][32];
+    const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
+    const int d = blockIdx.x * 32 + lane;
+    const int per = (chunks + kColSegs - 1) / kColSegs;
+    const int c0 = seg * per, c1 = min(chunks, c0 + per);
+    unsigned sum = 0u;
     if (d < radix) {
-        for (int c0 = 0; c0 < chunks; c0 += kColBatch) {
-            unsigned v[kColBatch];
+#pragma unroll 8
+        for (int c = c0; c < c1; ++c) sum += S[(size_t)c * radix + d];
+    }
+    seg_sum[seg][lane] = sum;
+    __syncthreads();
+    unsigned run = 0u, tot = 0u;
+    for (int j = 0; j < kColSegs; ++j) {
+        const unsigned v = seg_sum[j][lane];
+        if (j < seg) run += v;
+        tot += v;
+    }
+    if (d < radix) {
+        for (int cb = c0; cb < c1; cb += 8) {
+            unsigned v[8];
 #pragma unroll
-            for (int j = 0; j < kColBatch; ++j) v[j] = (c0 + j < chunks) ? S[(size_t)(c0 + j) * radix + d] : 0u;
+            for (int j = 0; j < 8; ++j) v[j] = (cb + j < c1) ? S[(size_t)(cb + j) * radix + d] : 0u;
 #pragma unroll
-            for (int j = 0; j < kColBatch; ++j) {
-                if (c0 + j < chunks) S[(size_t)(c0 + j) * radix + d] = run;
+            for (int j = 0; j < 8; ++j) {
+                if (cb + j < c1) S[(size_t)(cb + j) * radix + d] = run;
                 run += v[j];
             }
         }
+        if (seg == 0) T[d] = tot;
     }
-    const unsigned base = block_exclusive(d < radix ? run : 0u, tmp, nullptr);
-    if (d < radix)
-        for (int c = 0; c < chunks; ++c) S[(size_t)c * radix + d] += base;
 }
 
-// counts[t][d] <- offset(t, d), running through the chunk's tiles from S[c][d]
+__global__ void __launch_bounds__(1024) k_col_bases(unsigned* __restrict__ T, int radix) {
+    __shared__ unsigned tmp[33];
+    const int d = threadIdx.x;
+    const unsigned v = (d < radix) ? T[d] : 0u;
+    const unsigned base = block_exclusive(v, tmp, nullptr);
+    if (d < radix) T[d] = base;
+}
+
+// CTA per (chunk, 32-digit slab): the chunk's 64 x 32 counts staged in shared
+// memory, scanned down each column in 8 segments of 8 tiles.
 __global__ void __launch_bounds__(kColThreads) k_col_apply(unsigned* __restrict__ counts, int tiles, int radix,
-                                                           const unsigned* __restrict__ S) {
-    const int c = blockIdx.x, d = blockIdx.y * kColThreads + threadIdx.x;
-    if (d >= radix) return;
-    const int t0 = c * kColChunk, t1 = min(tiles, t0 + kColChunk);
-    unsigned run = S[(size_t)c * radix + d];
-    for (int tb = t0; tb < t1; tb += kColBatch) {
-        unsigned v[kColBatch];
+                                                           const unsigned* __restrict__ S,
+                                                           const unsigned* __restrict__ T) {
+    __shared__ unsigned tile[kColChunk][33];
+    __shared__ unsigned seg_sum[kColSegs][32];
+    const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
+    const int c = blockIdx.x, d = blockIdx.y * 32 + lane;
+    const int t0 = c * kColChunk, rows = min(tiles - t0, kColChunk);
+    constexpr int kRowsPerSeg = kColChunk / kColSegs;
 #pragma unroll
-        for (int j = 0; j < kColBatch; ++j) v[j] = (tb + j < t1) ? counts[(size_t)(tb + j) * radix + d] : 0u;
+    for (int j = 0; j < kRowsPerSeg; ++j) {
+        const int r = seg + j * kColSegs;
+        tile[r][lane] = (r < rows && d < radix) ? counts[(size_t)(t0 + r) * radix + d] : 0u;
+    }
+    __syncthreads();
+    unsigned sum = 0u;
 #pragma unroll
-        for (int j = 0; j < kColBatch; ++j) {
-            if (tb + j < t1) counts[(size_t)(tb + j) * radix + d] = run;
-            run += v[j];
-        }
+    for (int j = 0; j < kRowsPerSeg; ++j) sum += tile[seg * kRowsPerSeg + j][lane];
+    seg_sum[seg][lane] = sum;
+    __syncthreads();
+    unsigned run = (d < radix) ? T[d] + S[(size_t)c * radix + d] : 0u;
+    for (int j = 0; j < seg; ++j) run += seg_sum[j][lane];
+#pragma unroll
+    for (int j = 0; j < kRowsPerSeg; ++j) {
+        const int r = seg * kRowsPerSeg + j;
+        const unsigned v = tile[r][lane];
+        tile[r][lane] = run;
+        run += v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kRowsPerSeg; ++j) {
+        const int r = seg + j * kColSegs;
+        if (r < rows && d < radix) counts[(size_t)(t0 + r) * radix + d] = tile[r][lane];
     }
 }
 
@@ -277,14 +323,14 @@ __global__ void k_copy_keys(const uint32_t* __restrict__ kin, const int32_t* __r
     vout[i] = vin ? vin[i] : i;
 }
 
-// Thread i writes row_start[r] = i for every key-space row r in
-// [keys[i-1], keys[i]) (keys are key+1, so empty slots never start a row); the
-// last thread closes the tail up to `rows` with n.
+// Sorted row keys (tiled order: key = row) -> row_start[r] = first i with key >= r.
+// Thread i writes row_start[r] = i for every r in (keys[i-1], keys[i]]; the last
+// thread closes the tail up to `rows` with n.
 __global__ void k_row_bounds(const uint32_t* __restrict__ keys, int n, int rows, int* __restrict__ row_start) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > n) return;
-    const int lo = (i == 0) ? 0 : (int)min(keys[i - 1], (uint32_t)rows);
-    const int hi = (i == n) ? rows + 1 : (int)min(keys[i], (uint32_t)rows);
+    const int lo = (i == 0) ? 0 : (int)min(keys[i - 1] + 1u, (uint32_t)rows);
+    const int hi = (i == n) ? rows + 1 : (int)min(keys[i] + 1u, (uint32_t)rows);
     for (int r = lo; r < hi; ++r) row_start[r] = i;
 }
 
@@ -308,18 +354,23 @@ static int col_chunks(int tiles) { return (tiles + kColChunk - 1) / kColChunk; }
 size_t sort_workspace_bytes(int n) {
     const int tiles = std::max(1, (n + kSortTile - 1) / kSortTile);
     const size_t radix = (size_t)1 << kMaxRadixBits;
-    return align_up(radix * tiles * sizeof(unsigned), 256) + align_up(radix * col_chunks(tiles) * sizeof(unsigned), 256);
+    return align_up(radix * tiles * sizeof(unsigned), 256) +
+           align_up(radix * (col_chunks(tiles) + 1) * sizeof(unsigned), 256);
 }
 
-// counts[tiles][radix] (tile-major) -> exclusive global offsets, in place
+// counts[tiles][radix] (tile-major) -> exclusive global offsets, in place;
+// S holds chunks * radix chunk prefixes followed by the radix digit bases
 static int scan_offsets(unsigned* counts, int tiles, int radix, unsigned* S, cudaStream_t s) {
     const int chunks = col_chunks(tiles);
-    const dim3 grid(chunks, (radix + kColThreads - 1) / kColThreads);
-    k_col_sums<<<grid, kColThreads, 0, s>>>(counts, tiles, radix, S);
+    unsigned* T = S + (size_t)chunks * radix;
+    const int slabs = (radix + 31) / 32;
+    k_col_sums<<<dim3(chunks, (radix + kColThreads - 1) / kColThreads), kColThreads, 0, s>>>(counts, tiles, radix, S);
     SD_LAUNCHED(s);
-    k_col_bases<<<1, 1024, 0, s>>>(S, chunks, radix);
+    k_col_prefix<<<slabs, kColThreads, 0, s>>>(S, chunks, radix, T);
     SD_LAUNCHED(s);
-    k_col_apply<<<grid, kColThreads, 0, s>>>(counts, tiles, radix, S);
+    k_col_bases<<<1, 1024, 0, s>>>(T, radix);
+    SD_LAUNCHED(s);
+    k_col_apply<<<dim3(chunks, slabs), kColThreads, 0, s>>>(counts, tiles, radix, S, T);
     SD_LAUNCHED(s);
     return SD_OK;
 }

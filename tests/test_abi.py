@@ -46,10 +46,10 @@ def test_static_queries(lib):
     assert lib.sd_abi_version() == 1
     assert lib.sd_max_grid_size(L.SD_BOUNDARY_PERIODIC) == 512       # Sim.cu:4158
     assert lib.sd_max_grid_size(L.SD_BOUNDARY_ISOLATED) == 256
-    # key bits of key+1: G^3 + 1 values for row-major / Morton, G^2 + 1 for tile rows
+    # key bits of key+1: G^3 + 1 values for row-major / Morton; tile rows: G^2 values
     assert lib.sd_key_bits(64, L.SD_ORDER_ROWMAJOR) == 19
     assert lib.sd_key_bits(512, L.SD_ORDER_ROWMAJOR) == 28
-    assert lib.sd_key_bits(512, L.SD_ORDER_TILED) == 19
+    assert lib.sd_key_bits(512, L.SD_ORDER_TILED) == 18
     small = lib.sd_estimate_bytes(1000, 64, L.SD_BOUNDARY_PERIODIC)
     big = lib.sd_estimate_bytes(1000, 128, L.SD_BOUNDARY_PERIODIC)
     assert 0 < small < big

@@ -50,7 +50,8 @@ def test_cell_keys_bit_exact(cuda, lib, oracle, order, G):
     pd = dev(cuda, pos)
     L.check(lib.sd_cell_keys(pd.data_ptr(), len(pos), G, order, keys.data_ptr(), None), "keys")
     sync(cuda)
-    ref = oracle.cell_keys(pos, G, order).astype(np.int64) + 1
+    ref = oracle.cell_keys(pos, G, order).astype(np.int64)
+    ref = np.maximum(ref, 0) if order == 2 else ref + 1  # tiled: row index, empty slots share row 0
     assert np.array_equal(keys.cpu().numpy().view(np.uint32).astype(np.int64), ref)
 
 
@@ -109,7 +110,11 @@ def test_sort_cell_keys_matches_oracle_and_reorder(cuda, lib, oracle, order):
     L.check(lib.sd_reorder(pd.data_ptr(), vd.data_ptr(), vout.data_ptr(), p2.data_ptr(), v2.data_ptr(), n, None),
             "reorder")
     sync(cuda)
-    ref_perm = oracle.stable_sort_perm(oracle.cell_keys(pos, G, order), bits)
+    okeys = oracle.cell_keys(pos, G, order)
+    if order == 2:  # tiled keys are row indices with empty slots in row 0
+        ref_perm = np.argsort(np.maximum(okeys, 0), kind="stable").astype(np.int32)
+    else:
+        ref_perm = oracle.stable_sort_perm(okeys, bits)
     assert np.array_equal(vout.cpu().numpy(), ref_perm)
     assert np.array_equal(p2.cpu().numpy(), pos[ref_perm])
     assert np.array_equal(v2.cpu().numpy(), vel[ref_perm])
