@@ -7,7 +7,8 @@
 // float2 per warp: the two-wavefront minimum for 8-byte accesses, with no
 // padding and no bank conflicts.
 //
-// Stages are mixed radix (8, then 4 or 2 for the remainder) in the self-sorting
+// Stages are mixed radix (32 or 16 where every thread still gets a butterfly,
+// else 8, then 4 or 2 for the remainder) in the self-sorting
 // Stockham form: the stage with radix R and sub-transform length Ns reads
 // in[j + r*N/R], multiplies by W_{Ns*R}^{(j mod Ns)*r}, does an R-point DFT in
 // registers and writes out[(j/Ns)*Ns*R + (j mod Ns) + r*Ns]. Output is in
@@ -35,9 +36,57 @@ __device__ __forceinline__ float2 mul_mi(float2 a) {
     return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
 }
 
+// W_32^k = exp(-2 pi i k / 32), k < 16 (mathematical constants; the inverse uses
+// conjugates). W_16^k = W_32^(2k).
+namespace w32 {
+constexpr float c1 = 0.98078528040323044913f, s1 = 0.19509032201612826785f;
+constexpr float c2 = 0.92387953251128675613f, s2 = 0.38268343236508977173f;
+constexpr float c3 = 0.83146961230254523708f, s3 = 0.55557023301960222474f;
+constexpr float r = 0.70710678118654752440f;
+__device__ __forceinline__ float2 get(int k) {  // k is a compile-time constant after unrolling
+    switch (k) {
+        case 0: return make_float2(1.f, 0.f);
+        case 1: return make_float2(c1, -s1);
+        case 2: return make_float2(c2, -s2);
+        case 3: return make_float2(c3, -s3);
+        case 4: return make_float2(r, -r);
+        case 5: return make_float2(s3, -c3);
+        case 6: return make_float2(s2, -c2);
+        case 7: return make_float2(s1, -c1);
+        case 8: return make_float2(0.f, -1.f);
+        case 9: return make_float2(-s1, -c1);
+        case 10: return make_float2(-s2, -c2);
+        case 11: return make_float2(-s3, -c3);
+        case 12: return make_float2(-r, -r);
+        case 13: return make_float2(-c3, -s3);
+        case 14: return make_float2(-c2, -s2);
+        default: return make_float2(-c1, -s1);
+    }
+}
+}  // namespace w32
+
 template <int R, bool INV>
 __device__ __forceinline__ void dft(float2* v) {
-    if constexpr (R == 2) {
+    if constexpr (R == 16 || R == 32) {
+        // radix-2 split: DFTs of the even and odd inputs, combined with W_R^k
+        constexpr int H = R / 2;
+        float2 e[H], o[H];
+#pragma unroll
+        for (int i = 0; i < H; ++i) {
+            e[i] = v[2 * i];
+            o[i] = v[2 * i + 1];
+        }
+        dft<H, INV>(e);
+        dft<H, INV>(o);
+#pragma unroll
+        for (int k = 0; k < H; ++k) {
+            float2 w = w32::get(k * (32 / R));
+            if (INV) w.y = -w.y;
+            const float2 t = (k == 0) ? o[k] : cmul(o[k], w);
+            v[k] = cadd(e[k], t);
+            v[k + H] = csub(e[k], t);
+        }
+    } else if constexpr (R == 2) {
         const float2 a = v[0], b = v[1];
         v[0] = cadd(a, b);
         v[1] = csub(a, b);
@@ -71,16 +120,24 @@ __device__ __forceinline__ void dft(float2* v) {
     }
 }
 
-template <int REM>
+// Radix of the next stage for a remaining length REM of an N-point transform on
+// NT threads: the largest of 32, 16 that divides REM and still gives every thread
+// a butterfly (16 N / R >= NT), else 8, 4 or 2. Fewer, wider stages mean fewer
+// shared-memory round trips.
+template <int REM, int N, int NT>
 struct radix_of {
-    static constexpr int value = (REM % 8 == 0) ? 8 : ((REM % 4 == 0) ? 4 : 2);
+    static constexpr int value = (REM % 32 == 0 && 16 * N / 32 >= NT)   ? 32
+                                 : (REM % 16 == 0 && 16 * N / 16 >= NT) ? 16
+                                 : (REM % 8 == 0)                       ? 8
+                                 : (REM % 4 == 0)                       ? 4
+                                                                        : 2;
 };
 
 // One Stockham stage on the 16 interleaved lines, then recurse.
 template <int N, int Ns, int NT, int TWS, bool INV>
 __device__ __forceinline__ void stages16(float2* s, const float2* tw) {
     if constexpr (Ns < N) {
-        constexpr int R = radix_of<N / Ns>::value;
+        constexpr int R = radix_of<N / Ns, N, NT>::value;
         constexpr int NB = N / R;
         constexpr int TOT = 16 * NB;
         constexpr int PER = (TOT + NT - 1) / NT;
