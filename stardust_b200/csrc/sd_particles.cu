@@ -155,7 +155,7 @@ __device__ __forceinline__ void block_sum4(double v0, double v1, double v2, doub
 // (kReorder, Sim.cu:2488-2495): slot i takes particle perm[i] of the input
 // arrays and the results go to separate output arrays. keys_out (optional)
 // receives the order key of each new position for the next step's sort.
-__global__ void __launch_bounds__(kGatherThreads) k_gather_kick_drift(
+__global__ void __launch_bounds__(kGatherThreads, 4) k_gather_kick_drift(
     const float* __restrict__ phi, int G, float h, const float4* pos_in, const float4* vel_in,
     const int* __restrict__ perm, float4* pos_out, float4* vel_out, uint32_t* __restrict__ keys_out, int order, int n,
     float dt_kick, float dt_drift, float c2, const float* __restrict__ mean_vel, double* __restrict__ partials,

@@ -381,18 +381,24 @@ __global__ void __launch_bounds__(kFftThreads, 3) k_pass_c(float2* __restrict__ 
     const int bx = blockIdx.x, by = blockIdx.y;
     for (int i = threadIdx.x; i < G; i += kFftThreads) tw[i] = tw_g[i];
     for (int i = threadIdx.x; i <= H; i += kFftThreads) gexp[i] = gexp_g[i];
-    load_lines<G, 2>(s, spec, bx, by);
-    fft::lines16<G, kFftThreads, 1, false>(s, tw);
-    // Green's function: -scale/k^2 * exp(-k^2 s^2/2), k = 0 -> 0 (Sim.cu:536-556);
-    // padding columns kx > H are zeroed.
-    for (int u = threadIdx.x; u < 16 * G; u += kFftThreads) {
-        const int l = u & 15, kz = u >> 4;
+    __shared__ float line_g[16];
+    __shared__ int line_k2[16];
+    if (threadIdx.x < 16) {
+        const int l = threadIdx.x;
         const int kx = bx * 4 + (l & 3), ky = by * 4 + (l >> 2);
         const int kyf = (ky <= G / 2) ? ky : ky - G;
+        line_g[l] = (kx <= H) ? -scale * (gexp_g[kx] * gexp_g[abs(kyf)]) : 0.f;  // the global table: no barrier yet
+        line_k2[l] = kx * kx + kyf * kyf;
+    }
+    load_lines<G, 2>(s, spec, bx, by);  // ends with a barrier
+    fft::lines16<G, kFftThreads, 1, false>(s, tw);
+    // Green's function: -scale/k^2 * exp(-k^2 s^2/2), k = 0 -> 0 (Sim.cu:536-556),
+    // with the per-line factors of (kx, ky) hoisted; padding columns kx > H are zeroed.
+    for (int u = threadIdx.x; u < 16 * G; u += kFftThreads) {
+        const int l = u & 15, kz = u >> 4;
         const int kzf = (kz <= G / 2) ? kz : kz - G;
-        const int k2 = kx * kx + kyf * kyf + kzf * kzf;
-        float m = 0.f;
-        if (k2 != 0 && kx <= H) m = (-scale / (float)k2) * (gexp[kx] * gexp[abs(kyf)] * gexp[abs(kzf)]);
+        const int k2 = line_k2[l] + kzf * kzf;
+        const float m = (k2 != 0) ? __fdividef(line_g[l] * gexp[abs(kzf)], (float)k2) : 0.f;
         float2& e = s[u];
         e.x *= m;
         e.y *= m;
@@ -456,11 +462,31 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_e(const float2* __restrict
     }
     __syncthreads();
     fft::lines16<H, kFftThreads, 2, true>(s, tw);
+    // Interleaved lines -> row-major rows (stride H + 2 float2, 16-byte aligned) in
+    // place through registers, so each warp then writes 512 contiguous bytes of
+    // one row instead of 32 bytes of each of 16 rows.
+    constexpr int RS = H + 2;
+    constexpr int TITEMS = 16 * H;
+    constexpr int TPER = (TITEMS + kFftThreads - 1) / kFftThreads;
+    static_assert(16 * RS <= 16 * T::PX, "row staging fits the line buffer");
+    float2 t[TPER];
+#pragma unroll
+    for (int p = 0; p < TPER; ++p) {
+        const int u = threadIdx.x + p * kFftThreads;
+        if (TITEMS % kFftThreads == 0 || u < TITEMS) t[p] = s[(u >> 4) * 16 + (u & 15)];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < TPER; ++p) {
+        const int u = threadIdx.x + p * kFftThreads;
+        if (TITEMS % kFftThreads == 0 || u < TITEMS) s[(u & 15) * RS + (u >> 4)] = t[p];
+    }
+    __syncthreads();
     for (int u = threadIdx.x; u < 16 * (H / 2); u += kFftThreads) {
-        const int l = u & 15, mp = u >> 4;
+        const int l = u / (H / 2), mp = u % (H / 2);
         const size_t row = ((size_t)(bz * 4 + (l >> 2)) * G + by * 4 + (l & 3)) * G;
-        const float2 a = s[(2 * mp) * 16 + l], b = s[(2 * mp + 1) * 16 + l];
-        *reinterpret_cast<float4*>(phi + row + 4 * mp) = make_float4(a.x, a.y, b.x, b.y);
+        const float4 ab = *reinterpret_cast<const float4*>(s + l * RS + 2 * mp);
+        *reinterpret_cast<float4*>(phi + row + 4 * mp) = ab;
     }
 }
 
