@@ -162,7 +162,8 @@ def run_ours(args, rank, world):
     pos, vel, G, dt = make_workload(args.workload)
     n = len(pos)
     cfg = SimConfig(particle_count=n, grid_size=G, gravity=1.0, units=L.SD_UNITS_NEWTON, softening_cells=1.0,
-                    sort_interval=1, order=args.order, keep_density=0)
+                    sort_interval=1, order=args.order, keep_density=0,
+                    diagnostics=0 if args.no_diagnostics else 1)
     stream = torch.cuda.Stream(device=dev)
     sim = Sim(dev)
     sim.init(cfg)
@@ -191,6 +192,14 @@ def run_ours(args, rank, world):
     clock_info = clocks.stop()
     launches = Sim.kernel_launches() - launches0
     ms = e0.elapsed_time(e1) / args.steps
+    diag = None
+    if not args.no_diagnostics:  # the FP64 records of the timed steps
+        h = sim.diagnostics_history(args.steps)
+        e = h[:, 1] + h[:, 2]
+        diag = {"records": int(len(h)), "kinetic_first": float(h[0, 1]), "potential_first": float(h[0, 2]),
+                "energy_drift_rel_to_potential": float((e[-1] - e[0]) / abs(h[0, 2])),
+                "max_abs_momentum": float(np.abs(h[:, 3:6]).max()),
+                "note": "FP64 energy and momentum every step, accumulated inside the gather"}
     t = torch.tensor([ms], device="cuda")
     if dist:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -260,6 +269,7 @@ def run_ours(args, rank, world):
         "config": {"workload": args.workload, "particles_per_gpu": n, "grid": G, "dt": dt,
                    "order": ["rowmajor", "morton", "tiled"][args.order], "sort_every_step": True,
                    "units": "newton G=1 M=1", "softening_cells": 1.0, "parallelism": f"replicas x{world}",
+                   "fp64_diagnostics_every_step": not args.no_diagnostics,
                    "l2": "inputs exceed L2 (no flush)", "timed_path": "sd_steps (CUDA graph, 2 steps/replay)"},
         "roofline": {"bound": "hbm", "achieved": dom_achieved, "peak": peak, "unit": "GB/s",
                      "frac": dom_achieved / peak, "traffic": traffic, "kernel": dom,
@@ -275,6 +285,7 @@ def run_ours(args, rank, world):
                 "path": "sd_set_particles(host) + sd_step + sd_get_particles(host), pinned"},
         "gpu_launches": int(launches),
         "clocks": clock_info,
+        "diagnostics": diag,
     }
     return out
 
@@ -446,6 +457,7 @@ def main(argv=None) -> int:
     ap.add_argument("--order", type=int, default=2, help="0 row-major (reference), 1 Morton, 2 tiled (fused deposit)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-scene batched ensemble")
+    ap.add_argument("--no-diagnostics", action="store_true", help="time the step without the per-step FP64 records")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-correction comparison (2M particles, 128^3 + MLP vs 128..512^3)")
     args = ap.parse_args(argv)

@@ -82,7 +82,7 @@ typedef struct sd_config {
     int32_t order;            /* SD_ORDER_* */
     int32_t integrator;       /* SD_INT_* */
     int32_t units;            /* SD_UNITS_* */
-    int32_t diagnostics;      /* 1 = FP64 energy and momentum every step (sd_diagnostics) */
+    int32_t diagnostics;      /* 1 = FP64 energy and momentum of every step (sd_diagnostics_history) */
     int32_t keep_density;     /* 1 = keep the step-start density for sd_density_device_ptr (4 B/cell more traffic) */
     int32_t reserved[6];
 } sd_config;
@@ -197,6 +197,14 @@ double sd_measure_total_grid_mass(sd_sim* sim);                     /* Sim.cu:48
 double sd_measure_max_density(sd_sim* sim);                         /* Sim.cu:4908-4924 */
 double sd_measure_kinetic_energy(sd_sim* sim);                      /* Sim.cu:5141-5149 */
 int sd_diagnostics_get(sd_sim* sim, sd_diagnostics* out);
+/* Per-step FP64 records of the steps taken with diagnostics = 1 (accumulated
+ * inside the gather, no extra pass; kept in a device ring of the last 4096
+ * steps; also inside sd_steps graphs). Copies the most recent min(max_records,
+ * available) records, oldest first, 8 doubles each:
+ *   {record index, kinetic, potential, momentum x, y, z, live count, |mean velocity removed|}
+ * kinetic = sum 1/2 m |v|^2 of the step's zeroed end velocities; potential =
+ * 1/2 sum m phi(x) at the step-start positions with the step's potential. */
+int sd_diagnostics_history(sd_sim* sim, double* out, int max_records, int* count_out);
 /* Number of kernel launches the handle issued since creation. */
 long long sd_kernel_launches(const sd_sim* sim);
 
@@ -308,7 +316,7 @@ typedef struct sd_scene_tuning {
 } sd_scene_tuning;
 int sd_ensemble_create(sd_ensemble** out, int device);
 int sd_ensemble_destroy(sd_ensemble* ens);
-/* adds a scene (sort_interval 0 or 1, diagnostics off); returns its index or a negative status */
+/* adds a scene (sort_interval 0 or 1); returns its index or a negative status */
 int sd_ensemble_add(sd_ensemble* ens, const sd_config* cfg, const float* pos, const float* vel, int n, int where);
 int sd_ensemble_size(const sd_ensemble* ens);
 sd_sim* sd_ensemble_scene(sd_ensemble* ens, int index);

@@ -127,6 +127,7 @@ SIGNATURES = [
     ("sd_gather_kick_drift", _I, [_P, _I, _F, _P, _P, _I, _F, _F, _F, _P, _P, _P, _S, _P]),
     ("sd_gather_workspace_bytes", _S, [_I]),
     ("sd_interpolate_accel", _I, [_P, _I, _F, _P, _P, _I, _P]),
+    ("sd_diagnostics_history", _I, [_P, _P, _I, _P]),
     ("sd_mlp_param_count", _I, []),
     ("sd_mlp_features", _I, [_P, _P, _I, _P, _I, _F, _P, _P]),
     ("sd_mlp_infer", _I, [_P, _P, _P, _I, _P, _I, _F, _F, _P, _P]),

@@ -69,7 +69,7 @@ void drop_graphs(sd_ensemble* e) {
 }
 
 bool graphable(const sd_sim* s) {
-    return s->configured && (s->cfg.sort_interval == 0 || s->cfg.sort_interval == 1) && !s->cfg.diagnostics;
+    return s->configured && (s->cfg.sort_interval == 0 || s->cfg.sort_interval == 1);
 }
 
 struct HostCounters {
@@ -100,7 +100,7 @@ int prepare_scenes(sd_ensemble* e, float dt) {
     for (auto& sl : e->scenes) {
         sd_sim* s = sl.sim;
         if (!graphable(s))
-            return fail(SD_E_STATE, "ensemble: scenes must sort every step or never and have diagnostics off");
+            return fail(SD_E_STATE, "ensemble: scenes must sort every step or never");
         if (s->cfg.integrator == SD_INT_KDK && !s->lf_open) {
             if (int rc = do_step(s, dt, sort_due(s), false)) return rc;
         }
@@ -306,7 +306,7 @@ int sd_ensemble_add(sd_ensemble* e, const sd_config* cfg, const float* pos, cons
     if (!rc) rc = sd_init(s, cfg);
     if (!rc && pos) rc = sd_set_particles(s, pos, vel, n, where);
     if (!rc && !graphable(s))
-        rc = fail(SD_E_ARG, "ensemble_add: scenes must sort every step or never and have diagnostics off");
+        rc = fail(SD_E_ARG, "ensemble_add: scenes must sort every step or never");
     SceneSlot sl;
     if (!rc) rc = SD_CUDA(cudaEventCreateWithFlags(&sl.join, cudaEventDisableTiming));
     if (rc) {

@@ -66,11 +66,19 @@ size_t gather_partials(int n);
 // keys_out (optional) receives the next step's order keys (key + 1).
 // extra (optional) is an acceleration added to the PM one, indexed like the outputs.
 // max_blocks > 0 caps the grid (grid-stride loop); partials need gather_partials(n) blocks.
+// diag (optional): per-step FP64 energy/momentum record appended to a device ring
+// of `cap` records of 8 doubles; count is a device counter of records written.
+struct DiagRecord {
+    double* rec = nullptr;
+    unsigned long long* count = nullptr;
+    int cap = 0;
+    double mass = 0.0;  // particle mass, 1/N
+};
 int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const float4* pos_in, const float4* vel_in,
                              const int* perm, float4* pos_out, float4* vel_out, uint32_t* keys_out, int order, int n,
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
                              double* mom_out, float* mean_out, cudaStream_t s, const float4* extra = nullptr,
-                             int max_blocks = 0);
+                             int max_blocks = 0, const DiagRecord* diag = nullptr);
 int launch_interpolate_accel(const float* phi, int G, float pot_scale, const float4* pos, float4* acc, int n,
                              cudaStream_t s, const float4* extra = nullptr);
 // learned correction (sd_mlp.cu): out[i] = out_scale * MLP(features of pos[perm ? perm[i] : i])

@@ -74,7 +74,8 @@ __global__ void k_clear_u64(unsigned long long* __restrict__ a, size_t n) {
 //   A[oy][oz][d]  rows (iy+oy, iz+oz), x = ix-1+d, d < 4
 //   Y[e][oz][ox]  rows (iy-1+3e, iz+oz), x = ix+ox
 //   Z[e][oy][ox]  rows (iy+oy, iz-1+3e), x = ix+ox
-__device__ __forceinline__ float3 gather_accel(const float* __restrict__ phi, int G, float h, float4 p) {
+__device__ __forceinline__ float3 gather_accel(const float* __restrict__ phi, int G, float h, float4 p,
+                                               float* phi_at = nullptr) {
     int ix, iy, iz;
     float fx, fy, fz;
     cic_axis(p.x, G, ix, fx);
@@ -124,26 +125,33 @@ __device__ __forceinline__ float3 gather_accel(const float* __restrict__ phi, in
         a.y = __fmaf_rn(gy, w, a.y);
         a.z = __fmaf_rn(gz, w, a.z);
     }
+    if (phi_at) {  // CIC-interpolated potential: the corners are A[oy][oz][1 + ox]
+        float f = 0.f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            f = __fmaf_rn(cic_weight(k, fx, fy, fz), A[(k >> 1) & 1][(k >> 2) & 1][1 + (k & 1)], f);
+        *phi_at = f;
+    }
     return a;
 }
 
-// FP64 block sum of 4 values into partials[blockIdx.x*4 + j], fixed tree order.
-__device__ __forceinline__ void block_sum4(double v0, double v1, double v2, double v3, double* partials) {
-    __shared__ double red[4][kGatherThreads / 32];
+// FP64 block sums of K values into partials[blockIdx.x*K + j], fixed tree order.
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double* partials) {
+    __shared__ double red[K][kGatherThreads / 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        v0 += __shfl_down_sync(0xffffffffu, v0, o);
-        v1 += __shfl_down_sync(0xffffffffu, v1, o);
-        v2 += __shfl_down_sync(0xffffffffu, v2, o);
-        v3 += __shfl_down_sync(0xffffffffu, v3, o);
-    }
-    if (lane == 0) { red[0][w] = v0; red[1][w] = v1; red[2][w] = v2; red[3][w] = v3; }
+    for (int j = 0; j < K; ++j)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[j] += __shfl_down_sync(0xffffffffu, v[j], o);
+    if (lane == 0)
+#pragma unroll
+        for (int j = 0; j < K; ++j) red[j][w] = v[j];
     __syncthreads();
-    if (threadIdx.x < 4) {
+    if (threadIdx.x < K) {
         double s = 0.0;
         for (int j = 0; j < kGatherThreads / 32; ++j) s += red[threadIdx.x][j];
-        partials[(size_t)blockIdx.x * 4 + threadIdx.x] = s;
+        partials[(size_t)blockIdx.x * K + threadIdx.x] = s;
     }
 }
 
@@ -155,12 +163,17 @@ __device__ __forceinline__ void block_sum4(double v0, double v1, double v2, doub
 // (kReorder, Sim.cu:2488-2495): slot i takes particle perm[i] of the input
 // arrays and the results go to separate output arrays. keys_out (optional)
 // receives the order key of each new position for the next step's sort.
+//
+// DIAG: the FP64 partials also carry sum |v|^2 of the kicked velocities and sum
+// phi(x) at the step-start positions (the potential the kick used), for the
+// per-step energy record written by the finalize kernel.
+template <bool DIAG>
 __global__ void __launch_bounds__(kGatherThreads, 4) k_gather_kick_drift(
     const float* __restrict__ phi, int G, float h, const float4* pos_in, const float4* vel_in,
     const int* __restrict__ perm, float4* pos_out, float4* vel_out, uint32_t* __restrict__ keys_out, int order, int n,
     float dt_kick, float dt_drift, float c2, const float* __restrict__ mean_vel, double* __restrict__ partials,
     const float4* __restrict__ extra) {
-    double sx = 0.0, sy = 0.0, sz = 0.0, cnt = 0.0;
+    double sx = 0.0, sy = 0.0, sz = 0.0, cnt = 0.0, sv2 = 0.0, sphi = 0.0;
     const float mx = mean_vel ? mean_vel[0] : 0.f, my = mean_vel ? mean_vel[1] : 0.f,
                 mz = mean_vel ? mean_vel[2] : 0.f;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -180,7 +193,8 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_gather_kick_drift(
             v.y = __fsub_rn(v.y, my);
             v.z = __fsub_rn(v.z, mz);
         }
-        float3 a = gather_accel(phi, G, h, p);
+        float phi_p = 0.f;
+        float3 a = gather_accel(phi, G, h, p, DIAG ? &phi_p : nullptr);
         if (extra) {  // learned correction, indexed like the outputs
             const float4 e = extra[i];
             a.x = __fadd_rn(a.x, e.x);
@@ -219,33 +233,72 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_gather_kick_drift(
         sy += v.y;
         sz += v.z;
         cnt += 1.0;
+        if (DIAG) {
+            sv2 += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z;
+            sphi += (double)phi_p;
+        }
     }
-    if (partials) block_sum4(sx, sy, sz, cnt, partials);
+    if (partials) {
+        if (DIAG) {
+            double v6[6] = {sx, sy, sz, cnt, sv2, sphi};
+            block_sum<6>(v6, partials);
+        } else {
+            double v4[4] = {sx, sy, sz, cnt};
+            block_sum<4>(v4, partials);
+        }
+    }
 }
 
 // Fixed-order sum of the per-block partials; mean = (float)(sum / count).
+// With K = 6 it also appends one record to the diagnostics ring rec[cap][8]:
+//   {step, kinetic, potential, px, py, pz, live, mean removed |mu|}
+// kinetic = sum 1/2 m |v - mu|^2 of the zeroed velocities (from sum |v|^2, sum v
+// and the float mean mu actually subtracted), potential = 1/2 m pot_scale sum phi
+// at the step-start positions, momentum = m (sum v - live mu), m = 1/N.
+template <int K>
 __global__ void __launch_bounds__(256) k_finalize_mean(const double* __restrict__ partials, int blocks,
-                                                       double* __restrict__ mom_out, float* __restrict__ mean_out) {
-    __shared__ double red[4][256];
-    double s[4] = {0.0, 0.0, 0.0, 0.0};
+                                                       double* __restrict__ mom_out, float* __restrict__ mean_out,
+                                                       double* __restrict__ rec, unsigned long long* __restrict__ rec_n,
+                                                       int cap, double mass, double pot_scale) {
+    __shared__ double red[K][256];
+    double s[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) s[j] = 0.0;
     for (int b = threadIdx.x; b < blocks; b += 256)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) s[j] += partials[(size_t)b * 4 + j];
+        for (int j = 0; j < K; ++j) s[j] += partials[(size_t)b * K + j];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) red[j][threadIdx.x] = s[j];
+    for (int j = 0; j < K; ++j) red[j][threadIdx.x] = s[j];
     __syncthreads();
     for (int o = 128; o > 0; o >>= 1) {
         if (threadIdx.x < o)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) red[j][threadIdx.x] += red[j][threadIdx.x + o];
+            for (int j = 0; j < K; ++j) red[j][threadIdx.x] += red[j][threadIdx.x + o];
         __syncthreads();
     }
     if (threadIdx.x == 0) {
+        const double c = red[3][0];
+        float mu[3];
+        for (int j = 0; j < 3; ++j) mu[j] = (c >= 1.0) ? (float)(red[j][0] / c) : 0.f;
         if (mom_out)
             for (int j = 0; j < 4; ++j) mom_out[j] = red[j][0];
-        if (mean_out) {
-            const double c = red[3][0];
-            for (int j = 0; j < 3; ++j) mean_out[j] = (c >= 1.0) ? (float)(red[j][0] / c) : 0.f;
+        if (mean_out)
+            for (int j = 0; j < 3; ++j) mean_out[j] = mu[j];
+        if (K == 6 && rec) {
+            const unsigned long long idx = *rec_n;
+            *rec_n = idx + 1;
+            double* r = rec + (size_t)(idx % (unsigned long long)cap) * 8;
+            double mv = 0.0, mu2 = 0.0;
+            for (int j = 0; j < 3; ++j) {
+                mv += (double)mu[j] * red[j][0];
+                mu2 += (double)mu[j] * mu[j];
+            }
+            r[0] = (double)idx;
+            r[1] = 0.5 * mass * (red[K - 2][0] - 2.0 * mv + c * mu2);
+            r[2] = 0.5 * mass * pot_scale * red[K - 1][0];
+            for (int j = 0; j < 3; ++j) r[3 + j] = mass * (red[j][0] - c * (double)mu[j]);
+            r[6] = c;
+            r[7] = sqrt(mu2);
         }
     }
 }
@@ -442,16 +495,27 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
                              const int* perm, float4* pos_out, float4* vel_out, uint32_t* keys_out, int order, int n,
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
                              double* mom_out, float* mean_out, cudaStream_t s, const float4* extra,
-                             int max_blocks) {
+                             int max_blocks, const DiagRecord* diag) {
     if (n <= 0) return SD_OK;
     const float h = (0.5f * (float)G) * pot_scale;  // Sim.cu:604
     int blocks = (int)gather_partials(n);
     if (max_blocks > 0 && blocks > max_blocks) blocks = max_blocks;
-    k_gather_kick_drift<<<blocks, kGatherThreads, 0, s>>>(phi, G, h, pos_in, vel_in, perm, pos_out, vel_out, keys_out,
-                                                          order, n, dt_kick, dt_drift, c2, mean_vel, partials, extra);
+    const bool dg = diag && partials;
+    if (dg)
+        k_gather_kick_drift<true><<<blocks, kGatherThreads, 0, s>>>(phi, G, h, pos_in, vel_in, perm, pos_out, vel_out,
+                                                                    keys_out, order, n, dt_kick, dt_drift, c2,
+                                                                    mean_vel, partials, extra);
+    else
+        k_gather_kick_drift<false><<<blocks, kGatherThreads, 0, s>>>(phi, G, h, pos_in, vel_in, perm, pos_out,
+                                                                     vel_out, keys_out, order, n, dt_kick, dt_drift,
+                                                                     c2, mean_vel, partials, extra);
     SD_LAUNCHED(s);
-    if (partials && (mom_out || mean_out)) {
-        k_finalize_mean<<<1, 256, 0, s>>>(partials, blocks, mom_out, mean_out);
+    if (dg) {
+        k_finalize_mean<6><<<1, 256, 0, s>>>(partials, blocks, mom_out, mean_out, diag->rec, diag->count, diag->cap,
+                                            diag->mass, (double)pot_scale);
+        SD_LAUNCHED(s);
+    } else if (partials && (mom_out || mean_out)) {
+        k_finalize_mean<4><<<1, 256, 0, s>>>(partials, blocks, mom_out, mean_out, nullptr, nullptr, 1, 0.0, 0.0);
         SD_LAUNCHED(s);
     }
     return SD_OK;

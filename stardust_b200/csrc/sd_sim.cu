@@ -128,6 +128,8 @@ void free_buffers(sd_sim* s) {
     free_dev(s->acc); free_dev(s->row_start); free_dev(s->spec); free_dev(s->phi); free_dev(s->rho);
     free_dev(s->partials); free_dev(s->mom); free_dev(s->mean);
     free_dev(s->mlp_out);
+    free_dev(s->diag_rec);
+    free_dev(s->diag_count);
     poisson_plan_free(s->plan);
     if (s->graph) cudaGraphExecDestroy(s->graph);
     s->graph = nullptr;
@@ -185,6 +187,8 @@ int allocate(sd_sim* s) {
     rc = rc ? rc : alloc_dev(s->partials, s->partials_count);
     rc = rc ? rc : alloc_dev(s->mom, 8);
     rc = rc ? rc : alloc_dev(s->mean, 4);
+    rc = rc ? rc : alloc_dev(s->diag_rec, (size_t)kDiagCap * 8);
+    rc = rc ? rc : alloc_dev(s->diag_count, 1);
     if (rc) {
         free_buffers(s);
         return rc;
@@ -198,6 +202,7 @@ int allocate(sd_sim* s) {
     if (SD_CUDA(cudaMemsetAsync(s->acc, 0, sizeof(long long) * cells, s->stream)) ||
         SD_CUDA(cudaMemsetAsync(s->mean, 0, sizeof(float) * 4, s->stream)) ||
         SD_CUDA(cudaMemsetAsync(s->mom, 0, sizeof(double) * 8, s->stream)) ||
+        SD_CUDA(cudaMemsetAsync(s->diag_count, 0, sizeof(unsigned long long), s->stream)) ||
         SD_CUDA(cudaMemsetAsync(s->phi, 0, sizeof(float) * cells, s->stream))) {
         free_buffers(s);
         return SD_E_CUDA;
@@ -328,9 +333,16 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     // velocities; the finalize kernel then overwrites it with this step's mean.
     float4* pos_out = perm ? s->pos2 : s->pos;
     float4* vel_out = perm ? s->vel2 : s->vel;
+    // FP64 energy and momentum of every step, accumulated by the gather itself
+    DiagRecord diag;
+    diag.rec = s->diag_rec;
+    diag.count = s->diag_count;
+    diag.cap = kDiagCap;
+    diag.mass = 1.0 / (double)(s->N > 0 ? s->N : 1);
     rc = launch_gather_kick_drift(s->phi, s->G, pot_scale_of(s), s->pos, s->vel, perm, pos_out, vel_out, s->keys,
                                   s->cfg.order, s->N, dt_kick, dt_drift, c2, s->mean, s->partials, s->mom, s->mean,
-                                  s->stream, s->mlp_on ? s->mlp_out : nullptr, s->gather_blocks);
+                                  s->stream, s->mlp_on ? s->mlp_out : nullptr, s->gather_blocks,
+                                  s->cfg.diagnostics ? &diag : nullptr);
     if (rc) return sim_error(s, rc);
     if (perm) {
         std::swap(s->pos, s->pos2);
@@ -340,12 +352,6 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     s->mean_pending = true;
     if (timed) cudaEventRecord(s->ev[4], s->stream);
     s->ev_valid = timed;
-    if (s->cfg.diagnostics) {
-        // FP64 energy and momentum after the step (phi is that of the step-start positions)
-        rc = launch_energy(s->phi, s->G, s->pos, s->vel, s->N, s->mean, s->partials, s->mom, s->stream);
-        if (rc) return sim_error(s, rc);
-        s->diag_valid = true;
-    }
     s->sim_time += dt;
     ++s->step_count;
     return SD_OK;
@@ -545,7 +551,9 @@ int sd_reset(sd_sim* s) {
     s->lf_open = false;
     s->rho_valid = false;
     s->keys_valid = false;
-    if (SD_CUDA(cudaMemsetAsync(s->mean, 0, sizeof(float) * 4, s->stream))) return SD_E_CUDA;
+    if (SD_CUDA(cudaMemsetAsync(s->mean, 0, sizeof(float) * 4, s->stream)) ||
+        SD_CUDA(cudaMemsetAsync(s->diag_count, 0, sizeof(unsigned long long), s->stream)))
+        return SD_E_CUDA;
     return launch_hide_range(s->pos, s->vel, 0, s->N, s->stream);
 }
 
@@ -695,7 +703,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
     if (!s || !s->configured) return fail(SD_E_STATE, "steps: not initialised");
     if (nsteps < 0) return fail(SD_E_ARG, "steps: negative count");
     DeviceGuard g(s->device);
-    const bool graphable = (s->cfg.sort_interval == 0 || s->cfg.sort_interval == 1) && !s->cfg.diagnostics;
+    const bool graphable = s->cfg.sort_interval == 0 || s->cfg.sort_interval == 1;
     int done = 0;
     // leapfrog opening kick and odd counts run eagerly
     while (done < nsteps && (!graphable || (s->cfg.integrator == SD_INT_KDK && !s->lf_open))) {
@@ -954,6 +962,25 @@ int sd_diagnostics_get(sd_sim* s, sd_diagnostics* out) {
     out->momentum[2] = d[4] * m;
     for (int j = 0; j < 3; ++j) out->mean_velocity_removed[j] = s->mean_pending ? mean[j] : 0.0;
     out->live_count = d[5];
+    return SD_OK;
+}
+
+int sd_diagnostics_history(sd_sim* s, double* out, int max_records, int* count_out) {
+    if (!s || !s->configured || !out || max_records < 0) return fail(SD_E_ARG, "diagnostics_history: bad arguments");
+    DeviceGuard g(s->device);
+    unsigned long long total = 0;
+    if (copy_out(&total, s->diag_count, sizeof(total), SD_HOST, s->stream)) return sim_error(s, SD_E_CUDA);
+    const unsigned long long avail = total < (unsigned long long)kDiagCap ? total : (unsigned long long)kDiagCap;
+    const int k = (int)(avail < (unsigned long long)max_records ? avail : (unsigned long long)max_records);
+    // the last k records, oldest first; the ring may wrap once inside them
+    for (int i = 0; i < k; ++i) {
+        const unsigned long long idx = total - (unsigned long long)k + (unsigned long long)i;
+        const double* src = s->diag_rec + (size_t)(idx % (unsigned long long)kDiagCap) * 8;
+        if (SD_CUDA(cudaMemcpyAsync(out + (size_t)i * 8, src, sizeof(double) * 8, cudaMemcpyDeviceToHost, s->stream)))
+            return sim_error(s, SD_E_CUDA);
+    }
+    if (SD_CUDA(cudaStreamSynchronize(s->stream))) return sim_error(s, SD_E_CUDA);
+    if (count_out) *count_out = k;
     return SD_OK;
 }
 

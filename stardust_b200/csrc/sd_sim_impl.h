@@ -59,6 +59,10 @@ struct sd_sim {
 
     int gather_blocks = 0;   // cap of the gather grid (0: the default); set by the ensemble autotuner
 
+    // per-step FP64 diagnostics ring (cfg.diagnostics): kDiagCap records of 8 doubles
+    double* diag_rec = nullptr;
+    unsigned long long* diag_count = nullptr;
+
     // captured steps for sd_steps
     cudaGraphExec_t graph = nullptr;
     float graph_dt = 0.f;
@@ -68,6 +72,8 @@ struct sd_sim {
 
 
 namespace sdsim {
+
+constexpr int kDiagCap = 4096;
 
 struct DeviceGuard {
     int prev = -1;

@@ -261,6 +261,15 @@ class Sim:
         return {"kinetic": d.kinetic, "potential": d.potential, "momentum": list(d.momentum),
                 "mean_velocity_removed": list(d.mean_velocity_removed), "live_count": d.live_count}
 
+    def diagnostics_history(self, max_records: int = 4096) -> np.ndarray:
+        """Per-step FP64 records (diagnostics = 1), oldest first: columns
+        step, kinetic, potential, px, py, pz, live, |mean removed|."""
+        out = np.zeros((max_records, 8), np.float64)
+        k = ctypes.c_int(0)
+        L.check(L.lib().sd_diagnostics_history(self._h, out.ctypes.data, max_records, ctypes.byref(k)),
+                "sd_diagnostics_history")
+        return out[:k.value]
+
     @staticmethod
     def kernel_launches() -> int:
         return int(L.lib().sd_kernel_launches(None))
