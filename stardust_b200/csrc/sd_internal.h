@@ -61,6 +61,8 @@ int launch_poisson_ex(const PoissonPlan& p, const long long* rho_fixed, const fl
 int launch_row_bounds(const uint32_t* keys, int n, int rows, int* row_start, cudaStream_t s);
 
 size_t gather_partials(int n);
+// one-time per-device set-up of the gather's default grid (call outside stream capture)
+int gather_prepare(int device);
 // perm != nullptr: slot i takes input particle perm[i] (fused reorder) and the
 // outputs must be separate arrays; otherwise pos_out/vel_out may alias the inputs.
 // keys_out (optional) receives the next step's order keys (key + 1).

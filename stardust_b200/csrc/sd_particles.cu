@@ -491,6 +491,32 @@ size_t gather_partials(int n) {
     return (size_t)(b < 1 ? 1 : (b > kGatherMaxBlocks ? kGatherMaxBlocks : b));
 }
 
+// Gather CTAs that are resident at once on each device (one full wave): the
+// default grid, so every CTA runs the grid-stride loop from start to end with
+// no partial last wave. Filled by gather_prepare outside any stream capture.
+namespace {
+int g_gather_wave[64] = {0};
+}
+
+int gather_prepare(int device) {
+    if (device < 0 || device >= 64) return SD_OK;
+    if (g_gather_wave[device] > 0) return SD_OK;
+    int sms = 0, per_sm = 0, per_sm_diag = 0;
+    if (SD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) ||
+        SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather_kick_drift<false>, kGatherThreads, 0)) ||
+        SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_diag, k_gather_kick_drift<true>, kGatherThreads, 0)))
+        return SD_E_CUDA;
+    const int w = sms * (per_sm < per_sm_diag ? per_sm : per_sm_diag);
+    g_gather_wave[device] = w > 0 ? w : kGatherMaxBlocks;
+    return SD_OK;
+}
+
+static int gather_wave() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || g_gather_wave[dev] <= 0) return kGatherMaxBlocks;
+    return g_gather_wave[dev];
+}
+
 int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const float4* pos_in, const float4* vel_in,
                              const int* perm, float4* pos_out, float4* vel_out, uint32_t* keys_out, int order, int n,
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
@@ -499,7 +525,8 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
     if (n <= 0) return SD_OK;
     const float h = (0.5f * (float)G) * pot_scale;  // Sim.cu:604
     int blocks = (int)gather_partials(n);
-    if (max_blocks > 0 && blocks > max_blocks) blocks = max_blocks;
+    const int cap = max_blocks > 0 ? max_blocks : gather_wave();
+    if (blocks > cap) blocks = cap;
     const bool dg = diag && partials;
     if (dg)
         k_gather_kick_drift<true><<<blocks, kGatherThreads, 0, s>>>(phi, G, h, pos_in, vel_in, perm, pos_out, vel_out,

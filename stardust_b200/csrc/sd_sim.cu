@@ -497,6 +497,11 @@ int sd_create(sd_sim** out, int device) {
     }
     s->own_stream = true;
     sd_config_default(&s->cfg);
+    if (int rc = gather_prepare(device)) {
+        cudaStreamDestroy(s->stream);
+        delete s;
+        return rc;
+    }
     *out = s;
     return SD_OK;
 }
