@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_y(float2* __restrict__ spe
 
 // ---- pass C: z-lines of CTA (bx, by): forward, Green's function, inverse ---------
 template <int G>
-__global__ void __launch_bounds__(kFftThreads, 3) k_pass_c(float2* __restrict__ spec, const float2* __restrict__ tw_g,
+__global__ void __launch_bounds__(kFftThreads) k_pass_c(float2* __restrict__ spec, const float2* __restrict__ tw_g,
                                                         const float* __restrict__ gexp_g, float scale) {
     using T = Geo<G>;
     constexpr int H = T::H;

@@ -326,18 +326,38 @@ __global__ void k_copy_keys(const uint32_t* __restrict__ kin, const int32_t* __r
 // Sorted row keys (tiled order: key = row) -> row_start[r] = first i with key >= r.
 // Thread i writes row_start[r] = i for every r in (keys[i-1], keys[i]]; the last
 // thread closes the tail up to `rows` with n.
+// Each thread covers 8 consecutive indices (two 16-byte key loads plus the key
+// before them), so the kernel streams the keys instead of waiting on them.
+constexpr int kBoundsPer = 8;
 __global__ void k_row_bounds(const uint32_t* __restrict__ keys, int n, int rows, int* __restrict__ row_start) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i > n) return;
-    const int lo = (i == 0) ? 0 : (int)min(keys[i - 1] + 1u, (uint32_t)rows);
-    const int hi = (i == n) ? rows + 1 : (int)min(keys[i] + 1u, (uint32_t)rows);
-    for (int r = lo; r < hi; ++r) row_start[r] = i;
+    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * kBoundsPer;
+    if (i0 > n) return;
+    uint32_t k[kBoundsPer];
+    if (i0 + kBoundsPer <= n) {
+        const uint4 a = *reinterpret_cast<const uint4*>(keys + i0);
+        const uint4 b = *reinterpret_cast<const uint4*>(keys + i0 + 4);
+        k[0] = a.x; k[1] = a.y; k[2] = a.z; k[3] = a.w;
+        k[4] = b.x; k[5] = b.y; k[6] = b.z; k[7] = b.w;
+    } else {
+#pragma unroll
+        for (int j = 0; j < kBoundsPer; ++j) k[j] = (i0 + j < n) ? keys[i0 + j] : 0u;
+    }
+    int lo = (i0 == 0) ? 0 : (int)min(keys[i0 - 1] + 1u, (uint32_t)rows);
+#pragma unroll
+    for (int j = 0; j < kBoundsPer; ++j) {
+        const int i = i0 + j;
+        if (i > n) break;
+        const int hi = (i == n) ? rows + 1 : (int)min(k[j] + 1u, (uint32_t)rows);
+        for (int r = lo; r < hi; ++r) row_start[r] = i;
+        if (hi > lo) lo = hi;
+    }
 }
 
 }  // namespace
 
 int launch_row_bounds(const uint32_t* keys, int n, int rows, int* row_start, cudaStream_t s) {
-    k_row_bounds<<<(n + 1 + 255) / 256, 256, 0, s>>>(keys, n, rows, row_start);
+    const int threads = (n + 1 + kBoundsPer - 1) / kBoundsPer;
+    k_row_bounds<<<(threads + 255) / 256, 256, 0, s>>>(keys, n, rows, row_start);
     SD_LAUNCHED(s);
     return SD_OK;
 }
