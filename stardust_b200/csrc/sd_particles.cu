@@ -168,7 +168,7 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double* partials) {
 // phi(x) at the step-start positions (the potential the kick used), for the
 // per-step energy record written by the finalize kernel.
 template <bool DIAG>
-__global__ void __launch_bounds__(kGatherThreads, 4) k_gather_kick_drift(
+__global__ void __launch_bounds__(kGatherThreads, 3) k_gather_kick_drift(
     const float* __restrict__ phi, int G, float h, const float4* pos_in, const float4* vel_in,
     const int* __restrict__ perm, float4* pos_out, float4* vel_out, uint32_t* __restrict__ keys_out, int order, int n,
     float dt_kick, float dt_drift, float c2, const float* __restrict__ mean_vel, double* __restrict__ partials,

@@ -410,7 +410,7 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_c(float2* __restrict__ spe
 
 // ---- pass E: kx bins -> real rows (y = 4by + y_l, z = 4bz + z_l) ----------------
 template <int G>
-__global__ void __launch_bounds__(kFftThreads) k_pass_e(const float2* __restrict__ spec, float* __restrict__ phi,
+__global__ void __launch_bounds__(kFftThreads, 5) k_pass_e(const float2* __restrict__ spec, float* __restrict__ phi,
                                                         const float2* __restrict__ tw_g) {
     using T = Geo<G>;
     constexpr int H = T::H, NBX = T::NBX;
