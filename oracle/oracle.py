@@ -257,6 +257,92 @@ def pm_accel_f64(pos: np.ndarray, G: int, pot_scale: float, soft_cells: float) -
     return a
 
 
+# ---------------------------------------------------------------------------
+# Isolated boundary in FP64 (Hockney-Eastwood on the 2G box, the reference's
+# kScatter with clamped corners Sim.cu:96-100,503-521, kGreen Sim.cu:563-576,
+# kMulSpec + FFT normalisation Sim.cu:3586-3603, kGridAccel and sampleAcc with
+# clamped indices Sim.cu:589-629).
+# ---------------------------------------------------------------------------
+def cic_weights_iso_f64(pos: np.ndarray, G: int):
+    """CIC corner cells clamped to [0, G) and their weights in FP64."""
+    g = pos[:, :3].astype(np.float64) * G - 0.5
+    i = np.floor(g).astype(np.int64)
+    f = g - i
+    out_idx, out_w = [], []
+    for k in range(8):
+        o = np.array([k & 1, (k >> 1) & 1, (k >> 2) & 1])
+        out_idx.append(np.clip(i + o, 0, G - 1))
+        out_w.append(np.prod(np.where(o[None, :] == 1, f, 1.0 - f), axis=1))
+    return out_idx, out_w
+
+
+def density_iso_f64(pos: np.ndarray, G: int) -> np.ndarray:
+    p = pos[pos[:, 0] >= 0]
+    rho = np.zeros((G, G, G), np.float64)
+    idx, w = cic_weights_iso_f64(p, G)
+    for c, wk in zip(idx, w):
+        np.add.at(rho, (c[:, 2], c[:, 1], c[:, 0]), wk)
+    return rho
+
+
+def green_isolated_f64(S: int, soft_cells: float) -> np.ndarray:
+    """kGreen: -1/(r + soft) in cells to the nearest corner copy of the S^3 box,
+    soft floored at half a cell (buildGreen, Sim.cu:3572)."""
+    soft = max(float(soft_cells), 0.5)
+    d = np.arange(S)
+    d = np.minimum(d, S - d).astype(np.float64)
+    r = np.sqrt(d[:, None, None] ** 2 + d[None, :, None] ** 2 + d[None, None, :] ** 2)
+    return -1.0 / (r + soft)
+
+
+def poisson_isolated_f64(rho: np.ndarray, soft_cells: float) -> np.ndarray:
+    """Potential on the G^3 region: the zero-padded density convolved with the
+    isolated kernel on the 2G box (what the reference's FFT pair computes)."""
+    G = rho.shape[0]
+    S = 2 * G
+    pad = np.zeros((S, S, S), np.float64)
+    pad[:G, :G, :G] = rho
+    spec = np.fft.rfftn(pad) * np.fft.rfftn(green_isolated_f64(S, soft_cells))
+    return np.fft.irfftn(spec, s=(S, S, S), axes=(0, 1, 2))[:G, :G, :G]
+
+
+def central_gradient_iso_f64(phi: np.ndarray, pot_scale: float) -> np.ndarray:
+    """kGridAccel with neighbours clamped to [0, G): (G,G,G,3), axes (x,y,z)."""
+    G = phi.shape[0]
+    h = 0.5 * G * pot_scale
+    i = np.arange(G)
+    ip, im = np.minimum(i + 1, G - 1), np.maximum(i - 1, 0)
+    ax = -(phi[:, :, ip] - phi[:, :, im]) * h
+    ay = -(phi[:, ip, :] - phi[:, im, :]) * h
+    az = -(phi[ip, :, :] - phi[im, :, :]) * h
+    return np.stack([ax, ay, az], axis=-1)
+
+
+def pm_accel_iso_f64(pos: np.ndarray, G: int, pot_scale: float, soft_cells: float) -> np.ndarray:
+    rho = density_iso_f64(pos, G)
+    grad = central_gradient_iso_f64(poisson_isolated_f64(rho, soft_cells), pot_scale)
+    idx, w = cic_weights_iso_f64(pos, G)
+    a = np.zeros((len(pos), 3), np.float64)
+    for c, wk in zip(idx, w):
+        a += grad[c[:, 2], c[:, 1], c[:, 0]] * wk[:, None]
+    return a
+
+
+def isolated_wall(p: np.ndarray, v: np.ndarray):
+    """The reference's isolated wall (Sim.cu:895-903), float32: a coordinate past
+    0.002 / 0.998 is set there and its velocity reversed inward at a quarter speed."""
+    p = p.astype(np.float32).copy()
+    v = v.astype(np.float32).copy()
+    for ax in range(3):
+        lo = p[:, ax] < np.float32(0.002)
+        p[lo, ax] = np.float32(0.002)
+        v[lo, ax] = np.abs(v[lo, ax]) * np.float32(0.25)
+        hi = p[:, ax] > np.float32(0.998)
+        p[hi, ax] = np.float32(0.998)
+        v[hi, ax] = -np.abs(v[hi, ax]) * np.float32(0.25)
+    return p, v
+
+
 def force_error(a: np.ndarray, a_ref: np.ndarray) -> dict:
     """eps = RMS(|a - a_ref|) / RMS(|a_ref|), the reference's scoring metric
     (.drive/nbody-simulator/method-search/scoring.md:38), plus the max."""

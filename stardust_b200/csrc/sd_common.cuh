@@ -22,6 +22,12 @@ __device__ __forceinline__ void cic_axis(float p, int G, int& i, float& f) {
     f = __fsub_rn(g, fl);
 }
 
+// Cell index of a CIC corner: wrapped (periodic) or clamped to the edge cell
+// (isolated; gidx3, Sim.cu:96-100 -- weights past the edge land on it).
+__device__ __forceinline__ int cic_cell(int i, int G, bool periodic) {
+    return periodic ? (i & (G - 1)) : min(max(i, 0), G - 1);
+}
+
 // Weight of corner k = ox | oy<<1 | oz<<2, as (wx*wy)*wz (Sim.cu:515).
 __device__ __forceinline__ float cic_weight(int k, float fx, float fy, float fz) {
     const float wx = (k & 1) ? fx : __fsub_rn(1.f, fx);

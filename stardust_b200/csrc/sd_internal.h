@@ -31,7 +31,8 @@ int launch_reorder(const float4* pos_in, const float4* vel_in, const int32_t* pe
                    float4* vel_out, int n, cudaStream_t s);
 
 size_t deposit_workspace_bytes(int G);
-int launch_deposit_fixed(const float4* pos, int n, int G, long long* acc, cudaStream_t s);
+// periodic = 0: corners past the edge are clamped onto the edge cells (isolated boundary)
+int launch_deposit_fixed(const float4* pos, int n, int G, long long* acc, cudaStream_t s, int periodic = 1);
 int launch_clear_u64(long long* a, size_t n, cudaStream_t s);
 int launch_fixed_to_float(const long long* acc, int G, float* rho, int clear, cudaStream_t s);
 
@@ -54,9 +55,24 @@ int launch_poisson(const PoissonPlan& p, const long long* rho_fixed, const float
 // pos != nullptr: the first pass deposits the particles itself (SD_ORDER_TILED
 // order, row_start from launch_row_bounds) instead of reading a density grid.
 // ev (optional): 4 events recorded after passes A, B, C and D.
-int launch_poisson_ex(const PoissonPlan& p, const long long* rho_fixed, const float* rho_float, const float4* pos,
-                      const int* perm, const int* row_start, float* rho_keep, float2* spec, float* phi,
-                      cudaStream_t s, cudaEvent_t* ev = nullptr);
+// Isolated-boundary options of the Poisson solve (Hockney-Eastwood, kGreen/kMulSpec,
+// Sim.cu:563-584): the density has side src_g inside the 2 src_g transform box;
+// table is the real Green spectrum (green_table_elems floats), applied with
+// table_scale; forward_only stops after the forward transform (table build).
+struct PoissonIso {
+    int src_g = 0;
+    const float* table = nullptr;
+    float table_scale = 0.f;
+    bool forward_only = false;
+};
+int launch_poisson_ex(const PoissonPlan& p, const long long* acc, const float* rho, const float4* pos,
+                      const int* perm, const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s,
+                      cudaEvent_t* ev = nullptr, const PoissonIso* iso = nullptr);
+size_t green_table_elems(int S);
+// Green spectrum of the isolated boundary on an S^3 transform box (plan of size S);
+// kernel_grid (S^3 floats) and spec are scratch.
+int build_green_table(const PoissonPlan& p, float softening_cells, float* kernel_grid, float2* spec, float* table,
+                      cudaStream_t s);
 // row_start[r] = first index i with sorted row keys[i] >= r, for r in [0, rows]
 int launch_row_bounds(const uint32_t* keys, int n, int rows, int* row_start, cudaStream_t s);
 
@@ -80,9 +96,10 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
                              const int* perm, float4* pos_out, float4* vel_out, uint32_t* keys_out, int order, int n,
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
                              double* mom_out, float* mean_out, cudaStream_t s, const float4* extra = nullptr,
-                             int max_blocks = 0, const DiagRecord* diag = nullptr);
+                             int max_blocks = 0, const DiagRecord* diag = nullptr, int iso_S = 0);
+// iso_S > 0: isolated boundary, potential box of side iso_S (= 2G), clamped sampling
 int launch_interpolate_accel(const float* phi, int G, float pot_scale, const float4* pos, float4* acc, int n,
-                             cudaStream_t s, const float4* extra = nullptr);
+                             cudaStream_t s, const float4* extra = nullptr, int iso_S = 0);
 // learned correction (sd_mlp.cu): out[i] = out_scale * MLP(features of pos[perm ? perm[i] : i])
 size_t mlp_param_count();
 int launch_mlp_infer(const float* params, const float4* pos, const int* perm, int n, const float* rho, int G,
@@ -91,7 +108,7 @@ int launch_apply_mean(float4* vel, const float4* pos, int n, const float* mean_v
 int launch_max_speed(const float4* pos, const float4* vel, int n, const float* mean_vel, float* out,
                      cudaStream_t s);
 int launch_energy(const float* phi, int G, const float4* pos, const float4* vel, int n, const float* mean_vel,
-                  double* partials, double* out8, cudaStream_t s);
+                  double* partials, double* out8, cudaStream_t s, int iso_S = 0);
 int launch_reduce_grid(const float* rho, size_t cells, int op, double* partials, double* out, cudaStream_t s);
 int launch_hide_range(float4* pos, float4* vel, int from, int to, cudaStream_t s);
 

@@ -34,7 +34,7 @@ constexpr int kGatherThreads = 256;
 constexpr int kGatherMaxBlocks = 4096;
 
 __global__ void __launch_bounds__(256) k_deposit_fixed(const float4* __restrict__ pos, int n, int G,
-                                                       unsigned long long* __restrict__ acc) {
+                                                       unsigned long long* __restrict__ acc, int periodic) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 p = pos[i];
@@ -44,12 +44,11 @@ __global__ void __launch_bounds__(256) k_deposit_fixed(const float4* __restrict_
     cic_axis(p.x, G, ix, fx);
     cic_axis(p.y, G, iy, fy);
     cic_axis(p.z, G, iz, fz);
-    const int m = G - 1;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-        const int cx = (ix + (k & 1)) & m;
-        const int cy = (iy + ((k >> 1) & 1)) & m;
-        const int cz = (iz + ((k >> 2) & 1)) & m;
+        const int cx = cic_cell(ix + (k & 1), G, periodic);
+        const int cy = cic_cell(iy + ((k >> 1) & 1), G, periodic);
+        const int cz = cic_cell(iz + ((k >> 2) & 1), G, periodic);
         const long long q = fixed_weight(cic_weight(k, fx, fy, fz));
         atomicAdd(acc + ((size_t)cz * G + cy) * G + cx, (unsigned long long)q);
     }
@@ -135,6 +134,49 @@ __device__ __forceinline__ float3 gather_accel(const float* __restrict__ phi, in
     return a;
 }
 
+// Isolated boundary (kGridAccel/sampleAcc with clamped indices, Sim.cu:589-629):
+// the potential lives in the low G^3 corner of an S^3 box (rows S apart); every
+// corner cell and its gradient neighbours are clamped to [0, G). The 8 corners'
+// 48 reads are not merged (edge clamping makes them differ); this path is not
+// the benchmark's.
+__device__ __forceinline__ float3 gather_accel_iso(const float* __restrict__ phi, int G, int S, float h, float4 p,
+                                                   float* phi_at = nullptr) {
+    int ix, iy, iz;
+    float fx, fy, fz;
+    cic_axis(p.x, G, ix, fx);
+    cic_axis(p.y, G, iy, fy);
+    cic_axis(p.z, G, iz, fz);
+    auto at = [&](int x, int y, int z) { return __ldg(phi + ((size_t)z * S + y) * S + x); };
+    float3 a = make_float3(0.f, 0.f, 0.f);
+    float f = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int cx = cic_cell(ix + (k & 1), G, false);
+        const int cy = cic_cell(iy + ((k >> 1) & 1), G, false);
+        const int cz = cic_cell(iz + ((k >> 2) & 1), G, false);
+        const int xm = max(cx - 1, 0), xp = min(cx + 1, G - 1);
+        const int ym = max(cy - 1, 0), yp = min(cy + 1, G - 1);
+        const int zm = max(cz - 1, 0), zp = min(cz + 1, G - 1);
+        const float w = cic_weight(k, fx, fy, fz);
+        const float gx = __fmul_rn(-__fsub_rn(at(xp, cy, cz), at(xm, cy, cz)), h);
+        const float gy = __fmul_rn(-__fsub_rn(at(cx, yp, cz), at(cx, ym, cz)), h);
+        const float gz = __fmul_rn(-__fsub_rn(at(cx, cy, zp), at(cx, cy, zm)), h);
+        a.x = __fmaf_rn(gx, w, a.x);
+        a.y = __fmaf_rn(gy, w, a.y);
+        a.z = __fmaf_rn(gz, w, a.z);
+        if (phi_at) f = __fmaf_rn(w, at(cx, cy, cz), f);
+    }
+    if (phi_at) *phi_at = f;
+    return a;
+}
+
+// Acceleration at p: periodic grid (S == 0) or the isolated box of side S.
+template <bool ISO>
+__device__ __forceinline__ float3 accel_at(const float* __restrict__ phi, int G, int S, float h, float4 p,
+                                           float* phi_at = nullptr) {
+    return ISO ? gather_accel_iso(phi, G, S, h, p, phi_at) : gather_accel(phi, G, h, p, phi_at);
+}
+
 // FP64 block sums of K values into partials[blockIdx.x*K + j], fixed tree order.
 template <int K>
 __device__ __forceinline__ void block_sum(double (&v)[K], double* partials) {
@@ -167,12 +209,16 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double* partials) {
 // DIAG: the FP64 partials also carry sum |v|^2 of the kicked velocities and sum
 // phi(x) at the step-start positions (the potential the kick used), for the
 // per-step energy record written by the finalize kernel.
-template <bool DIAG>
+//
+// ISO: isolated boundary (potential box of side S, clamped sampling, and the
+// reference's wall at [0.002, 0.998] that stops a particle and returns a quarter
+// of its speed, Sim.cu:895-903) instead of the periodic wrap.
+template <bool DIAG, bool ISO>
 __global__ void __launch_bounds__(kGatherThreads, 3) k_gather_kick_drift(
     const float* __restrict__ phi, int G, float h, const float4* pos_in, const float4* vel_in,
     const int* __restrict__ perm, float4* pos_out, float4* vel_out, uint32_t* __restrict__ keys_out, int order, int n,
     float dt_kick, float dt_drift, float c2, const float* __restrict__ mean_vel, double* __restrict__ partials,
-    const float4* __restrict__ extra) {
+    const float4* __restrict__ extra, int S) {
     double sx = 0.0, sy = 0.0, sz = 0.0, cnt = 0.0, sv2 = 0.0, sphi = 0.0;
     const float mx = mean_vel ? mean_vel[0] : 0.f, my = mean_vel ? mean_vel[1] : 0.f,
                 mz = mean_vel ? mean_vel[2] : 0.f;
@@ -194,7 +240,7 @@ __global__ void __launch_bounds__(kGatherThreads, 3) k_gather_kick_drift(
             v.z = __fsub_rn(v.z, mz);
         }
         float phi_p = 0.f;
-        float3 a = gather_accel(phi, G, h, p, DIAG ? &phi_p : nullptr);
+        float3 a = accel_at<ISO>(phi, G, S, h, p, DIAG ? &phi_p : nullptr);
         if (extra) {  // learned correction, indexed like the outputs
             const float4 e = extra[i];
             a.x = __fadd_rn(a.x, e.x);
@@ -223,9 +269,18 @@ __global__ void __launch_bounds__(kGatherThreads, 3) k_gather_kick_drift(
             if (keys_out) keys_out[i] = 0u;
             continue;
         }
-        p.x = __fsub_rn(p.x, floorf(p.x));
-        p.y = __fsub_rn(p.y, floorf(p.y));
-        p.z = __fsub_rn(p.z, floorf(p.z));
+        if (ISO) {
+            if (p.x < 0.002f) { p.x = 0.002f; v.x = __fmul_rn(fabsf(v.x), 0.25f); }
+            if (p.x > 0.998f) { p.x = 0.998f; v.x = -__fmul_rn(fabsf(v.x), 0.25f); }
+            if (p.y < 0.002f) { p.y = 0.002f; v.y = __fmul_rn(fabsf(v.y), 0.25f); }
+            if (p.y > 0.998f) { p.y = 0.998f; v.y = -__fmul_rn(fabsf(v.y), 0.25f); }
+            if (p.z < 0.002f) { p.z = 0.002f; v.z = __fmul_rn(fabsf(v.z), 0.25f); }
+            if (p.z > 0.998f) { p.z = 0.998f; v.z = -__fmul_rn(fabsf(v.z), 0.25f); }
+        } else {
+            p.x = __fsub_rn(p.x, floorf(p.x));
+            p.y = __fsub_rn(p.y, floorf(p.y));
+            p.z = __fsub_rn(p.z, floorf(p.z));
+        }
         pos_out[i] = p;
         vel_out[i] = v;
         if (keys_out) keys_out[i] = order_key(p, G, order);
@@ -305,7 +360,7 @@ __global__ void __launch_bounds__(256) k_finalize_mean(const double* __restrict_
 
 __global__ void __launch_bounds__(256) k_interpolate_accel(const float* __restrict__ phi, int G, float h,
                                                            const float4* __restrict__ pos, float4* __restrict__ acc,
-                                                           int n, const float4* __restrict__ extra) {
+                                                           int n, const float4* __restrict__ extra, int S) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 p = pos[i];
@@ -313,7 +368,7 @@ __global__ void __launch_bounds__(256) k_interpolate_accel(const float* __restri
         acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         return;
     }
-    float3 a = gather_accel(phi, G, h, p);
+    float3 a = S ? gather_accel_iso(phi, G, S, h, p) : gather_accel(phi, G, h, p);
     if (extra) {
         const float4 e = extra[i];
         a.x = __fadd_rn(a.x, e.x);
@@ -358,7 +413,7 @@ __global__ void __launch_bounds__(kGatherThreads) k_energy(const float* __restri
                                                            const float4* __restrict__ pos,
                                                            const float4* __restrict__ vel, int n,
                                                            const float* __restrict__ mean_vel,
-                                                           double* __restrict__ partials) {
+                                                           double* __restrict__ partials, int S) {
     double ke = 0.0, pe = 0.0, px = 0.0, py = 0.0, pz = 0.0, c = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 p = pos[i];
@@ -380,11 +435,13 @@ __global__ void __launch_bounds__(kGatherThreads) k_energy(const float* __restri
             cic_axis(p.x, G, ix, fx);
             cic_axis(p.y, G, iy, fy);
             cic_axis(p.z, G, iz, fz);
-            const int m = G - 1;
+            const bool per = S == 0;
+            const int R = per ? G : S;  // row stride of the potential
             double f = 0.0;
             for (int k = 0; k < 8; ++k) {
-                const int cx = (ix + (k & 1)) & m, cy = (iy + ((k >> 1) & 1)) & m, cz = (iz + ((k >> 2) & 1)) & m;
-                f += (double)cic_weight(k, fx, fy, fz) * (double)phi[((size_t)cz * G + cy) * G + cx];
+                const int cx = cic_cell(ix + (k & 1), G, per), cy = cic_cell(iy + ((k >> 1) & 1), G, per),
+                          cz = cic_cell(iz + ((k >> 2) & 1), G, per);
+                f += (double)cic_weight(k, fx, fy, fz) * (double)phi[((size_t)cz * R + cy) * R + cx];
             }
             pe += 0.5 * f;
         }
@@ -466,9 +523,10 @@ __global__ void k_hide_range(float4* __restrict__ pos, float4* __restrict__ vel,
 
 size_t deposit_workspace_bytes(int G) { return align_up(sizeof(long long) * (size_t)G * G * G, 256); }
 
-int launch_deposit_fixed(const float4* pos, int n, int G, long long* acc, cudaStream_t s) {
+int launch_deposit_fixed(const float4* pos, int n, int G, long long* acc, cudaStream_t s, int periodic) {
     if (n <= 0) return SD_OK;
-    k_deposit_fixed<<<(n + 255) / 256, 256, 0, s>>>(pos, n, G, reinterpret_cast<unsigned long long*>(acc));
+    k_deposit_fixed<<<(n + 255) / 256, 256, 0, s>>>(pos, n, G, reinterpret_cast<unsigned long long*>(acc),
+                                                     periodic);
     SD_LAUNCHED(s);
     return SD_OK;
 }
@@ -503,8 +561,8 @@ int gather_prepare(int device) {
     if (g_gather_wave[device] > 0) return SD_OK;
     int sms = 0, per_sm = 0, per_sm_diag = 0;
     if (SD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) ||
-        SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather_kick_drift<false>, kGatherThreads, 0)) ||
-        SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_diag, k_gather_kick_drift<true>, kGatherThreads, 0)))
+        SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather_kick_drift<false, false>, kGatherThreads, 0)) ||
+        SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_diag, k_gather_kick_drift<true, false>, kGatherThreads, 0)))
         return SD_E_CUDA;
     const int w = sms * (per_sm < per_sm_diag ? per_sm : per_sm_diag);
     g_gather_wave[device] = w > 0 ? w : kGatherMaxBlocks;
@@ -521,21 +579,25 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
                              const int* perm, float4* pos_out, float4* vel_out, uint32_t* keys_out, int order, int n,
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
                              double* mom_out, float* mean_out, cudaStream_t s, const float4* extra,
-                             int max_blocks, const DiagRecord* diag) {
+                             int max_blocks, const DiagRecord* diag, int iso_S) {
     if (n <= 0) return SD_OK;
     const float h = (0.5f * (float)G) * pot_scale;  // Sim.cu:604
     int blocks = (int)gather_partials(n);
     const int cap = max_blocks > 0 ? max_blocks : gather_wave();
     if (blocks > cap) blocks = cap;
     const bool dg = diag && partials;
-    if (dg)
-        k_gather_kick_drift<true><<<blocks, kGatherThreads, 0, s>>>(phi, G, h, pos_in, vel_in, perm, pos_out, vel_out,
-                                                                    keys_out, order, n, dt_kick, dt_drift, c2,
-                                                                    mean_vel, partials, extra);
-    else
-        k_gather_kick_drift<false><<<blocks, kGatherThreads, 0, s>>>(phi, G, h, pos_in, vel_in, perm, pos_out,
-                                                                     vel_out, keys_out, order, n, dt_kick, dt_drift,
-                                                                     c2, mean_vel, partials, extra);
+#define SD_GATHER(D, I)                                                                                            \
+    k_gather_kick_drift<D, I><<<blocks, kGatherThreads, 0, s>>>(phi, G, h, pos_in, vel_in, perm, pos_out, vel_out, \
+                                                                keys_out, order, n, dt_kick, dt_drift, c2, mean_vel,  \
+                                                                partials, extra, iso_S)
+    if (iso_S) {
+        if (dg) SD_GATHER(true, true);
+        else SD_GATHER(false, true);
+    } else {
+        if (dg) SD_GATHER(true, false);
+        else SD_GATHER(false, false);
+    }
+#undef SD_GATHER
     SD_LAUNCHED(s);
     if (dg) {
         k_finalize_mean<6><<<1, 256, 0, s>>>(partials, blocks, mom_out, mean_out, diag->rec, diag->count, diag->cap,
@@ -549,10 +611,10 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
 }
 
 int launch_interpolate_accel(const float* phi, int G, float pot_scale, const float4* pos, float4* acc, int n,
-                             cudaStream_t s, const float4* extra) {
+                             cudaStream_t s, const float4* extra, int iso_S) {
     if (n <= 0) return SD_OK;
     const float h = (0.5f * (float)G) * pot_scale;
-    k_interpolate_accel<<<(n + 255) / 256, 256, 0, s>>>(phi, G, h, pos, acc, n, extra);
+    k_interpolate_accel<<<(n + 255) / 256, 256, 0, s>>>(phi, G, h, pos, acc, n, extra, iso_S);
     SD_LAUNCHED(s);
     return SD_OK;
 }
@@ -574,10 +636,10 @@ int launch_max_speed(const float4* pos, const float4* vel, int n, const float* m
 }
 
 int launch_energy(const float* phi, int G, const float4* pos, const float4* vel, int n, const float* mean_vel,
-                  double* partials, double* out8, cudaStream_t s) {
+                  double* partials, double* out8, cudaStream_t s, int iso_S) {
     if (n <= 0) return SD_OK;
     const int blocks = (int)gather_partials(n);  // partials hold 8 doubles per block
-    k_energy<<<blocks, kGatherThreads, 0, s>>>(phi, G, pos, vel, n, mean_vel, partials);
+    k_energy<<<blocks, kGatherThreads, 0, s>>>(phi, G, pos, vel, n, mean_vel, partials, iso_S);
     SD_LAUNCHED(s);
     k_finalize8<<<1, 256, 0, s>>>(partials, blocks, out8);
     SD_LAUNCHED(s);

@@ -48,10 +48,13 @@ struct Geo {
 
 // ---- pass A: rows (y = 4by + y_l, z = 4bz + z_l) -> kx bins -----------------
 // line l = z_l*4 + y_l; positions m < H hold z[m] = x[2m] + i x[2m+1].
-template <int G, int SRC>  // SRC 0: float grid, 1: int64 fixed-point grid (zeroed after reading)
+// SRC 0: float grid, 1: int64 fixed-point grid (zeroed after reading). The source
+// grid has side src_g <= G: a smaller one (the isolated boundary's density) sits in
+// the low corner of the transform box and everything outside it reads as zero.
+template <int G, int SRC>
 __global__ void __launch_bounds__(kFftThreads) k_pass_a(const float* __restrict__ rho, long long* __restrict__ acc,
                                                         float* __restrict__ rho_keep, float2* __restrict__ spec,
-                                                        const float2* __restrict__ tw_g) {
+                                                        const float2* __restrict__ tw_g, int src_g) {
     using T = Geo<G>;
     constexpr int H = T::H, NBX = T::NBX;
     constexpr int ITEMS = 16 * (H / 2);  // (line, pair of positions)
@@ -68,14 +71,18 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_a(const float* __restrict_
         const int u = threadIdx.x + p * kFftThreads;
         if (ITEMS % kFftThreads == 0 || u < ITEMS) {
             const int l = u & 15, mp = u >> 4;
-            const size_t row = ((size_t)(bz * 4 + (l >> 2)) * G + by * 4 + (l & 3)) * G;
-            if (SRC == 0) {
-                v[p] = *reinterpret_cast<const float4*>(rho + row + 4 * mp);
-            } else {
-                const longlong2 q0 = *reinterpret_cast<const longlong2*>(acc + row + 4 * mp);
-                const longlong2 q1 = *reinterpret_cast<const longlong2*>(acc + row + 4 * mp + 2);
-                v[p] = make_float4(fixed_to_float(q0.x), fixed_to_float(q0.y), fixed_to_float(q1.x),
-                                   fixed_to_float(q1.y));
+            const int y = by * 4 + (l & 3), z = bz * 4 + (l >> 2);
+            const size_t row = ((size_t)z * src_g + y) * src_g;
+            v[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (y < src_g && z < src_g && 4 * mp < src_g) {
+                if (SRC == 0) {
+                    v[p] = *reinterpret_cast<const float4*>(rho + row + 4 * mp);
+                } else {
+                    const longlong2 q0 = *reinterpret_cast<const longlong2*>(acc + row + 4 * mp);
+                    const longlong2 q1 = *reinterpret_cast<const longlong2*>(acc + row + 4 * mp + 2);
+                    v[p] = make_float4(fixed_to_float(q0.x), fixed_to_float(q0.y), fixed_to_float(q1.x),
+                                       fixed_to_float(q1.y));
+                }
             }
         }
     }
@@ -84,12 +91,15 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_a(const float* __restrict_
         const int u = threadIdx.x + p * kFftThreads;
         if (ITEMS % kFftThreads == 0 || u < ITEMS) {
             const int l = u & 15, mp = u >> 4;
-            const size_t row = ((size_t)(bz * 4 + (l >> 2)) * G + by * 4 + (l & 3)) * G;
-            if (SRC == 1) {
-                *reinterpret_cast<longlong2*>(acc + row + 4 * mp) = make_longlong2(0, 0);
-                *reinterpret_cast<longlong2*>(acc + row + 4 * mp + 2) = make_longlong2(0, 0);
+            const int y = by * 4 + (l & 3), z = bz * 4 + (l >> 2);
+            const size_t row = ((size_t)z * src_g + y) * src_g;
+            if (y < src_g && z < src_g && 4 * mp < src_g) {
+                if (SRC == 1) {
+                    *reinterpret_cast<longlong2*>(acc + row + 4 * mp) = make_longlong2(0, 0);
+                    *reinterpret_cast<longlong2*>(acc + row + 4 * mp + 2) = make_longlong2(0, 0);
+                }
+                if (rho_keep) *reinterpret_cast<float4*>(rho_keep + row + 4 * mp) = v[p];
             }
-            if (rho_keep) *reinterpret_cast<float4*>(rho_keep + row + 4 * mp) = v[p];
             s[(2 * mp) * 16 + l] = make_float2(v[p].x, v[p].y);
             s[(2 * mp + 1) * 16 + l] = make_float2(v[p].z, v[p].w);
         }
@@ -369,9 +379,15 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_y(float2* __restrict__ spe
 }
 
 // ---- pass C: z-lines of CTA (bx, by): forward, Green's function, inverse ---------
-template <int G>
+// MODE 0: the periodic Green's function (analytic, Sim.cu:528-557).
+// MODE 1: forward transform only (builds the isolated boundary's Green spectrum).
+// MODE 2: multiply by a tabulated real Green spectrum table[|ky|][kx][|kz|]
+//         ((H+1)^3 floats) times table_scale, then inverse (isolated boundary,
+//         kMulSpec, Sim.cu:578-584).
+template <int G, int MODE>
 __global__ void __launch_bounds__(kFftThreads) k_pass_c(float2* __restrict__ spec, const float2* __restrict__ tw_g,
-                                                        const float* __restrict__ gexp_g, float scale) {
+                                                        const float* __restrict__ gexp_g, float scale,
+                                                        const float* __restrict__ table, float table_scale) {
     using T = Geo<G>;
     constexpr int H = T::H;
     extern __shared__ float2 sm[];
@@ -380,10 +396,11 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_c(float2* __restrict__ spe
     float2* s = sm + G + (H + 2) / 2 + 1;
     const int bx = blockIdx.x, by = blockIdx.y;
     for (int i = threadIdx.x; i < G; i += kFftThreads) tw[i] = tw_g[i];
-    for (int i = threadIdx.x; i <= H; i += kFftThreads) gexp[i] = gexp_g[i];
+    if (MODE == 0)
+        for (int i = threadIdx.x; i <= H; i += kFftThreads) gexp[i] = gexp_g[i];
     __shared__ float line_g[16];
     __shared__ int line_k2[16];
-    if (threadIdx.x < 16) {
+    if (MODE == 0 && threadIdx.x < 16) {
         const int l = threadIdx.x;
         const int kx = bx * 4 + (l & 3), ky = by * 4 + (l >> 2);
         const int kyf = (ky <= G / 2) ? ky : ky - G;
@@ -392,13 +409,24 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_c(float2* __restrict__ spe
     }
     load_lines<G, 2>(s, spec, bx, by);  // ends with a barrier
     fft::lines16<G, kFftThreads, 1, false>(s, tw);
-    // Green's function: -scale/k^2 * exp(-k^2 s^2/2), k = 0 -> 0 (Sim.cu:536-556),
-    // with the per-line factors of (kx, ky) hoisted; padding columns kx > H are zeroed.
+    if (MODE == 1) {
+        store_lines<G, 2>(s, spec, bx, by);
+        return;
+    }
     for (int u = threadIdx.x; u < 16 * G; u += kFftThreads) {
         const int l = u & 15, kz = u >> 4;
         const int kzf = (kz <= G / 2) ? kz : kz - G;
-        const int k2 = line_k2[l] + kzf * kzf;
-        const float m = (k2 != 0) ? __fdividef(line_g[l] * gexp[abs(kzf)], (float)k2) : 0.f;
+        float m;
+        if (MODE == 0) {
+            // Green's function: -scale/k^2 * exp(-k^2 s^2/2), k = 0 -> 0 (Sim.cu:536-556), with
+            // the per-line factors of (kx, ky) hoisted; padding columns kx > H are zeroed.
+            const int k2 = line_k2[l] + kzf * kzf;
+            m = (k2 != 0) ? __fdividef(line_g[l] * gexp[abs(kzf)], (float)k2) : 0.f;
+        } else {
+            const int kx = bx * 4 + (l & 3), ky = by * 4 + (l >> 2);
+            const int kyf = (ky <= G / 2) ? ky : G - ky;
+            m = (kx <= H) ? table[((size_t)kyf * (H + 1) + kx) * (H + 1) + abs(kzf)] * table_scale : 0.f;
+        }
         float2& e = s[u];
         e.x *= m;
         e.y *= m;
@@ -406,6 +434,32 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_c(float2* __restrict__ spe
     __syncthreads();
     fft::lines16<G, kFftThreads, 1, true>(s, tw);
     store_lines<G, 2>(s, spec, bx, by);
+}
+
+// Real part of a forward spectrum (bricked) into table[|ky|][kx][|kz|], ky, kz, kx <= H.
+template <int G>
+__global__ void k_green_table(const float2* __restrict__ spec, float* __restrict__ table) {
+    using T = Geo<G>;
+    constexpr int H = T::H;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t n = (size_t)(H + 1) * (H + 1) * (H + 1);
+    if (i >= n) return;
+    const int kz = (int)(i % (H + 1)), kx = (int)((i / (H + 1)) % (H + 1)), ky = (int)(i / ((size_t)(H + 1) * (H + 1)));
+    const size_t e = T::brick(kx >> 2, ky >> 2, kz >> 2) + (size_t)((kz & 3) * 16 + (ky & 3) * 4 + (kx & 3));
+    table[i] = spec[e].x;
+}
+
+// Real-space isolated kernel on the transform box (kGreen, Sim.cu:563-576):
+// g = -1 / (r + soft), r the distance in cells to the nearest corner copy.
+__global__ void k_green_kernel(float* __restrict__ g, int S, float soft) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)S * S * S) return;
+    const int x = (int)(i % S), y = (int)((i / S) % S), z = (int)(i / ((size_t)S * S));
+    const int dx = (x <= S / 2) ? x : S - x;
+    const int dy = (y <= S / 2) ? y : S - y;
+    const int dz = (z <= S / 2) ? z : S - z;
+    const float r = sqrtf((float)(dx * dx + dy * dy + dz * dz)) + soft;
+    g[i] = -1.0f / r;
 }
 
 // ---- pass E: kx bins -> real rows (y = 4by + y_l, z = 4bz + z_l) ----------------
@@ -510,7 +564,9 @@ struct Launcher {
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a<G, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_y<G, false>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_y<G, true>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
-        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_c<G>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_c<G, 0>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_c<G, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_c<G, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_e<G>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a_deposit<G>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a<G, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ae()));
@@ -519,7 +575,9 @@ struct Launcher {
                                            (int)smem_bd()));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_y<G, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem_bd()));
-        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_c<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c()));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_c<G, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c()));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_c<G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c()));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_c<G, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c()));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_e<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ae()));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a_deposit<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem_dep()));
@@ -527,21 +585,32 @@ struct Launcher {
     }
 
     static int run(const PoissonPlan& p, const long long* acc, const float* rho, const float4* pos, const int* perm,
-                   const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s, cudaEvent_t* ev) {
+                   const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s, cudaEvent_t* ev,
+                   const PoissonIso* iso) {
         const dim3 grid_rows(T::NBY, T::NBZ), grid_y(T::NBX, T::NBZ), grid_z(T::NBX, T::NBY);
+        const int src_g = (iso && iso->src_g > 0) ? iso->src_g : G;
         if (pos)
             k_pass_a_deposit<G><<<grid_rows, kDepositThreads, smem_dep(), s>>>(pos, perm, row_start, keep, spec, p.tw);
         else if (acc)
             k_pass_a<G, 1><<<grid_rows, kFftThreads, smem_ae(), s>>>(nullptr, const_cast<long long*>(acc), keep, spec,
-                                                                     p.tw);
+                                                                     p.tw, src_g);
         else
-            k_pass_a<G, 0><<<grid_rows, kFftThreads, smem_ae(), s>>>(rho, nullptr, keep, spec, p.tw);
+            k_pass_a<G, 0><<<grid_rows, kFftThreads, smem_ae(), s>>>(rho, nullptr, keep, spec, p.tw, src_g);
         SD_LAUNCHED(s);
         if (ev) cudaEventRecord(ev[0], s);
         k_pass_y<G, false><<<grid_y, kFftThreads, smem_bd(), s>>>(spec, p.tw);
         SD_LAUNCHED(s);
         if (ev) cudaEventRecord(ev[1], s);
-        k_pass_c<G><<<grid_z, kFftThreads, smem_c(), s>>>(spec, p.tw, p.gexp, p.scale);
+        if (iso && iso->forward_only) {
+            k_pass_c<G, 1><<<grid_z, kFftThreads, smem_c(), s>>>(spec, p.tw, p.gexp, p.scale, nullptr, 0.f);
+            SD_LAUNCHED(s);
+            return SD_OK;
+        }
+        if (iso && iso->table)
+            k_pass_c<G, 2><<<grid_z, kFftThreads, smem_c(), s>>>(spec, p.tw, p.gexp, p.scale, iso->table,
+                                                                 iso->table_scale);
+        else
+            k_pass_c<G, 0><<<grid_z, kFftThreads, smem_c(), s>>>(spec, p.tw, p.gexp, p.scale, nullptr, 0.f);
         SD_LAUNCHED(s);
         if (ev) cudaEventRecord(ev[2], s);
         k_pass_y<G, true><<<grid_y, kFftThreads, smem_bd(), s>>>(spec, p.tw);
@@ -609,16 +678,47 @@ int launch_poisson(const PoissonPlan& p, const long long* acc, const float* rho,
 
 int launch_poisson_ex(const PoissonPlan& p, const long long* acc, const float* rho, const float4* pos,
                       const int* perm, const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s,
-                      cudaEvent_t* ev) {
+                      cudaEvent_t* ev, const PoissonIso* iso) {
     switch (p.G) {
-        case 16: return Launcher<16>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev);
-        case 32: return Launcher<32>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev);
-        case 64: return Launcher<64>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev);
-        case 128: return Launcher<128>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev);
-        case 256: return Launcher<256>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev);
-        case 512: return Launcher<512>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev);
+        case 16: return Launcher<16>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso);
+        case 32: return Launcher<32>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso);
+        case 64: return Launcher<64>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso);
+        case 128: return Launcher<128>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso);
+        case 256: return Launcher<256>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso);
+        case 512: return Launcher<512>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso);
         default: return fail(SD_E_UNSUPPORTED, "poisson: grid size %d not supported", p.G);
     }
+}
+
+size_t green_table_elems(int S) {
+    const size_t h = (size_t)S / 2 + 1;
+    return h * h * h;
+}
+
+int build_green_table(const PoissonPlan& p, float softening_cells, float* kernel_grid, float2* spec, float* table,
+                      cudaStream_t s) {
+    const int S = p.G;
+    const size_t cells = (size_t)S * S * S;
+    // the reference floors the isolated softening at half a cell (buildGreen, Sim.cu:3569-3575)
+    const float soft = softening_cells > 0.5f ? softening_cells : 0.5f;
+    k_green_kernel<<<(unsigned)((cells + 255) / 256), 256, 0, s>>>(kernel_grid, S, soft);
+    SD_LAUNCHED(s);
+    PoissonIso fwd;
+    fwd.forward_only = true;
+    if (int rc = launch_poisson_ex(p, nullptr, kernel_grid, nullptr, nullptr, nullptr, nullptr, spec, nullptr, s,
+                                   nullptr, &fwd))
+        return rc;
+    const size_t n = green_table_elems(S);
+    switch (S) {
+        case 32: k_green_table<32><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(spec, table); break;
+        case 64: k_green_table<64><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(spec, table); break;
+        case 128: k_green_table<128><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(spec, table); break;
+        case 256: k_green_table<256><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(spec, table); break;
+        case 512: k_green_table<512><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(spec, table); break;
+        default: return fail(SD_E_UNSUPPORTED, "isolated: transform size %d not supported", S);
+    }
+    SD_LAUNCHED(s);
+    return SD_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -105,11 +105,30 @@ int key_bits_for(int G, int order) {
     return b;
 }
 
+bool isolated(const sd_sim* s) { return s->cfg.boundary == SD_BOUNDARY_ISOLATED; }
+
+// Side of the Poisson transform box: G (periodic) or 2G (isolated, Sim.cu:3100).
+int box_of(int G, int boundary) { return boundary == SD_BOUNDARY_ISOLATED ? 2 * G : G; }
+
 float pot_scale_of(const sd_sim* s) {
     const double n = (double)(s->N > 0 ? s->N : 1);
-    if (s->cfg.units == SD_UNITS_NEWTON)
-        return (float)(4.0 * 3.14159265358979323846 * (double)s->G * s->G * s->G * (double)s->cfg.gravity / n);
+    if (s->cfg.units == SD_UNITS_NEWTON) {
+        // periodic: the spectral Green's function carries 1/(4 pi^2) in box units (factor
+        // 4 pi G^3); isolated: -1/r in cell units (factor G)
+        const double f = isolated(s) ? (double)s->G : 4.0 * 3.14159265358979323846 * (double)s->G * s->G * s->G;
+        return (float)(f * (double)s->cfg.gravity / n);
+    }
     return s->cfg.gravity / (float)(s->N > 0 ? s->N : 1);  // potScale (Sim.cu:3107-3109)
+}
+
+// Isolated-boundary options of a Poisson solve on this handle (nullptr: periodic).
+const PoissonIso* iso_opts(const sd_sim* s, PoissonIso& o) {
+    if (!isolated(s)) return nullptr;
+    const int S = 2 * s->G;
+    o.src_g = s->G;
+    o.table = s->green;
+    o.table_scale = (float)(1.0 / ((double)S * S * S));  // kMulSpec's FFT normalisation (Sim.cu:3590-3599)
+    return &o;
 }
 
 template <class T>
@@ -126,6 +145,7 @@ void free_buffers(sd_sim* s) {
     s->sort_ws = nullptr;
     s->sort_ws_bytes = 0;
     free_dev(s->acc); free_dev(s->row_start); free_dev(s->spec); free_dev(s->phi); free_dev(s->rho);
+    free_dev(s->green);
     free_dev(s->partials); free_dev(s->mom); free_dev(s->mean);
     free_dev(s->mlp_out);
     free_dev(s->diag_rec);
@@ -146,15 +166,18 @@ int alloc_dev(T*& p, size_t count) {
     return SD_OK;
 }
 
-size_t estimate_bytes(int n, int G) {
+size_t estimate_bytes(int n, int G, int boundary) {
     const size_t N = (size_t)(n > 0 ? n : 1), cells = (size_t)G * G * G;
+    const int S = box_of(G, boundary);
+    const size_t box = (size_t)S * S * S;
     size_t b = 0;
     b += sizeof(float4) * N * 4;                       // pos, vel, pos2, vel2
     b += (sizeof(uint32_t) * 3 + sizeof(int32_t) * 2) * N;
     b += sort_workspace_bytes((int)N);
     b += sizeof(long long) * cells;                    // fixed-point deposit
-    b += sizeof(float2) * poisson_spectrum_elems(G);
-    b += sizeof(float) * cells * 2;                    // phi, kept density
+    b += sizeof(float2) * poisson_spectrum_elems(S);
+    b += sizeof(float) * (box + cells);                // phi, kept density
+    if (S != G) b += sizeof(float) * green_table_elems(S);
     b += sizeof(double) * 8 * (gather_partials((int)N) + 1024);
     return b;
 }
@@ -162,6 +185,8 @@ size_t estimate_bytes(int n, int G) {
 int allocate(sd_sim* s) {
     free_buffers(s);
     const size_t N = (size_t)s->N, cells = (size_t)s->G * s->G * s->G;
+    const int S = box_of(s->G, s->cfg.boundary);
+    const size_t box = (size_t)S * S * S;
     int rc = SD_OK;
     rc = rc ? rc : alloc_dev(s->pos, N);
     rc = rc ? rc : alloc_dev(s->vel, N);
@@ -179,8 +204,9 @@ int allocate(sd_sim* s) {
     }
     rc = rc ? rc : alloc_dev(s->acc, cells);
     rc = rc ? rc : alloc_dev(s->row_start, (size_t)s->G * s->G + 1);
-    rc = rc ? rc : alloc_dev(s->spec, poisson_spectrum_elems(s->G));
-    rc = rc ? rc : alloc_dev(s->phi, cells);
+    rc = rc ? rc : alloc_dev(s->spec, poisson_spectrum_elems(S));
+    rc = rc ? rc : alloc_dev(s->phi, box);
+    if (!rc && isolated(s)) rc = alloc_dev(s->green, green_table_elems(S));
     if (!rc && (s->cfg.keep_density || s->mlp_on)) rc = alloc_dev(s->rho, cells);
     if (!rc && s->mlp_on) rc = alloc_dev(s->mlp_out, N);
     s->partials_count = 8 * (gather_partials(s->N) + 1024);
@@ -193,7 +219,9 @@ int allocate(sd_sim* s) {
         free_buffers(s);
         return rc;
     }
-    rc = poisson_plan_build(s->plan, s->G, s->cfg.softening_cells);
+    rc = poisson_plan_build(s->plan, S, s->cfg.softening_cells);
+    // the isolated Green spectrum, with phi and the spectrum as scratch (buildGreen, Sim.cu:3569-3576)
+    if (!rc && isolated(s)) rc = build_green_table(s->plan, s->cfg.softening_cells, s->phi, s->spec, s->green, s->stream);
     if (rc) {
         free_buffers(s);
         return rc;
@@ -203,7 +231,7 @@ int allocate(sd_sim* s) {
         SD_CUDA(cudaMemsetAsync(s->mean, 0, sizeof(float) * 4, s->stream)) ||
         SD_CUDA(cudaMemsetAsync(s->mom, 0, sizeof(double) * 8, s->stream)) ||
         SD_CUDA(cudaMemsetAsync(s->diag_count, 0, sizeof(unsigned long long), s->stream)) ||
-        SD_CUDA(cudaMemsetAsync(s->phi, 0, sizeof(float) * cells, s->stream))) {
+        SD_CUDA(cudaMemsetAsync(s->phi, 0, sizeof(float) * box, s->stream))) {
         free_buffers(s);
         return SD_E_CUDA;
     }
@@ -217,8 +245,8 @@ int validate_config(const sd_config* c) {
     if (!c) return fail(SD_E_ARG, "config: null");
     if (c->particle_count <= 0 || c->particle_count > 400000000)
         return fail(SD_E_ARG, "config: particle_count %d out of range", c->particle_count);
-    if (c->boundary != SD_BOUNDARY_PERIODIC)
-        return fail(SD_E_UNSUPPORTED, "config: only the periodic boundary is implemented");
+    if (c->boundary != SD_BOUNDARY_PERIODIC && c->boundary != SD_BOUNDARY_ISOLATED)
+        return fail(SD_E_ARG, "config: bad boundary %d", c->boundary);
     if (c->order < SD_ORDER_ROWMAJOR || c->order > SD_ORDER_TILED) return fail(SD_E_ARG, "config: bad order");
     if (c->integrator != SD_INT_KD && c->integrator != SD_INT_KDK) return fail(SD_E_ARG, "config: bad integrator");
     if (c->units != SD_UNITS_REFERENCE && c->units != SD_UNITS_NEWTON) return fail(SD_E_ARG, "config: bad units");
@@ -278,9 +306,11 @@ int do_sort(sd_sim* s, int32_t* perm_out_dev) {
 
 // Field for the current positions: deposit + Poisson -> phi (computeAccel, Sim.cu:3605-3633).
 int do_field(sd_sim* s, bool keep) {
-    int rc = launch_deposit_fixed(s->pos, s->N, s->G, s->acc, s->stream);
+    int rc = launch_deposit_fixed(s->pos, s->N, s->G, s->acc, s->stream, isolated(s) ? 0 : 1);
     if (rc) return rc;
-    rc = launch_poisson(s->plan, s->acc, nullptr, keep ? s->rho : nullptr, s->spec, s->phi, s->stream);
+    PoissonIso io;
+    rc = launch_poisson_ex(s->plan, s->acc, nullptr, nullptr, nullptr, nullptr, keep ? s->rho : nullptr, s->spec,
+                           s->phi, s->stream, nullptr, iso_opts(s, io));
     if (rc) return rc;
     if (keep) s->rho_valid = true;
     return SD_OK;
@@ -314,16 +344,19 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     const bool keep = keeps_rho(s);
     // Tiled order right after a sort: the first FFT pass deposits the particles
     // itself from the row table. Otherwise: int64 atomics (any particle order).
-    const bool fused = sort && s->cfg.order == SD_ORDER_TILED;
+    // (The isolated boundary always takes the atomic deposit, which clamps corners
+    // onto the edge cells.)
+    const bool fused = sort && s->cfg.order == SD_ORDER_TILED && !isolated(s);
     if (fused) {
         if ((rc = launch_row_bounds(s->keys2, s->N, s->G * s->G, s->row_start, s->stream))) return sim_error(s, rc);
-    } else if ((rc = launch_deposit_fixed(s->pos, s->N, s->G, s->acc, s->stream))) {
+    } else if ((rc = launch_deposit_fixed(s->pos, s->N, s->G, s->acc, s->stream, isolated(s) ? 0 : 1))) {
         return sim_error(s, rc);
     }
     if (timed) cudaEventRecord(s->ev[2], s->stream);
+    PoissonIso io;
     if ((rc = launch_poisson_ex(s->plan, fused ? nullptr : s->acc, nullptr, fused ? s->pos : nullptr, perm,
                                 s->row_start, keep ? s->rho : nullptr, s->spec, s->phi, s->stream,
-                                timed ? s->pev : nullptr)))
+                                timed ? s->pev : nullptr, iso_opts(s, io))))
         return sim_error(s, rc);
     if (keep) s->rho_valid = true;
     if (timed) cudaEventRecord(s->ev[3], s->stream);
@@ -342,7 +375,7 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     rc = launch_gather_kick_drift(s->phi, s->G, pot_scale_of(s), s->pos, s->vel, perm, pos_out, vel_out, s->keys,
                                   s->cfg.order, s->N, dt_kick, dt_drift, c2, s->mean, s->partials, s->mom, s->mean,
                                   s->stream, s->mlp_on ? s->mlp_out : nullptr, s->gather_blocks,
-                                  s->cfg.diagnostics ? &diag : nullptr);
+                                  s->cfg.diagnostics ? &diag : nullptr, isolated(s) ? 2 * s->G : 0);
     if (rc) return sim_error(s, rc);
     if (perm) {
         std::swap(s->pos, s->pos2);
@@ -386,7 +419,11 @@ int reconfigure(sd_sim* s, const sd_config* c) {
     if (!structural) {
         if (s->graph) cudaGraphExecDestroy(s->graph);
         s->graph = nullptr;
-        return soft_changed ? poisson_plan_build(s->plan, s->G, s->cfg.softening_cells) : SD_OK;
+        if (!soft_changed) return SD_OK;
+        rc = poisson_plan_build(s->plan, box_of(s->G, s->cfg.boundary), s->cfg.softening_cells);
+        if (!rc && isolated(s))
+            rc = build_green_table(s->plan, s->cfg.softening_cells, s->phi, s->spec, s->green, s->stream);
+        return rc;
     }
     s->N = c->particle_count;
     s->G = G;
@@ -477,7 +514,7 @@ int sd_max_grid_size(int boundary) { return boundary == SD_BOUNDARY_ISOLATED ? 2
 
 size_t sd_estimate_bytes(int particle_count, int grid_size, int boundary) {
     const int G = ceil_pow2_clamp(grid_size, sd_max_grid_size(boundary));
-    return estimate_bytes(particle_count, G);
+    return estimate_bytes(particle_count, G, boundary);
 }
 
 int sd_create(sd_sim** out, int device) {
@@ -629,7 +666,15 @@ int sd_get_density(sd_sim* s, float* out, int where) {
 int sd_get_potential(sd_sim* s, float* out, int where) {
     if (!s || !s->configured || !out) return fail(SD_E_STATE, "get_potential: not initialised");
     DeviceGuard g(s->device);
-    return copy_out(out, s->phi, sizeof(float) * (size_t)s->G * s->G * s->G, where, s->stream);
+    if (!isolated(s)) return copy_out(out, s->phi, sizeof(float) * (size_t)s->G * s->G * s->G, where, s->stream);
+    // isolated: the G^3 corner of the 2G box, one 2D copy per z plane
+    const int G = s->G, S = 2 * G;
+    const cudaMemcpyKind k = (where == SD_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    for (int z = 0; z < G; ++z)
+        if (SD_CUDA(cudaMemcpy2DAsync(out + (size_t)z * G * G, sizeof(float) * G, s->phi + (size_t)z * S * S,
+                                      sizeof(float) * S, sizeof(float) * G, G, k, s->stream)))
+            return sim_error(s, SD_E_CUDA);
+    return (where == SD_HOST) ? SD_CUDA(cudaStreamSynchronize(s->stream)) : SD_OK;
 }
 
 int sd_get_accel(sd_sim* s, float* out, int n, int where) {
@@ -643,7 +688,7 @@ int sd_get_accel(sd_sim* s, float* out, int n, int where) {
     float4* tmp = nullptr;
     if (where == SD_HOST) tmp = s->pos2;  // scratch: pos2 is free between steps
     rc = launch_interpolate_accel(s->phi, s->G, pot_scale_of(s), s->pos, tmp ? tmp : dst, n, s->stream,
-                                  s->mlp_on ? s->mlp_out : nullptr);
+                                  s->mlp_on ? s->mlp_out : nullptr, isolated(s) ? 2 * s->G : 0);
     if (rc) return sim_error(s, rc);
     if (tmp) return copy_out(out, tmp, sizeof(float4) * (size_t)n, SD_HOST, s->stream);
     return SD_OK;
@@ -651,6 +696,7 @@ int sd_get_accel(sd_sim* s, float* out, int n, int where) {
 
 int sd_set_mlp(sd_sim* s, const float* params_device, float out_scale) {
     if (!s || !s->configured) return fail(SD_E_STATE, "set_mlp: not initialised");
+    if (params_device && isolated(s)) return fail(SD_E_UNSUPPORTED, "set_mlp: the correction is trained for periodic boxes");
     DeviceGuard g(s->device);
     if (s->graph) cudaGraphExecDestroy(s->graph);  // replays must see the new setting
     s->graph = nullptr;
@@ -794,7 +840,8 @@ int sd_synchronize(sd_sim* s) {
     const float c2 = light_speed_sq(s->cfg.length_scale, s->cfg.time_unit_scale);
     rc = launch_gather_kick_drift(s->phi, s->G, pot_scale_of(s), s->pos, s->vel, nullptr, s->pos, s->vel, s->keys,
                                   s->cfg.order, s->N, 0.5f * s->lf_dt_prev, 0.f, c2, s->mean, s->partials, s->mom,
-                                  s->mean, s->stream, s->mlp_on ? s->mlp_out : nullptr);
+                                  s->mean, s->stream, s->mlp_on ? s->mlp_out : nullptr, 0, nullptr,
+                                  isolated(s) ? 2 * s->G : 0);
     if (rc) return sim_error(s, rc);
     s->mean_pending = true;
     s->lf_open = false;
@@ -951,7 +998,7 @@ int sd_diagnostics_get(sd_sim* s, sd_diagnostics* out) {
     double d[8];
     // momentum sums of the last gather (before zeroing) and energies after zeroing
     int rc = launch_energy(s->phi, s->G, s->pos, s->vel, s->N, s->mean_pending ? s->mean : nullptr, s->partials,
-                           s->mom, s->stream);
+                           s->mom, s->stream, isolated(s) ? 2 * s->G : 0);
     if (rc) return sim_error(s, rc);
     rc = copy_out(d, s->mom, sizeof(double) * 8, SD_HOST, s->stream);
     if (rc) return sim_error(s, rc);

@@ -30,6 +30,7 @@ struct sd_sim {
     float2* spec = nullptr;     // bricked spectrum, transformed in place
     float* phi = nullptr;
     float* rho = nullptr;        // kept density (keep_density)
+    float* green = nullptr;      // isolated boundary: real Green spectrum of the 2G box
     double* partials = nullptr;  // gather / energy / reduction partials
     size_t partials_count = 0;
     double* mom = nullptr;       // 8 doubles: momentum sums of the last step, energy results

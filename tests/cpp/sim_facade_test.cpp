@@ -181,13 +181,12 @@ static void test_sticky_failure() {
     sd_clear_error();
     Sim sim;
     SimConfig cfg;
-    cfg.particleCount = 1000;
+    cfg.particleCount = 0;  // rejected: no particles
     cfg.gridSize = 32;
-    cfg.boundary = Boundary::Isolated;  // not implemented in this build
     sim.init(cfg);
     const bool f1 = Sim::failed();
     const std::string m = Sim::failMessage();
-    check(f1 && !m.empty(), "an unsupported configuration sets failed() with a message", m);
+    check(f1 && !m.empty(), "an invalid configuration sets failed() with a message", m);
     sd_clear_error();
 }
 

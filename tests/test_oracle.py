@@ -121,3 +121,20 @@ def test_oracle_against_reference_fixtures(oracle, path):
     assert err < 2e-4, err
     dp = (p1[:, :3] - f["pos_out"][:, :3] + 0.5) % 1.0 - 0.5
     assert np.abs(dp).max() < 1e-5
+
+
+def test_isolated_oracle_two_particles_attract_newtonianly(oracle):
+    """The FP64 isolated solve: two particles far from the walls and from each
+    other's padding copies attract with ~1/(r + soft)^2 in cell units."""
+    G = 32
+    pos = np.array([[0.40, 0.5, 0.5, 0], [0.60, 0.5, 0.5, 0]], np.float32)
+    a = oracle.pm_accel_iso_f64(pos, G, 1.0, 1.0)
+    r_cells = 0.2 * G
+    assert a[0, 0] > 0 and a[1, 0] < 0
+    assert abs(a[0, 0] + a[1, 0]) < 1e-9 * abs(a[0, 0])  # equal and opposite
+    # gravity 1, unit masses in count units: F ~ d/dr [1/(r + soft)] in cells, times 1/2 G per cell of gradient
+    assert a[0, 0] == pytest.approx(1.0 / (r_cells + 1.0) ** 2 * G, rel=0.15)
+    # no periodic images: the force on a particle near a wall points only to its partner
+    pos2 = np.array([[0.05, 0.5, 0.5, 0], [0.25, 0.5, 0.5, 0]], np.float32)
+    b = oracle.pm_accel_iso_f64(pos2, G, 1.0, 1.0)
+    assert b[0, 0] > 0 and b[0, 0] == pytest.approx(a[0, 0], rel=0.05)
