@@ -39,11 +39,11 @@ struct Header {
 };
 static_assert(sizeof(Header) == 76, "header layout");
 
-SimConfig plain_pm(int n, int G, float gravity, float soft, float time_scale, int sort_interval) {
+SimConfig plain_pm(int n, int G, float gravity, float soft, float time_scale, int sort_interval, Boundary b) {
     SimConfig c;  // reference defaults, then every non-gravity feature off
     c.particleCount = n;
     c.gridSize = G;
-    c.boundary = Boundary::Periodic;
+    c.boundary = b;
     c.preset = Preset::Empty;
     c.gravity = gravity;
     c.softeningCells = soft;
@@ -82,11 +82,13 @@ const char* ref_fail_message() {
     return m.c_str();
 }
 
-// Configure plain PM and load (pos, vel) through a state file at tmp_path.
-int ref_load(void* h, const float* pos, const float* vel, int n, int G, float gravity, float soft, float time_scale,
-             int sort_interval, const char* tmp_path) {
+// Configure plain PM (boundary 0 isolated, 1 periodic, as Sim.h's Boundary) and
+// load (pos, vel) through a state file at tmp_path.
+int ref_load_b(void* h, const float* pos, const float* vel, int n, int G, float gravity, float soft,
+               float time_scale, int sort_interval, int boundary, const char* tmp_path) {
+    const Boundary b = boundary == 0 ? Boundary::Isolated : Boundary::Periodic;
     Sim* s = static_cast<Sim*>(h);
-    s->init(plain_pm(n, G, gravity, soft, time_scale, sort_interval));
+    s->init(plain_pm(n, G, gravity, soft, time_scale, sort_interval, b));
     if (Sim::failed()) return -2;
     Header hd;
     std::memset(&hd, 0, sizeof(hd));
@@ -95,7 +97,7 @@ int ref_load(void* h, const float* pos, const float* vel, int n, int G, float gr
     hd.count = n;
     hd.gridSize = G;
     hd.preset = (int)Preset::Empty;
-    hd.boundary = (int)Boundary::Periodic;
+    hd.boundary = (int)b;
     hd.gravity = gravity;
     FILE* f = std::fopen(tmp_path, "wb");
     if (!f) return -5;
@@ -106,6 +108,11 @@ int ref_load(void* h, const float* pos, const float* vel, int n, int G, float gr
     if (!s->loadState(tmp_path)) return -6;
     cudaDeviceSynchronize();
     return Sim::failed() ? -2 : 0;
+}
+
+int ref_load(void* h, const float* pos, const float* vel, int n, int G, float gravity, float soft, float time_scale,
+             int sort_interval, const char* tmp_path) {
+    return ref_load_b(h, pos, vel, n, G, gravity, soft, time_scale, sort_interval, 1, tmp_path);
 }
 
 int ref_step(void* h) {
@@ -127,6 +134,7 @@ int ref_get(void* h, float* pos, float* vel, int n) {
     return 0;
 }
 
+// The density buffer holds `side`^3 floats: G (periodic) or the 2G box (isolated).
 int ref_density(void* h, float* out, int G) {
     Sim* s = static_cast<Sim*>(h);
     const size_t cells = (size_t)G * G * G;

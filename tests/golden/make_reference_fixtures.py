@@ -34,6 +34,7 @@ def load_ref():
     L.ref_create.restype = P
     L.ref_destroy.argtypes = [P]
     L.ref_load.argtypes = [P, P, P, I, I, F, F, F, I, ctypes.c_char_p]
+    L.ref_load_b.argtypes = [P, P, P, I, I, F, F, F, I, I, ctypes.c_char_p]
     L.ref_step.argtypes = [P]
     L.ref_steps.argtypes = [P, I]
     L.ref_get.argtypes = [P, P, P, I]
@@ -45,18 +46,21 @@ def load_ref():
     return L
 
 
-def run_case(L, pos, vel, G, gravity, soft, dt, tmpdir):
+def run_case(L, pos, vel, G, gravity, soft, dt, tmpdir, boundary=1):
+    """boundary: 1 periodic, 0 isolated (Sim.h's Boundary enum)."""
     n = len(pos)
     h = L.ref_create()
     try:
         path = os.path.join(tmpdir, "in.stardust").encode()
         # timeScale = dt / 0.0016 gives dt = 0.0016 * dtScaleFor(timeScale) (Sim.h:89-93)
         ts = np.float32(dt) / np.float32(0.0016)
-        rc = L.ref_load(h, pos.ctypes.data, vel.ctypes.data, n, G, gravity, soft, float(ts), 1, path)
+        rc = L.ref_load_b(h, pos.ctypes.data, vel.ctypes.data, n, G, gravity, soft, float(ts), 1, boundary, path)
         if rc != 0:
             raise RuntimeError(f"ref_load failed: {rc} {L.ref_fail_message()}")
-        rho = np.empty(G ** 3, np.float32)
-        L.ref_density(h, rho.ctypes.data, G)
+        side = G if boundary == 1 else 2 * G  # the isolated density lives in the 2G box
+        rho = np.empty(side ** 3, np.float32)
+        L.ref_density(h, rho.ctypes.data, side)
+        rho = rho.reshape(side, side, side)[:G, :G, :G].copy()
         rc = L.ref_step(h)
         if rc != 0:
             raise RuntimeError(f"ref_step failed: {L.ref_fail_message()}")
@@ -65,7 +69,7 @@ def run_case(L, pos, vel, G, gravity, soft, dt, tmpdir):
         L.ref_get(h, p1.ctypes.data, v1.ctypes.data, n)
         t = np.empty(6, np.float32)
         L.ref_timings(h, t.ctypes.data)
-        return rho.reshape(G, G, G), p1, v1, float(t[4])
+        return rho, p1, v1, float(t[4])
     finally:
         L.ref_destroy(h)
 
@@ -80,23 +84,29 @@ def cases():
     pos[:, :3][pos[:, :3] >= 1.0] = 0.0
     vel = np.zeros((n, 4), np.float32)
     vel[:, :3] = rng.normal(scale=0.2, size=(n, 3))
-    yield "clustered_g16", pos, vel, 16, float(4 * np.pi * 16 ** 3), 1.0, 1e-3
+    yield "clustered_g16", pos, vel, 16, float(4 * np.pi * 16 ** 3), 1.0, 1e-3, 1
     p, v = scenes.disk_galaxy(8192, 7)
-    yield "disk_g32", p, v, 32, float(4 * np.pi * 32 ** 3), 1.0, 1e-3
+    yield "disk_g32", p, v, 32, float(4 * np.pi * 32 ** 3), 1.0, 1e-3, 1
+    # isolated boundary (the reference's default): a disk galaxy, a few particles
+    # against the walls moving into them; gravity G = Newton's G = 1 for -1/r in cells
+    p, v = scenes.disk_galaxy(8192, 11)
+    p[:4, 0] = [0.0015, 0.0025, 0.9975, 0.9985]
+    v[:4, 0] = [-1.0, -2.0, 2.0, 1.0]
+    yield "isolated_g32", p, v, 32, 32.0, 1.5, 1e-3, 0
 
 
 def main(outdir: str) -> int:
     os.makedirs(outdir, exist_ok=True)
     L = load_ref()
     with tempfile.TemporaryDirectory() as tmp:
-        for name, pos, vel, G, grav, soft, dt in cases():
+        for name, pos, vel, G, grav, soft, dt, boundary in cases():
             pos = np.ascontiguousarray(pos, np.float32)
             vel = np.ascontiguousarray(vel, np.float32)
             vel[:, 3] = np.arange(len(vel), dtype=np.float32)  # id through the reference's sort
-            rho, p1, v1, dt_used = run_case(L, pos, vel, G, grav, soft, dt, tmp)
+            rho, p1, v1, dt_used = run_case(L, pos, vel, G, grav, soft, dt, tmp, boundary)
             np.savez_compressed(os.path.join(outdir, f"reference_{name}.npz"), pos_in=pos, vel_in=vel,
                                 rho_loaded=rho, pos_out=p1, vel_out=v1, grid=G, gravity=grav, soft=soft,
-                                dt=np.float32(dt_used))
+                                dt=np.float32(dt_used), boundary=boundary)
             print(name, "dt_used", dt_used, "mass", float(rho.sum()))
     return 0
 

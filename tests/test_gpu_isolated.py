@@ -118,3 +118,28 @@ def test_isolated_state_round_trip(cuda, tmp_path):
         assert t.config().boundary == L.SD_BOUNDARY_ISOLATED and t.grid_size() == G
         p1, v1 = t.get_particles()
     assert np.array_equal(p0, p1) and np.array_equal(v0, v1)
+
+
+def test_isolated_step_matches_reference_fixture(cuda):
+    """One step of the unmodified reference in isolated mode (committed fixture,
+    tests/golden/make_reference_fixtures.py) reproduced through the C ABI."""
+    import os
+
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_isolated_g32.npz")
+    f = np.load(path)
+    G, grav, soft, dt = int(f["grid"]), float(f["gravity"]), float(f["soft"]), float(f["dt"])
+    pos0, vel0 = f["pos_in"], f["vel_in"]
+    n = len(pos0)
+    with iso_sim(n, G, gravity=grav, softening_cells=soft) as s:
+        s.set_particles(pos0, vel0)
+        rho = s.density()
+        s.step(dt)
+        p1, v1 = s.get_particles()
+    assert np.abs(rho - f["rho_loaded"]).max() <= 2e-5 * float(f["rho_loaded"].max())
+    order = np.argsort(v1[:, 3].astype(np.int64))
+    ref_order = np.argsort(f["vel_out"][:, 3].astype(np.int64))
+    p1, v1 = p1[order], v1[order]
+    p_ref, v_ref = f["pos_out"][ref_order], f["vel_out"][ref_order]
+    dv, dv_ref = v1[:, :3] - vel0[:, :3], v_ref[:, :3] - vel0[:, :3]
+    assert rel_rms(dv, dv_ref) < 1e-4
+    assert np.abs(p1[:, :3] - p_ref[:, :3]).max() < 2e-6

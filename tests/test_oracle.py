@@ -92,8 +92,9 @@ def test_pm_accel_f64_two_particles_antisymmetric(oracle):
     assert abs(a[0, 0] + a[1, 0]) < 1e-9 * abs(a[0, 0]) + 1e-12
 
 
-def _golden_files():
-    return sorted(glob.glob(os.path.join(GOLDEN, "reference_*.npz")))
+def _golden_files(isolated=False):
+    files = sorted(glob.glob(os.path.join(GOLDEN, "reference_*.npz")))
+    return [f for f in files if ("isolated" in os.path.basename(f)) == isolated]
 
 
 @pytest.mark.skipif(not _golden_files(), reason="no reference fixtures committed")
@@ -138,3 +139,31 @@ def test_isolated_oracle_two_particles_attract_newtonianly(oracle):
     pos2 = np.array([[0.05, 0.5, 0.5, 0], [0.25, 0.5, 0.5, 0]], np.float32)
     b = oracle.pm_accel_iso_f64(pos2, G, 1.0, 1.0)
     assert b[0, 0] > 0 and b[0, 0] == pytest.approx(a[0, 0], rel=0.05)
+
+
+@pytest.mark.skipif(not _golden_files(True), reason="no isolated reference fixture committed")
+@pytest.mark.parametrize("path", _golden_files(True))
+def test_isolated_oracle_against_reference_fixture(oracle, path):
+    """The FP64 isolated oracle (clamped deposit, 2G-box Green's function,
+    clamped gradient and gather, the wall, momentum zeroing) reproduces one step
+    of the unmodified reference in its default isolated mode."""
+    f = np.load(path)
+    G, grav, soft, dt = int(f["grid"]), float(f["gravity"]), float(f["soft"]), float(f["dt"])
+    pos0, vel0 = f["pos_in"], f["vel_in"]
+    n = len(pos0)
+    rho = oracle.density_iso_f64(pos0, G)
+    assert np.abs(rho - f["rho_loaded"]).max() <= 2e-5 * float(rho.max())
+    a = oracle.pm_accel_iso_f64(pos0, G, grav / n, soft)
+    vk = (vel0[:, :3] + a * dt).astype(np.float32)
+    pk = (pos0[:, :3] + vk.astype(np.float64) * dt).astype(np.float32)
+    pw, vw = oracle.isolated_wall(pk, vk)
+    vw = vw - vw.mean(axis=0, dtype=np.float64).astype(np.float32)
+    ids = f["vel_out"][:, 3].astype(np.int64)
+    p_ref, v_ref = f["pos_out"][:, :3], f["vel_out"][:, :3]
+    dv_ref = v_ref - vel0[ids, :3]
+    dv = vw[ids] - vel0[ids, :3]
+    scale = np.sqrt(np.mean(np.sum(dv_ref.astype(np.float64) ** 2, axis=1)))
+    err = np.sqrt(np.mean(np.sum((dv - dv_ref).astype(np.float64) ** 2, axis=1))) / scale
+    assert err < 2e-4, err
+    assert np.abs(pw[ids] - p_ref).max() < 1e-5
+    assert p_ref.min() >= 0.002 and p_ref.max() <= 0.998
