@@ -329,6 +329,30 @@ int sd_ensemble_synchronize(sd_ensemble* ens);
 void* sd_ensemble_stream(const sd_ensemble* ens);
 long long sd_ensemble_graph_kernels(const sd_ensemble* ens);
 
+/* ---- headless point render (kSplatPoints -> kAccumToRGBA, RenderField.cu:318-735)
+ * Particle buffers to an RGBA8 image in device memory (rows top-down), without
+ * OpenGL. Gas particles (pos.w == 0) only; colour by density (0) or speed (2).
+ * Sums are 64-bit fixed point, so an image does not depend on particle order. */
+typedef struct sd_view {
+    float rot[9];        /* row-major view rotation (ViewRot.m, ViewRot.h:25-31) */
+    float center[3];     /* rotation centre (ViewRot.cx/cy/cz) */
+    int32_t fly;         /* 1: perspective from the centre, 0: orthographic */
+    float tan_half_fov;  /* perspective only */
+    float zoom, pan_x, pan_y;
+    float size_px;       /* particle footprint before the visibility cap */
+    int32_t color_by;    /* 0 density, 2 speed */
+    int32_t cmap;        /* 0 astro, 1 gray, 2 thermal */
+    float bright, inv_gamma;
+    int32_t use_cmap;    /* 1: accumulated brightness through the colour map */
+    int32_t reinhard;    /* 1: x / (1 + x) tone curve when use_cmap is 0 */
+    int32_t reserved[4];
+} sd_view;
+void sd_view_default(sd_view* view); /* top-down, zoom 1, density, astro map */
+size_t sd_render_workspace_bytes(int width, int height);
+/* pos, vel: device float4[n]; rgba_out: device uchar4[width * height] */
+int sd_render_points(const float* pos, const float* vel, int n, const sd_view* view, int width, int height,
+                     void* workspace, size_t workspace_bytes, void* rgba_out, void* stream);
+
 /* ---- FP64 reference forces (force-error judge; not on the step) ------------
  * Periodic Newtonian accelerations (G = 1, each source of mass 1/n_src, mean
  * density removed) of Gaussian-smoothed masses of width `softening` (box units;

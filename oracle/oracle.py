@@ -485,3 +485,94 @@ def mlp_loss_grad(params, X, T, round_bf16: bool = True):
     put("W1", c["X"].T @ dz1)
     put("b1", dz1.sum(axis=0))
     return sse, g
+
+
+# ---------------------------------------------------------------------------
+# Headless point render (kSplatPoints -> kAccumToRGBA, src/gfx/RenderField.cu
+# 318-735; projectPoint src/sim/ViewRot.h:76-96), numpy float64 math with the
+# same 2^-24 fixed-point accumulation as the GPU.
+# ---------------------------------------------------------------------------
+_ASTRO_C = np.array([[0.00, 0.00, 0.00], [0.05, 0.06, 0.19], [0.16, 0.14, 0.47], [0.47, 0.27, 0.67],
+                     [0.88, 0.55, 0.27], [1.00, 0.84, 0.51], [1.00, 1.00, 0.94]])
+_ASTRO_S = np.array([0.00, 0.18, 0.38, 0.58, 0.76, 0.90, 1.00])
+
+
+def _cmap(kind: int, t: np.ndarray) -> np.ndarray:
+    t = np.clip(np.asarray(t, np.float64), 0.0, 1.0)
+    if kind == 1:
+        return np.stack([t, t, t], axis=-1)
+    if kind == 2:
+        return np.stack([np.minimum(t * 2.2, 1.0), np.clip((t - 0.32) * 1.9, 0.0, 1.0),
+                         np.clip((t - 0.70) * 3.2, 0.0, 1.0)], axis=-1)
+    return np.stack([np.interp(t, _ASTRO_S, _ASTRO_C[:, j]) for j in range(3)], axis=-1)
+
+
+def render_points(pos, vel, view: dict, W: int, H: int) -> np.ndarray:
+    """(H, W, 4) uint8 image of the gas particles."""
+    pos = np.asarray(pos, np.float64)
+    vel = np.asarray(vel, np.float64)
+    n = len(pos)
+    keep = (pos[:, 0] >= 0) & (pos[:, 3] == 0)
+    p, v = pos[keep], vel[keep]
+    R = np.asarray(view["rot"], np.float64).reshape(3, 3)
+    f = p[:, :3] - np.asarray(view["center"], np.float64)
+    xc, yc, zc = f @ R[0], f @ R[1], f @ R[2]
+    depth = np.ones(len(p))
+    if view["fly"]:
+        ok = zc >= 1e-3
+        k = 0.5 / (np.where(ok, zc, 1.0) * view["tan_half_fov"])
+        u, w = xc * k + 0.5, yc * k + 0.5
+        depth = zc
+    else:
+        ok = np.ones(len(p), bool)
+        u = (xc + view["pan_x"]) * view["zoom"] + 0.5
+        w = (yc + view["pan_y"]) * view["zoom"] + 0.5
+    aspect = W / H
+    if aspect > 1:
+        u = (u - 0.5) / aspect + 0.5
+    else:
+        w = (w - 0.5) * aspect + 0.5
+    ok &= (u >= 0) & (u < 1) & (w >= 0) & (w < 1)
+    x = (u * W).astype(np.int64)
+    y = ((1.0 - w) * H).astype(np.int64)
+    ok &= (x >= 0) & (x < W) & (y >= 0) & (y < H)
+    if view["color_by"] == 0:
+        base = {1: [1.0, 1.0, 1.0], 2: list(_cmap(2, np.array([0.62]))[0])}.get(view["cmap"], [0.55, 0.42, 0.85])
+        c = np.tile(np.asarray(base, np.float64), (len(p), 1))
+    else:
+        t = np.full(len(p), 0.5)
+        if view["color_by"] == 2:
+            t = np.minimum(np.sqrt(np.sum(v[:, :3] ** 2, axis=1)) * 0.25, 1.0)
+        c = _cmap(view["cmap"], t)
+    visible = n / max(view["zoom"] ** 2, 1.0)
+    cap = 0 if visible > 8.0e6 else (1 if visible > 2.0e6 else 2)
+    grow = (np.minimum(0.35 / np.maximum(depth, 1e-3), 6.0) if view["fly"]
+            else np.full(len(p), min(np.sqrt(max(view["zoom"], 1.0)), 4.0)))
+    rr = view["size_px"] * grow
+    rad = np.minimum(np.where(rr < 2.0, 0, np.where(rr < 4.0, 1, 2)), cap)
+    acc = np.zeros((H, W, 3), np.int64)
+    kern = {0: np.array([1.0]), 1: np.array([0.25, 0.5, 0.25]), 2: np.array([0.0625, 0.25, 0.375, 0.25, 0.0625])}
+    for r in (0, 1, 2):
+        sel = ok & (rad == r)
+        k = kern[r]
+        for dy in range(-r, r + 1):
+            for dx in range(-r, r + 1):
+                xx, yy = x[sel] + dx, y[sel] + dy
+                inb = (xx >= 0) & (xx < W) & (yy >= 0) & (yy < H)
+                q = np.rint(c[sel][inb] * (k[dy + r] * k[dx + r]) * 16777216.0).astype(np.int64)
+                np.add.at(acc, (yy[inb], xx[inb]), q)
+    a = acc.astype(np.float64) / 16777216.0
+    lum = a.sum(axis=-1) * 0.3333
+    out = np.zeros((H, W, 4), np.uint8)
+    if view["use_cmap"]:
+        t = np.power(np.minimum(np.log1p(lum * view["bright"]) * 0.42, 1.0), view["inv_gamma"])
+        rgb = _cmap(view["cmap"], t)
+    else:
+        x_ = np.log1p(lum * view["bright"]) * 0.42
+        tone = (np.power(np.maximum(x_, 0) / (1 + np.maximum(x_, 0)), view["inv_gamma"]) if view["reinhard"]
+                else np.power(np.minimum(x_, 1.0), view["inv_gamma"]))
+        s = np.where(lum > 1e-6, tone / np.maximum(lum, 1e-30), 0.0)
+        rgb = np.minimum(a * s[..., None], 1.0)
+    out[..., :3] = (np.minimum(rgb, 1.0) * 255.0).astype(np.uint8)
+    out[..., 3] = 255
+    return out

@@ -54,6 +54,14 @@ class SdTimings(ctypes.Structure):
     ]
 
 
+class SdView(ctypes.Structure):
+    _fields_ = [("rot", ctypes.c_float * 9), ("center", ctypes.c_float * 3), ("fly", ctypes.c_int32),
+                ("tan_half_fov", ctypes.c_float), ("zoom", ctypes.c_float), ("pan_x", ctypes.c_float),
+                ("pan_y", ctypes.c_float), ("size_px", ctypes.c_float), ("color_by", ctypes.c_int32),
+                ("cmap", ctypes.c_int32), ("bright", ctypes.c_float), ("inv_gamma", ctypes.c_float),
+                ("use_cmap", ctypes.c_int32), ("reinhard", ctypes.c_int32), ("reserved", ctypes.c_int32 * 4)]
+
+
 class SdSceneTuning(ctypes.Structure):
     _fields_ = [("order", ctypes.c_int32), ("gather_blocks", ctypes.c_int32), ("step_ms", ctypes.c_float),
                 ("reserved", ctypes.c_int32)]
@@ -146,6 +154,9 @@ SIGNATURES = [
     ("sd_ensemble_synchronize", _I, [_P]),
     ("sd_ensemble_stream", _P, [_P]),
     ("sd_ensemble_graph_kernels", _LL, [_P]),
+    ("sd_view_default", None, [_P]),
+    ("sd_render_workspace_bytes", _S, [_I, _I]),
+    ("sd_render_points", _I, [_P, _P, _I, _P, _I, _I, _P, _S, _P, _P]),
     ("sd_ewald_modes", _I, [_I]),
     ("sd_ewald_workspace_bytes", _S, [_I]),
     ("sd_ewald_forces", _I, [_P, _I, _P, _I, _D, _D, _I, _P, _P, _S, _P]),
