@@ -120,12 +120,19 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* 
     int32_t v[kSortItems];
     unsigned rank[kSortItems];
     // Each warp owns a contiguous run of 32*kSortItems inputs, visited in order.
+    // All of a thread's loads are issued before the ranking, which synchronises
+    // the warp after every item.
 #pragma unroll
     for (int it = 0; it < kSortItems; ++it) {
         const int idx = tile0 + w * 32 * kSortItems + it * 32 + lane;
         const bool valid = idx < n;
         k[it] = valid ? keys_in[idx] : 0u;
         v[it] = valid ? (vals_in ? vals_in[idx] : idx) : 0;
+    }
+#pragma unroll
+    for (int it = 0; it < kSortItems; ++it) {
+        const int idx = tile0 + w * 32 * kSortItems + it * 32 + lane;
+        const bool valid = idx < n;
         const unsigned d = (k[it] >> shift) & mask;
         const unsigned vmask = __ballot_sync(0xffffffffu, valid);
         unsigned before = 0u, peers = 0u;
