@@ -83,10 +83,20 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_counts(const uint32_t* _
     for (int d = threadIdx.x; d < kRadix; d += kSortThreads) hist[d] = 0u;
     __syncthreads();
     const int base = blockIdx.x * kSortTile;
+    // Nearly sorted keys put few distinct digits in a warp: one shared add per
+    // digit and warp (of the number of lanes holding it) instead of one per key.
+    unsigned dd[kSortItems];
 #pragma unroll
     for (int it = 0; it < kSortItems; ++it) {
         const int idx = base + it * kSortThreads + threadIdx.x;
-        if (idx < n) atomicAdd(&hist[(keys[idx] >> shift) & mask], 1u);
+        dd[it] = (idx < n) ? ((keys[idx] >> shift) & mask) : 0xffffffffu;
+    }
+    const unsigned lt = lanemask_lt();
+#pragma unroll
+    for (int it = 0; it < kSortItems; ++it) {
+        const unsigned d = dd[it];
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        if ((peers & lt) == 0u && d != 0xffffffffu) atomicAdd(&hist[d], (unsigned)__popc(peers));
     }
     __syncthreads();
     // tile-major rows: one coalesced row of kRadix counts per tile
