@@ -134,9 +134,25 @@ struct radix_of {
 };
 
 // One Stockham stage on the 16 interleaved lines, then recurse.
-template <int N, int Ns, int NT, int TWS, bool INV>
+// radix_of as a constexpr function, and the sub-transform length Ns of the last
+// stage of an N-point transform on NT threads.
+constexpr int radix_for(int rem, int N, int NT) {
+    return (rem % 32 == 0 && 16 * N / 32 >= NT)   ? 32
+           : (rem % 16 == 0 && 16 * N / 16 >= NT) ? 16
+           : (rem % 8 == 0)                       ? 8
+           : (rem % 4 == 0)                       ? 4
+                                                  : 2;
+}
+constexpr int last_stage_ns(int N, int NT) {
+    int ns = 1;
+    while (ns * radix_for(N / ns, N, NT) < N) ns *= radix_for(N / ns, N, NT);
+    return ns;
+}
+
+// Stages from sub-transform length Ns on, stopping before the stage at STOP.
+template <int N, int Ns, int NT, int TWS, bool INV, int STOP = N>
 __device__ __forceinline__ void stages16(float2* s, const float2* tw) {
-    if constexpr (Ns < N) {
+    if constexpr (Ns < N && Ns < STOP) {
         constexpr int R = radix_of<N / Ns, N, NT>::value;
         constexpr int NB = N / R;
         constexpr int TOT = 16 * NB;
@@ -172,7 +188,7 @@ __device__ __forceinline__ void stages16(float2* s, const float2* tw) {
             }
         }
         __syncthreads();
-        stages16<N, Ns * R, NT, TWS, INV>(s, tw);
+        stages16<N, Ns * R, NT, TWS, INV, STOP>(s, tw);
     }
 }
 
@@ -181,6 +197,54 @@ __device__ __forceinline__ void stages16(float2* s, const float2* tw) {
 template <int N, int NT, int TWS, bool INV>
 __device__ __forceinline__ void lines16(float2* s, const float2* tw) {
     stages16<N, 1, NT, TWS, INV>(s, tw);
+}
+
+// Forward transform, a pointwise multiply, inverse transform of the 16 lines.
+// The forward's last stage (radix R, sub-length Ns = N / R) leaves, in each
+// thread's registers, the outputs at positions j + r Ns -- exactly the inputs of
+// an inverse first stage of the same radix. So that stage, the multiply
+// mul(line, position, value) and the inverse's first stage run in registers with
+// no shared-memory round trip or barrier between them; the inverse then goes on
+// from sub-length R. The caller synchronises before the call; it ends with a
+// barrier.
+template <int N, int NT, int TWS, class Mul>
+__device__ __forceinline__ void convolve16(float2* s, const float2* tw, Mul mul) {
+    constexpr int NsL = last_stage_ns(N, NT);
+    constexpr int R = N / NsL;
+    constexpr int NB = N / R;  // == NsL
+    constexpr int TOT = 16 * NB;
+    constexpr int PER = (TOT + NT - 1) / NT;
+    stages16<N, 1, NT, TWS, false, NsL>(s, tw);
+    float2 v[PER][R];
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+        const int u = threadIdx.x + p * NT;
+        if (TOT % NT == 0 || u < TOT) {
+            const int l = u & 15, j = u >> 4;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                float2 x = s[(j + r * NB) * 16 + l];
+                if (NsL > 1 && r > 0) x = cmul(x, tw[(j * r) * TWS]);
+                v[p][r] = x;
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+        const int u = threadIdx.x + p * NT;
+        if (TOT % NT == 0 || u < TOT) {
+            const int l = u & 15, j = u >> 4;
+            dft<R, false>(v[p]);
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[p][r] = mul(l, j + r * NsL, v[p][r]);
+            dft<R, true>(v[p]);
+#pragma unroll
+            for (int r = 0; r < R; ++r) s[(j * R + r) * 16 + l] = v[p][r];
+        }
+    }
+    __syncthreads();
+    stages16<N, R, NT, TWS, true>(s, tw);
 }
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {

@@ -408,13 +408,14 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_c(float2* __restrict__ spe
         line_k2[l] = kx * kx + kyf * kyf;
     }
     load_lines<G, 2>(s, spec, bx, by);  // ends with a barrier
-    fft::lines16<G, kFftThreads, 1, false>(s, tw);
     if (MODE == 1) {
+        fft::lines16<G, kFftThreads, 1, false>(s, tw);
         store_lines<G, 2>(s, spec, bx, by);
         return;
     }
-    for (int u = threadIdx.x; u < 16 * G; u += kFftThreads) {
-        const int l = u & 15, kz = u >> 4;
+    // forward, Green's function, inverse; the multiply happens in registers between
+    // the forward's last stage and the inverse's first
+    auto green = [&](int l, int kz, float2 x) {
         const int kzf = (kz <= G / 2) ? kz : kz - G;
         float m;
         if (MODE == 0) {
@@ -427,12 +428,9 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_c(float2* __restrict__ spe
             const int kyf = (ky <= G / 2) ? ky : G - ky;
             m = (kx <= H) ? table[((size_t)kyf * (H + 1) + kx) * (H + 1) + abs(kzf)] * table_scale : 0.f;
         }
-        float2& e = s[u];
-        e.x *= m;
-        e.y *= m;
-    }
-    __syncthreads();
-    fft::lines16<G, kFftThreads, 1, true>(s, tw);
+        return make_float2(x.x * m, x.y * m);
+    };
+    fft::convolve16<G, kFftThreads, 1>(s, tw, green);
     store_lines<G, 2>(s, spec, bx, by);
 }
 
