@@ -247,6 +247,48 @@ __device__ __forceinline__ void convolve16(float2* s, const float2* tw, Mul mul)
     stages16<N, R, NT, TWS, true>(s, tw);
 }
 
+// lines16, with the last stage writing its outputs row-major (line l at
+// s[l * RS + position]) instead of interleaved, for callers that store rows.
+template <int N, int NT, int TWS, bool INV, int RS>
+__device__ __forceinline__ void lines16_rows(float2* s, const float2* tw) {
+    constexpr int NsL = last_stage_ns(N, NT);
+    constexpr int R = N / NsL;
+    constexpr int NB = N / R;
+    constexpr int TOT = 16 * NB;
+    constexpr int PER = (TOT + NT - 1) / NT;
+    stages16<N, 1, NT, TWS, INV, NsL>(s, tw);
+    float2 v[PER][R];
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+        const int u = threadIdx.x + p * NT;
+        if (TOT % NT == 0 || u < TOT) {
+            const int l = u & 15, j = u >> 4;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                float2 x = s[(j + r * NB) * 16 + l];
+                if (NsL > 1 && r > 0) {
+                    float2 w = tw[(j * r) * TWS];
+                    if (INV) w.y = -w.y;
+                    x = cmul(x, w);
+                }
+                v[p][r] = x;
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+        const int u = threadIdx.x + p * NT;
+        if (TOT % NT == 0 || u < TOT) {
+            const int l = u & 15, j = u >> 4;
+            dft<R, INV>(v[p]);
+#pragma unroll
+            for (int r = 0; r < R; ++r) s[l * RS + j + r * NsL] = v[p][r];
+        }
+    }
+    __syncthreads();
+}
+
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");

@@ -513,27 +513,12 @@ __global__ void __launch_bounds__(kFftThreads, 5) k_pass_e(const float2* __restr
         }
     }
     __syncthreads();
-    fft::lines16<H, kFftThreads, 2, true>(s, tw);
-    // Interleaved lines -> row-major rows (stride H + 2 float2, 16-byte aligned) in
-    // place through registers, so each warp then writes 512 contiguous bytes of
-    // one row instead of 32 bytes of each of 16 rows.
+    // The last stage leaves the lines row-major (stride H + 2 float2, 16-byte
+    // aligned), so each warp then writes 512 contiguous bytes of one row instead
+    // of 32 bytes of each of 16 rows.
     constexpr int RS = H + 2;
-    constexpr int TITEMS = 16 * H;
-    constexpr int TPER = (TITEMS + kFftThreads - 1) / kFftThreads;
     static_assert(16 * RS <= 16 * T::PX, "row staging fits the line buffer");
-    float2 t[TPER];
-#pragma unroll
-    for (int p = 0; p < TPER; ++p) {
-        const int u = threadIdx.x + p * kFftThreads;
-        if (TITEMS % kFftThreads == 0 || u < TITEMS) t[p] = s[(u >> 4) * 16 + (u & 15)];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int p = 0; p < TPER; ++p) {
-        const int u = threadIdx.x + p * kFftThreads;
-        if (TITEMS % kFftThreads == 0 || u < TITEMS) s[(u & 15) * RS + (u >> 4)] = t[p];
-    }
-    __syncthreads();
+    fft::lines16_rows<H, kFftThreads, 2, true, RS>(s, tw);
     for (int u = threadIdx.x; u < 16 * (H / 2); u += kFftThreads) {
         const int l = u / (H / 2), mp = u % (H / 2);
         const size_t row = ((size_t)(bz * 4 + (l >> 2)) * G + by * 4 + (l & 3)) * G;
