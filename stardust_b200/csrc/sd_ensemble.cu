@@ -77,11 +77,12 @@ struct HostCounters {
     int step_count;
     bool lf_open;
     float lf_dt_prev;
-    bool mean_pending, keys_valid, rho_valid;
+    bool mean_pending, keys_valid, counts_valid, rho_valid;
 };
 
 HostCounters save_counters(const sd_sim* s) {
-    return {s->sim_time, s->step_count, s->lf_open, s->lf_dt_prev, s->mean_pending, s->keys_valid, s->rho_valid};
+    return {s->sim_time,  s->step_count,   s->lf_open,     s->lf_dt_prev,
+            s->mean_pending, s->keys_valid, s->counts_valid, s->rho_valid};
 }
 
 void restore_counters(sd_sim* s, const HostCounters& c) {
@@ -91,11 +92,12 @@ void restore_counters(sd_sim* s, const HostCounters& c) {
     s->lf_dt_prev = c.lf_dt_prev;
     s->mean_pending = c.mean_pending;
     s->keys_valid = c.keys_valid;
+    s->counts_valid = c.counts_valid;
     s->rho_valid = c.rho_valid;
 }
 
 // Everything a step needs that must not be inside the graph: leapfrog opening
-// kicks and keys of unsorted buffers.
+// kicks, and keys and first-pass sort counts of unsorted buffers.
 int prepare_scenes(sd_ensemble* e, float dt) {
     for (auto& sl : e->scenes) {
         sd_sim* s = sl.sim;
@@ -104,10 +106,8 @@ int prepare_scenes(sd_ensemble* e, float dt) {
         if (s->cfg.integrator == SD_INT_KDK && !s->lf_open) {
             if (int rc = do_step(s, dt, sort_due(s), false)) return rc;
         }
-        if (s->cfg.sort_interval == 1 && !s->keys_valid) {
-            if (int rc = launch_cell_keys(s->pos, s->N, s->G, s->cfg.order, s->keys, s->stream))
-                return sim_error(s, rc);
-            s->keys_valid = true;
+        if (s->cfg.sort_interval == 1) {
+            if (int rc = ensure_sort_inputs(s)) return sim_error(s, rc);
         }
     }
     return SD_OK;
@@ -194,6 +194,7 @@ void after_replay(sd_ensemble* e, float dt, int par) {
         ++s->step_count;
         s->mean_pending = true;
         s->keys_valid = s->cfg.sort_interval == 1;
+        s->counts_valid = s->cfg.sort_interval == 1;
         s->rho_valid = s->rho && (s->cfg.keep_density || s->mlp_on);
         s->ev_valid = false;
         if (s->cfg.integrator == SD_INT_KDK) {
@@ -234,6 +235,7 @@ int restore_snapshot(sd_sim* s, const Snapshot& sn) {
         return SD_E_CUDA;
     restore_counters(s, sn.c);
     s->keys_valid = false;  // keys of the restored order are recomputed
+    s->counts_valid = false;
     s->rho_valid = false;
     return SD_OK;
 }

@@ -26,7 +26,14 @@ int launch_cell_keys(const float4* pos, int n, int G, int order, uint32_t* keys,
 size_t sort_workspace_bytes(int n);
 int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t* keys_out, int32_t* vals_out,
                       uint32_t* keys_tmp, int32_t* vals_tmp, int n, int key_bits, void* ws, size_t ws_bytes,
-                      cudaStream_t s);
+                      cudaStream_t s, bool ws_zeroed = false, bool first_counts_ready = false);
+// ws_zeroed: the workspace's count buffers are zero, as every sort leaves them.
+// first_counts_ready: the first digit pass's tile counts are already in the
+// workspace (launch_sort_first_counts, or added by the gather that wrote the keys).
+constexpr int kSortTileShift = 11;  // sort tiles of 2048 keys
+int sort_digit_bits(int key_bits);  // digit width of the passes (0: no pass)
+unsigned* sort_first_counts(void* ws);  // tile-major counts[tile][1 << digit bits] of the first pass
+int launch_sort_first_counts(const uint32_t* keys, int n, int key_bits, void* ws, size_t ws_bytes, cudaStream_t s);
 int launch_reorder(const float4* pos_in, const float4* vel_in, const int32_t* perm, float4* pos_out,
                    float4* vel_out, int n, cudaStream_t s);
 
@@ -96,7 +103,10 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
                              const int* perm, float4* pos_out, float4* vel_out, uint32_t* keys_out, int order, int n,
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
                              double* mom_out, float* mean_out, cudaStream_t s, const float4* extra = nullptr,
-                             int max_blocks = 0, const DiagRecord* diag = nullptr, int iso_S = 0);
+                             int max_blocks = 0, const DiagRecord* diag = nullptr, int iso_S = 0,
+                             unsigned* tile_counts = nullptr, int count_bits = 0);
+// tile_counts: zeroed first-pass sort counts; the gather adds the digit (low
+// count_bits bits) of every key it writes to the row of the key's sort tile.
 // iso_S > 0: isolated boundary, potential box of side iso_S (= 2G), clamped sampling
 int launch_interpolate_accel(const float* phi, int G, float pot_scale, const float4* pos, float4* acc, int n,
                              cudaStream_t s, const float4* extra = nullptr, int iso_S = 0);

@@ -218,79 +218,94 @@ __global__ void __launch_bounds__(kGatherThreads, 3) k_gather_kick_drift(
     const float* __restrict__ phi, int G, float h, const float4* pos_in, const float4* vel_in,
     const int* __restrict__ perm, float4* pos_out, float4* vel_out, uint32_t* __restrict__ keys_out, int order, int n,
     float dt_kick, float dt_drift, float c2, const float* __restrict__ mean_vel, double* __restrict__ partials,
-    const float4* __restrict__ extra, int S) {
+    const float4* __restrict__ extra, int S, unsigned* __restrict__ tile_counts, int count_bits) {
     double sx = 0.0, sy = 0.0, sz = 0.0, cnt = 0.0, sv2 = 0.0, sphi = 0.0;
+    const unsigned cmask = (1u << count_bits) - 1u;
     const float mx = mean_vel ? mean_vel[0] : 0.f, my = mean_vel ? mean_vel[1] : 0.f,
                 mz = mean_vel ? mean_vel[2] : 0.f;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int j = perm ? perm[i] : i;
-        float4 p = pos_in[j];
-        float4 v = vel_in[j];
-        if (p.x < 0.f) {
-            if (perm) {
-                pos_out[i] = p;
-                vel_out[i] = v;
+        uint32_t key = 0u;  // the order key written for output i (0: empty or lost)
+        do {
+            const int j = perm ? perm[i] : i;
+            float4 p = pos_in[j];
+            float4 v = vel_in[j];
+            if (p.x < 0.f) {
+                if (perm) {
+                    pos_out[i] = p;
+                    vel_out[i] = v;
+                }
+                if (keys_out) keys_out[i] = 0u;
+                break;
             }
-            if (keys_out) keys_out[i] = 0u;
-            continue;
-        }
-        if (mean_vel) {
-            v.x = __fsub_rn(v.x, mx);
-            v.y = __fsub_rn(v.y, my);
-            v.z = __fsub_rn(v.z, mz);
-        }
-        float phi_p = 0.f;
-        float3 a = accel_at<ISO>(phi, G, S, h, p, DIAG ? &phi_p : nullptr);
-        if (extra) {  // learned correction, indexed like the outputs
-            const float4 e = extra[i];
-            a.x = __fadd_rn(a.x, e.x);
-            a.y = __fadd_rn(a.y, e.y);
-            a.z = __fadd_rn(a.z, e.z);
-        }
-        v.x = __fmaf_rn(a.x, dt_kick, v.x);
-        v.y = __fmaf_rn(a.y, dt_kick, v.y);
-        v.z = __fmaf_rn(a.z, dt_kick, v.z);
-        {  // light-speed clamp (Sim.cu:834-840)
-            const float sp2 = __fmaf_rn(v.z, v.z, __fmaf_rn(v.y, v.y, __fmul_rn(v.x, v.x)));
-            if (sp2 > c2) {
-                const float k = sqrtf(__fdiv_rn(c2, sp2));
-                v.x = __fmul_rn(v.x, k);
-                v.y = __fmul_rn(v.y, k);
-                v.z = __fmul_rn(v.z, k);
+            if (mean_vel) {
+                v.x = __fsub_rn(v.x, mx);
+                v.y = __fsub_rn(v.y, my);
+                v.z = __fsub_rn(v.z, mz);
             }
-        }
-        p.x = __fmaf_rn(v.x, dt_drift, p.x);
-        p.y = __fmaf_rn(v.y, dt_drift, p.y);
-        p.z = __fmaf_rn(v.z, dt_drift, p.z);
-        if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z) || !isfinite(v.x) || !isfinite(v.y) ||
-            !isfinite(v.z)) {
-            pos_out[i] = make_float4(-1.f, -1.f, -1.f, 0.f);
-            vel_out[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (keys_out) keys_out[i] = 0u;
-            continue;
-        }
-        if (ISO) {
-            if (p.x < 0.002f) { p.x = 0.002f; v.x = __fmul_rn(fabsf(v.x), 0.25f); }
-            if (p.x > 0.998f) { p.x = 0.998f; v.x = -__fmul_rn(fabsf(v.x), 0.25f); }
-            if (p.y < 0.002f) { p.y = 0.002f; v.y = __fmul_rn(fabsf(v.y), 0.25f); }
-            if (p.y > 0.998f) { p.y = 0.998f; v.y = -__fmul_rn(fabsf(v.y), 0.25f); }
-            if (p.z < 0.002f) { p.z = 0.002f; v.z = __fmul_rn(fabsf(v.z), 0.25f); }
-            if (p.z > 0.998f) { p.z = 0.998f; v.z = -__fmul_rn(fabsf(v.z), 0.25f); }
-        } else {
-            p.x = __fsub_rn(p.x, floorf(p.x));
-            p.y = __fsub_rn(p.y, floorf(p.y));
-            p.z = __fsub_rn(p.z, floorf(p.z));
-        }
-        pos_out[i] = p;
-        vel_out[i] = v;
-        if (keys_out) keys_out[i] = order_key(p, G, order);
-        sx += v.x;
-        sy += v.y;
-        sz += v.z;
-        cnt += 1.0;
-        if (DIAG) {
-            sv2 += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z;
-            sphi += (double)phi_p;
+            float phi_p = 0.f;
+            float3 a = accel_at<ISO>(phi, G, S, h, p, DIAG ? &phi_p : nullptr);
+            if (extra) {  // learned correction, indexed like the outputs
+                const float4 e = extra[i];
+                a.x = __fadd_rn(a.x, e.x);
+                a.y = __fadd_rn(a.y, e.y);
+                a.z = __fadd_rn(a.z, e.z);
+            }
+            v.x = __fmaf_rn(a.x, dt_kick, v.x);
+            v.y = __fmaf_rn(a.y, dt_kick, v.y);
+            v.z = __fmaf_rn(a.z, dt_kick, v.z);
+            {  // light-speed clamp (Sim.cu:834-840)
+                const float sp2 = __fmaf_rn(v.z, v.z, __fmaf_rn(v.y, v.y, __fmul_rn(v.x, v.x)));
+                if (sp2 > c2) {
+                    const float k = sqrtf(__fdiv_rn(c2, sp2));
+                    v.x = __fmul_rn(v.x, k);
+                    v.y = __fmul_rn(v.y, k);
+                    v.z = __fmul_rn(v.z, k);
+                }
+            }
+            p.x = __fmaf_rn(v.x, dt_drift, p.x);
+            p.y = __fmaf_rn(v.y, dt_drift, p.y);
+            p.z = __fmaf_rn(v.z, dt_drift, p.z);
+            if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z) || !isfinite(v.x) || !isfinite(v.y) ||
+                !isfinite(v.z)) {
+                pos_out[i] = make_float4(-1.f, -1.f, -1.f, 0.f);
+                vel_out[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (keys_out) keys_out[i] = 0u;
+                break;
+            }
+            if (ISO) {
+                if (p.x < 0.002f) { p.x = 0.002f; v.x = __fmul_rn(fabsf(v.x), 0.25f); }
+                if (p.x > 0.998f) { p.x = 0.998f; v.x = -__fmul_rn(fabsf(v.x), 0.25f); }
+                if (p.y < 0.002f) { p.y = 0.002f; v.y = __fmul_rn(fabsf(v.y), 0.25f); }
+                if (p.y > 0.998f) { p.y = 0.998f; v.y = -__fmul_rn(fabsf(v.y), 0.25f); }
+                if (p.z < 0.002f) { p.z = 0.002f; v.z = __fmul_rn(fabsf(v.z), 0.25f); }
+                if (p.z > 0.998f) { p.z = 0.998f; v.z = -__fmul_rn(fabsf(v.z), 0.25f); }
+            } else {
+                p.x = __fsub_rn(p.x, floorf(p.x));
+                p.y = __fsub_rn(p.y, floorf(p.y));
+                p.z = __fsub_rn(p.z, floorf(p.z));
+            }
+            pos_out[i] = p;
+            vel_out[i] = v;
+            if (keys_out) {
+                key = order_key(p, G, order);
+                keys_out[i] = key;
+            }
+            sx += v.x;
+            sy += v.y;
+            sz += v.z;
+            cnt += 1.0;
+            if (DIAG) {
+                sv2 += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z;
+                sphi += (double)phi_p;
+            }
+        } while (0);
+        // First sort pass's digit counts of the keys just written: the lanes that
+        // share (sort tile, digit) add once. A warp's outputs are consecutive, so
+        // they fall in one tile and, the particles being sorted, carry few digits.
+        if (tile_counts) {
+            const unsigned pair = (((unsigned)i >> kSortTileShift) << count_bits) | (key & cmask);
+            const unsigned peers = __match_any_sync(__activemask(), pair);
+            if ((peers & lanemask_lt()) == 0u) atomicAdd(tile_counts + pair, (unsigned)__popc(peers));
         }
     }
     if (partials) {
@@ -579,7 +594,8 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
                              const int* perm, float4* pos_out, float4* vel_out, uint32_t* keys_out, int order, int n,
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
                              double* mom_out, float* mean_out, cudaStream_t s, const float4* extra,
-                             int max_blocks, const DiagRecord* diag, int iso_S) {
+                             int max_blocks, const DiagRecord* diag, int iso_S, unsigned* tile_counts,
+                             int count_bits) {
     if (n <= 0) return SD_OK;
     const float h = (0.5f * (float)G) * pot_scale;  // Sim.cu:604
     int blocks = (int)gather_partials(n);
@@ -589,7 +605,7 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
 #define SD_GATHER(D, I)                                                                                            \
     k_gather_kick_drift<D, I><<<blocks, kGatherThreads, 0, s>>>(phi, G, h, pos_in, vel_in, perm, pos_out, vel_out, \
                                                                 keys_out, order, n, dt_kick, dt_drift, c2, mean_vel,  \
-                                                                partials, extra, iso_S)
+                                                                partials, extra, iso_S, tile_counts, count_bits)
     if (iso_S) {
         if (dg) SD_GATHER(true, true);
         else SD_GATHER(false, true);

@@ -202,6 +202,8 @@ int allocate(sd_sim* s) {
         cudaGetLastError();
         rc = fail(SD_E_NOMEM, "cudaMalloc of sort workspace failed");
     }
+    // the sort's count buffers start zero and every sort leaves them zero
+    if (!rc && SD_CUDA(cudaMemset(s->sort_ws, 0, s->sort_ws_bytes))) rc = SD_E_CUDA;
     rc = rc ? rc : alloc_dev(s->acc, cells);
     rc = rc ? rc : alloc_dev(s->row_start, (size_t)s->G * s->G + 1);
     rc = rc ? rc : alloc_dev(s->spec, poisson_spectrum_elems(S));
@@ -286,12 +288,30 @@ int mlp_correction(sd_sim* s, const int32_t* perm) {
                             s->stream);
 }
 
+// Keys and first-pass sort counts for the current order, where the last step's
+// gather has not left them.
+int ensure_sort_inputs(sd_sim* s) {
+    int rc = SD_OK;
+    if (!s->keys_valid) {
+        if ((rc = launch_cell_keys(s->pos, s->N, s->G, s->cfg.order, s->keys, s->stream))) return rc;
+        s->keys_valid = true;
+        s->counts_valid = false;
+    }
+    if (!s->counts_valid) {
+        if ((rc = launch_sort_first_counts(s->keys, s->N, key_bits_for(s->G, s->cfg.order), s->sort_ws,
+                                           s->sort_ws_bytes, s->stream)))
+            return rc;
+        s->counts_valid = true;
+    }
+    return SD_OK;
+}
+
 // Sort + reorder (sortParticles, Sim.cu:3656-3671).
 int do_sort(sd_sim* s, int32_t* perm_out_dev) {
     int rc = launch_cell_keys(s->pos, s->N, s->G, s->cfg.order, s->keys, s->stream);
     if (rc) return rc;
     rc = launch_sort_pairs(s->keys, nullptr, s->keys2, s->vals, s->keys3, s->vals2, s->N,
-                           key_bits_for(s->G, s->cfg.order), s->sort_ws, s->sort_ws_bytes, s->stream);
+                           key_bits_for(s->G, s->cfg.order), s->sort_ws, s->sort_ws_bytes, s->stream, true);
     if (rc) return rc;
     rc = launch_reorder(s->pos, s->vel, s->vals, s->pos2, s->vel2, s->N, s->stream);
     if (rc) return rc;
@@ -301,6 +321,7 @@ int do_sort(sd_sim* s, int32_t* perm_out_dev) {
     std::swap(s->pos, s->pos2);
     std::swap(s->vel, s->vel2);
     s->keys_valid = false;
+    s->counts_valid = false;
     return SD_OK;
 }
 
@@ -333,11 +354,11 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     // separate reorder pass runs.
     const int32_t* perm = nullptr;
     if (sort) {
-        if (!s->keys_valid && (rc = launch_cell_keys(s->pos, s->N, s->G, s->cfg.order, s->keys, s->stream)))
-            return sim_error(s, rc);
+        if ((rc = ensure_sort_inputs(s))) return sim_error(s, rc);
         rc = launch_sort_pairs(s->keys, nullptr, s->keys2, s->vals, s->keys3, s->vals2, s->N,
-                               key_bits_for(s->G, s->cfg.order), s->sort_ws, s->sort_ws_bytes, s->stream);
+                               key_bits_for(s->G, s->cfg.order), s->sort_ws, s->sort_ws_bytes, s->stream, true, true);
         if (rc) return sim_error(s, rc);
+        s->counts_valid = false;  // the sort consumed and cleared them
         perm = s->vals;
     }
     if (timed) cudaEventRecord(s->ev[1], s->stream);
@@ -375,13 +396,17 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     rc = launch_gather_kick_drift(s->phi, s->G, pot_scale_of(s), s->pos, s->vel, perm, pos_out, vel_out, s->keys,
                                   s->cfg.order, s->N, dt_kick, dt_drift, c2, s->mean, s->partials, s->mom, s->mean,
                                   s->stream, s->mlp_on ? s->mlp_out : nullptr, s->gather_blocks,
-                                  s->cfg.diagnostics ? &diag : nullptr, isolated(s) ? 2 * s->G : 0);
+                                  s->cfg.diagnostics ? &diag : nullptr, isolated(s) ? 2 * s->G : 0,
+                                  sort ? sort_first_counts(s->sort_ws) : nullptr,
+                                  sort_digit_bits(key_bits_for(s->G, s->cfg.order)));
     if (rc) return sim_error(s, rc);
     if (perm) {
         std::swap(s->pos, s->pos2);
         std::swap(s->vel, s->vel2);
     }
     s->keys_valid = true;
+    // after a sort the counts buffer was zero, and the gather counted the new keys
+    s->counts_valid = sort;
     s->mean_pending = true;
     if (timed) cudaEventRecord(s->ev[4], s->stream);
     s->ev_valid = timed;
@@ -764,11 +789,11 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
     }
     if (done >= nsteps) return SD_OK;
     const bool sort = s->cfg.sort_interval == 1;
-    // Keys are computed outside the graph, so replays never depend on them being stale.
-    if (sort && !s->keys_valid) {
-        int rc = launch_cell_keys(s->pos, s->N, s->G, s->cfg.order, s->keys, s->stream);
+    // Keys and first-pass counts are made outside the graph, so replays never
+    // depend on them being stale.
+    if (sort) {
+        int rc = ensure_sort_inputs(s);
         if (rc) return sim_error(s, rc);
-        s->keys_valid = true;
     }
     // A captured graph covers two steps so the pos/pos2 ping-pong returns to the
     // same buffers; it is rebuilt when dt changes or the particles sit in the
@@ -784,6 +809,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
         const float lfd = s->lf_dt_prev;
         const bool mp0 = s->mean_pending;
         const bool kv0 = s->keys_valid;
+        const bool cv0 = s->counts_valid;
         const long long l0 = launches();
         int rc = do_step(s, dt, sort, false);
         if (!rc) rc = do_step(s, dt, sort, false);
@@ -798,6 +824,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
         s->lf_dt_prev = lfd;
         s->mean_pending = mp0;
         s->keys_valid = kv0;
+        s->counts_valid = cv0;
         if (rc) {
             if (graph) cudaGraphDestroy(graph);
             return rc;
@@ -816,6 +843,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
         s->step_count += 2;
         s->mean_pending = true;
         s->keys_valid = true;
+        s->counts_valid = sort;
         if (s->cfg.integrator == SD_INT_KDK) {
             s->lf_open = true;
             s->lf_dt_prev = dt;
@@ -843,6 +871,7 @@ int sd_synchronize(sd_sim* s) {
                                   s->mean, s->stream, s->mlp_on ? s->mlp_out : nullptr, 0, nullptr,
                                   isolated(s) ? 2 * s->G : 0);
     if (rc) return sim_error(s, rc);
+    s->counts_valid = false;  // keys were rewritten (a lost particle changes its key)
     s->mean_pending = true;
     s->lf_open = false;
     return SD_OK;

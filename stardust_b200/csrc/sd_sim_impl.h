@@ -38,6 +38,7 @@ struct sd_sim {
     bool mean_pending = false;
     bool rho_valid = false;
     bool keys_valid = false;     // keys hold the order keys of the current pos order
+    bool counts_valid = false;   // the sort workspace holds the first-pass tile counts of keys
     sd::PoissonPlan plan;
 
     // leapfrog
@@ -84,6 +85,7 @@ struct DeviceGuard {
 
 int sim_error(sd_sim* s, int rc);
 bool sort_due(const sd_sim* s);
+int ensure_sort_inputs(sd_sim* s);
 int key_bits_for(int G, int order);
 // One step of one scene on s->stream (no host synchronisation; capturable).
 int do_step(sd_sim* s, float dt, bool sort, bool timed);

@@ -5,9 +5,12 @@
 //
 // The sort is a classic stable LSD radix sort with 8- to 10-bit digits (the key
 // width is split into the fewest passes of at most 10 bits), written for
-// sm_100a, in three kernels per digit pass:
-//   1. k_digit_counts: each 2048-key tile counts its digits in shared memory and
-//      writes them as one coalesced row (count[t][d]);
+// sm_100a, in three steps per digit pass:
+//   1. digit counts per 2048-key tile, count[t][d]: for the first pass
+//      k_digit_counts counts each tile in shared memory and writes one coalesced
+//      row; every later pass gets its counts from the scatter before it, which
+//      knows where each key lands and adds one count per (tile, digit) run of a
+//      warp into a zeroed buffer, so the keys are not read an extra time;
 //   2. a column scan over tiles (chunk sums, a per-digit scan of the chunk sums
 //      plus the digit bases, a rescan of each chunk) turns the rows into, for
 //      every (tile, digit), the global output offset: all keys of smaller digits
@@ -15,7 +18,8 @@
 //      result stable across tiles;
 //   3. k_digit_scatter: each tile ranks its keys stably (per warp, in input order,
 //      with __match_any_sync on the digit), stages them digit-sorted in shared
-//      memory and writes each digit run contiguously.
+//      memory and writes each digit run contiguously; it then clears its row of
+//      the offsets, so both count buffers are zero again when the sort ends.
 // No kernel waits on another block, so nothing can spin. Keys are key+1 as
 // uint32, so the empty slot (reference key -1) sorts first, as CUB does with the
 // reference's signed keys.
@@ -34,6 +38,7 @@ namespace {
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per tile
+static_assert(kSortTile == 1 << kSortTileShift, "sort tile size");
 constexpr int kMaxRadixBits = 10;
 constexpr int kWarps = kSortThreads / 32;
 
@@ -108,7 +113,8 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* 
                                                                 const int32_t* __restrict__ vals_in,
                                                                 uint32_t* __restrict__ keys_out,
                                                                 int32_t* __restrict__ vals_out, int n, int shift,
-                                                                const unsigned* __restrict__ offsets, int tiles) {
+                                                                unsigned* __restrict__ offsets,
+                                                                unsigned* __restrict__ next_counts, int next_shift) {
     constexpr int kRadix = 1 << BITS;
     constexpr unsigned mask = kRadix - 1;
     constexpr int DPT = (kRadix + kSortThreads - 1) / kSortThreads;  // digits per thread
@@ -192,6 +198,8 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* 
         }
     }
     __syncthreads();
+    // this tile's row of offsets is consumed: clear it for the next sort
+    for (int d = threadIdx.x; d < kRadix; d += kSortThreads) offsets[(size_t)blockIdx.x * kRadix + d] = 0u;
 
 #pragma unroll
     for (int it = 0; it < kSortItems; ++it) {
@@ -205,13 +213,27 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* 
     }
     __syncthreads();
 
+    // Digit runs go out contiguously. With next_counts, the next pass's digit of
+    // each key is counted for the tile its output position falls in: lanes that
+    // share (output tile, next digit) add once, by their lowest lane.
     const int count = min(kSortTile, n - tile0);
-    for (int i = threadIdx.x; i < count; i += kSortThreads) {
-        const uint32_t key = skeys[i];
-        const unsigned d = (key >> shift) & mask;
-        const unsigned dst = dst_base[d] + (unsigned)i;
-        keys_out[dst] = key;
-        vals_out[dst] = svals[i];
+#pragma unroll
+    for (int it = 0; it < kSortItems; ++it) {
+        const int i = it * kSortThreads + threadIdx.x;
+        unsigned pair = 0xffffffffu;  // (output tile << BITS | next digit); never all ones
+        if (i < count) {
+            const uint32_t key = skeys[i];
+            const unsigned d = (key >> shift) & mask;
+            const unsigned dst = dst_base[d] + (unsigned)i;
+            keys_out[dst] = key;
+            vals_out[dst] = svals[i];
+            pair = ((dst / (unsigned)kSortTile) << BITS) | ((key >> next_shift) & mask);
+        }
+        if (next_counts) {
+            const unsigned peers = __match_any_sync(0xffffffffu, pair);
+            if (pair != 0xffffffffu && (peers & lt) == 0u)
+                atomicAdd(next_counts + (size_t)(pair >> BITS) * kRadix + (pair & mask), (unsigned)__popc(peers));
+        }
     }
 }
 
@@ -388,11 +410,16 @@ int launch_cell_keys(const float4* pos, int n, int G, int order, uint32_t* keys,
 
 static int col_chunks(int tiles) { return (tiles + kColChunk - 1) / kColChunk; }
 
+// Two count buffers of tiles x radix (the pass being scattered and the next
+// pass's counts), then the column-scan sums.
+static size_t counts_bytes(int tiles) {
+    return align_up(((size_t)1 << kMaxRadixBits) * tiles * sizeof(unsigned), 256);
+}
+
 size_t sort_workspace_bytes(int n) {
     const int tiles = std::max(1, (n + kSortTile - 1) / kSortTile);
     const size_t radix = (size_t)1 << kMaxRadixBits;
-    return align_up(radix * tiles * sizeof(unsigned), 256) +
-           align_up(radix * (col_chunks(tiles) + 1) * sizeof(unsigned), 256);
+    return 2 * counts_bytes(tiles) + align_up(radix * (col_chunks(tiles) + 1) * sizeof(unsigned), 256);
 }
 
 // counts[tiles][radix] (tile-major) -> exclusive global offsets, in place;
@@ -412,9 +439,34 @@ static int scan_offsets(unsigned* counts, int tiles, int radix, unsigned* S, cud
     return SD_OK;
 }
 
+int sort_digit_bits(int key_bits) {
+    // fewest passes of at most kMaxRadixBits bits, then the even digit width (8, 9 or 10)
+    const int passes = (key_bits + kMaxRadixBits - 1) / kMaxRadixBits;
+    if (passes <= 0) return 0;
+    const int even = (key_bits + passes - 1) / passes;
+    return even <= 8 ? 8 : even;
+}
+
+unsigned* sort_first_counts(void* ws) { return (unsigned*)ws; }
+
+int launch_sort_first_counts(const uint32_t* keys, int n, int key_bits, void* ws, size_t ws_bytes, cudaStream_t s) {
+    const int bits = sort_digit_bits(key_bits);
+    if (n <= 0 || bits == 0) return SD_OK;
+    if (!keys || !ws || ws_bytes < sort_workspace_bytes(n)) return fail(SD_E_ARG, "sort counts: bad workspace");
+    const int tiles = (n + kSortTile - 1) / kSortTile;
+    unsigned* counts = sort_first_counts(ws);
+    switch (bits) {
+        case 8: k_digit_counts<8><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, counts, tiles); break;
+        case 9: k_digit_counts<9><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, counts, tiles); break;
+        default: k_digit_counts<10><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, counts, tiles); break;
+    }
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
+
 int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t* keys_out, int32_t* vals_out,
                       uint32_t* keys_tmp, int32_t* vals_tmp, int n, int key_bits, void* ws, size_t ws_bytes,
-                      cudaStream_t s) {
+                      cudaStream_t s, bool ws_zeroed, bool first_counts_ready) {
     if (n < 0 || key_bits < 0 || key_bits > 32) return fail(SD_E_ARG, "sort: bad n=%d or key_bits=%d", n, key_bits);
     if (n == 0) return SD_OK;
     if (!keys_in || !keys_out || !vals_out || !keys_tmp || !vals_tmp || !ws)
@@ -429,11 +481,16 @@ int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t*
         SD_LAUNCHED(s);
         return SD_OK;
     }
-    const int even = (key_bits + passes - 1) / passes;  // <= kMaxRadixBits
-    const int bits = even <= 8 ? 8 : even;               // digit width of the kernels (8, 9 or 10)
+    const int bits = sort_digit_bits(key_bits);
     const int tiles = (n + kSortTile - 1) / kSortTile;
-    unsigned* counts = (unsigned*)ws;
-    unsigned* sums = (unsigned*)((char*)ws + align_up((size_t)(1 << kMaxRadixBits) * tiles * sizeof(unsigned), 256));
+    unsigned* cnt[2] = {(unsigned*)ws, (unsigned*)((char*)ws + counts_bytes(tiles))};
+    unsigned* sums = (unsigned*)((char*)ws + 2 * counts_bytes(tiles));
+    // The scatters add the next pass's counts into the second buffer, which must
+    // start at zero; a sort leaves both buffers zero, so a workspace that only
+    // ever serves this sort is cleared once.
+    if (passes > 1 && !ws_zeroed &&
+        SD_CUDA(cudaMemsetAsync(cnt[1], 0, sizeof(unsigned) * ((size_t)tiles << bits), s)))
+        return SD_E_CUDA;
 
     const uint32_t* kin = keys_in;
     const int32_t* vin = vals_in;
@@ -443,24 +500,32 @@ int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t*
         const bool to_out = ((passes - 1 - p) % 2) == 0;
         uint32_t* kout = to_out ? keys_out : keys_tmp;
         int32_t* vout = to_out ? vals_out : vals_tmp;
+        unsigned* counts = cnt[p & 1];
+        unsigned* next = (p + 1 < passes) ? cnt[(p + 1) & 1] : nullptr;
+        const int next_shift = (p + 1) * bits;
         // key bits above key_bits are zero, so a last digit reaching past them is exact
-        switch (bits) {
-            case 8: k_digit_counts<8><<<tiles, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles); break;
-            case 9: k_digit_counts<9><<<tiles, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles); break;
-            default: k_digit_counts<10><<<tiles, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles); break;
+        if (p == 0 && !first_counts_ready) {
+            switch (bits) {
+                case 8: k_digit_counts<8><<<tiles, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles); break;
+                case 9: k_digit_counts<9><<<tiles, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles); break;
+                default: k_digit_counts<10><<<tiles, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles); break;
+            }
+            SD_LAUNCHED(s);
         }
-        SD_LAUNCHED(s);
         int rc = scan_offsets(counts, tiles, 1 << bits, sums, s);
         if (rc != SD_OK) return rc;
         switch (bits) {
             case 8:
-                k_digit_scatter<8><<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, tiles);
+                k_digit_scatter<8><<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, next,
+                                                                   next_shift);
                 break;
             case 9:
-                k_digit_scatter<9><<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, tiles);
+                k_digit_scatter<9><<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, next,
+                                                                   next_shift);
                 break;
             default:
-                k_digit_scatter<10><<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, tiles);
+                k_digit_scatter<10><<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, next,
+                                                                    next_shift);
                 break;
         }
         SD_LAUNCHED(s);

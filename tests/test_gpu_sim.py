@@ -257,6 +257,31 @@ def test_graph_replay_across_calls_and_parity(cuda):
     assert np.array_equal(outs[0][1].view(np.int32), outs[1][1].view(np.int32))
 
 
+@pytest.mark.parametrize("order", [L.SD_ORDER_TILED, L.SD_ORDER_MORTON])
+def test_sort_counts_follow_new_particles(cuda, order):
+    """The gather leaves the next sort's first-pass digit counts behind; replacing
+    the particles between (graph-replayed) steps must not let a stale count reach
+    the sort: the run equals a fresh one stepped eagerly from the new particles."""
+    G, n = 32, 80_000
+    a = random_particles(n, 31, clustered=True)
+    b = random_particles(n, 32, empty_every=53, clustered=True)
+    with make_sim(cuda, n, G, gravity=200.0, softening_cells=1.0, order=order) as s:
+        s.set_particles(*a)
+        s.steps(1e-3, 4)
+        s.set_particles(*b)
+        s.steps(1e-3, 4)
+        s.step(1e-3)
+        s.steps(1e-3, 2)
+        got = s.get_particles()
+    with make_sim(cuda, n, G, gravity=200.0, softening_cells=1.0, order=order) as t:
+        t.set_particles(*b)
+        for _ in range(7):
+            t.step(1e-3)
+        want = t.get_particles()
+    assert np.array_equal(got[0].view(np.int32), want[0].view(np.int32))
+    assert np.array_equal(got[1].view(np.int32), want[1].view(np.int32))
+
+
 def test_per_step_diagnostics_record_energy_and_momentum(cuda):
     """diagnostics = 1: every step (eager or graph-replayed) appends an FP64 record
     whose potential is that of the step-start state and whose kinetic energy is
