@@ -30,7 +30,8 @@ int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t*
 // ws_zeroed: the workspace's count buffers are zero, as every sort leaves them.
 // first_counts_ready: the first digit pass's tile counts are already in the
 // workspace (launch_sort_first_counts, or added by the gather that wrote the keys).
-constexpr int kSortTileShift = 11;  // sort tiles of 2048 keys
+constexpr int kSortTileShift = 11;   // sort tiles of 2048 keys
+constexpr int kSortChunkShift = 6;   // the column scan sums chunks of 64 tiles
 int sort_digit_bits(int key_bits);  // digit width of the passes (0: no pass)
 unsigned* sort_first_counts(void* ws);  // tile-major counts[tile][1 << digit bits] of the first pass
 int launch_sort_first_counts(const uint32_t* keys, int n, int key_bits, void* ws, size_t ws_bytes, cudaStream_t s);

@@ -171,18 +171,21 @@ __global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4
     __shared__ int range_lo[25], range_off[26];
     const int by = blockIdx.x, bz = blockIdx.y;
     const int m = G - 1;
+    // The row table is the head of this CTA's chain of dependent loads (row
+    // starts -> permutation -> positions): warp 0 issues it before the twiddle
+    // loads and the clearing of the sums, which then overlap its latency.
+    const int j = threadIdx.x;
+    int lo = 0, len = 0;
+    if (j < 25) {
+        // source rows (iy, iz) = (4by - 1 + j % 5, 4bz - 1 + j / 5)
+        const int iy = (4 * by - 1 + j % 5) & m, iz = (4 * bz - 1 + j / 5) & m;
+        const int key = ((iz >> 2) * (G / 4) + (iy >> 2)) * 16 + (iz & 3) * 4 + (iy & 3);
+        lo = row_start[key];
+        len = row_start[key + 1] - lo;
+    }
     for (int i = threadIdx.x; i < G; i += NT) tw[i] = tw_g[i];
     for (int i = threadIdx.x; i < 8 * RS; i += NT) reinterpret_cast<uint4*>(acc_lo)[i] = make_uint4(0u, 0u, 0u, 0u);
     if (threadIdx.x < 32) {
-        // source rows (iy, iz) = (4by - 1 + j % 5, 4bz - 1 + j / 5), j < 25
-        const int j = threadIdx.x;
-        int lo = 0, len = 0;
-        if (j < 25) {
-            const int iy = (4 * by - 1 + j % 5) & m, iz = (4 * bz - 1 + j / 5) & m;
-            const int key = ((iz >> 2) * (G / 4) + (iy >> 2)) * 16 + (iz & 3) * 4 + (iy & 3);
-            lo = row_start[key];
-            len = row_start[key + 1] - lo;
-        }
         int inc = len;  // inclusive scan of the lengths across the warp
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -198,21 +201,33 @@ __global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4
     __syncthreads();
     const int total = range_off[25];
     const bool split16 = total < 65536;
-    int r = 0;
-    // Loads are issued kBatch at a time so several particles are in flight per
-    // thread before the shared-memory adds.
+    // Up to kBatch particles per thread and round: their slots are located first
+    // (binary search of the row offsets), then all permutation loads and then all
+    // position loads are issued before any result is used.
     constexpr int kBatch = 4;
     for (int f0 = threadIdx.x; f0 < total; f0 += kBatch * NT) {
-        float4 pb[kBatch];
+        int src[kBatch];
 #pragma unroll
         for (int b = 0; b < kBatch; ++b) {
             const int f = f0 + b * NT;
+            src[b] = -1;
             if (f < total) {
-                while (f >= range_off[r + 1]) ++r;
-                const int idx = range_lo[r] + (f - range_off[r]);
-                pb[b] = pos[perm ? perm[idx] : idx];
+                int r = 0;  // largest r < 25 with range_off[r] <= f
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1)
+                    if (r + step < 25 && range_off[r + step] <= f) r += step;
+                src[b] = range_lo[r] + (f - range_off[r]);
             }
         }
+        if (perm) {
+#pragma unroll
+            for (int b = 0; b < kBatch; ++b)
+                if (src[b] >= 0) src[b] = perm[src[b]];
+        }
+        float4 pb[kBatch];
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b)
+            if (src[b] >= 0) pb[b] = pos[src[b]];
 #pragma unroll
         for (int b = 0; b < kBatch; ++b) {
             if (f0 + b * NT >= total) break;

@@ -15,7 +15,8 @@
 //      plus the digit bases, a rescan of each chunk) turns the rows into, for
 //      every (tile, digit), the global output offset: all keys of smaller digits
 //      plus the same digit's keys in earlier tiles, which is what makes the
-//      result stable across tiles;
+//      result stable across tiles. Counts added by a scatter bring their chunk
+//      sums with them; the first pass's counts have their chunks summed;
 //   3. k_digit_scatter: each tile ranks its keys stably (per warp, in input order,
 //      with __match_any_sync on the digit), stages them digit-sorted in shared
 //      memory and writes each digit run contiguously; it then clears its row of
@@ -41,6 +42,9 @@ constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per tile
 static_assert(kSortTile == 1 << kSortTileShift, "sort tile size");
 constexpr int kMaxRadixBits = 10;
 constexpr int kWarps = kSortThreads / 32;
+constexpr int kColChunk = 1 << kSortChunkShift;  // tiles per column-scan chunk
+constexpr int kColThreads = 256;
+constexpr int kColSegs = kColThreads / 32;  // 8 segments of a column per CTA
 
 __global__ void __launch_bounds__(256) k_cell_keys(const float4* __restrict__ pos, int n, int G, int order,
                                                    uint32_t* __restrict__ keys) {
@@ -114,7 +118,8 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* 
                                                                 uint32_t* __restrict__ keys_out,
                                                                 int32_t* __restrict__ vals_out, int n, int shift,
                                                                 unsigned* __restrict__ offsets,
-                                                                unsigned* __restrict__ next_counts, int next_shift) {
+                                                                unsigned* __restrict__ next_counts,
+                                                                unsigned* __restrict__ next_sums, int next_shift) {
     constexpr int kRadix = 1 << BITS;
     constexpr unsigned mask = kRadix - 1;
     constexpr int DPT = (kRadix + kSortThreads - 1) / kSortThreads;  // digits per thread
@@ -231,8 +236,11 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* 
         }
         if (next_counts) {
             const unsigned peers = __match_any_sync(0xffffffffu, pair);
-            if (pair != 0xffffffffu && (peers & lt) == 0u)
-                atomicAdd(next_counts + (size_t)(pair >> BITS) * kRadix + (pair & mask), (unsigned)__popc(peers));
+            if (pair != 0xffffffffu && (peers & lt) == 0u) {
+                const unsigned c = (unsigned)__popc(peers), t = pair >> BITS, d = pair & mask;
+                atomicAdd(next_counts + (size_t)t * kRadix + d, c);
+                atomicAdd(next_sums + (size_t)(t >> kSortChunkShift) * kRadix + d, c);
+            }
         }
     }
 }
@@ -241,13 +249,11 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* 
 //   offset(t, d) = base(d) + sum_{t' < t} counts[t'][d],  base(d) = sum_{d' < d} total(d'),
 // over chunks of kColChunk tiles and slabs of 32 digits, so every global access
 // is a coalesced 128-byte row piece and every chain of dependent adds is short:
-//   k_col_sums   S[c][d] = chunk sums
-//   k_col_prefix S[c][d] -> exclusive prefix over chunks, T[d] = digit totals
-//   k_col_bases  T[d] -> base(d) (one CTA)
-//   k_col_apply  counts[t][d] -> base(d) + S[c][d] + prefix within the chunk
-constexpr int kColChunk = 64;
-constexpr int kColThreads = 256;
-constexpr int kColSegs = kColThreads / 32;  // 8 segments of a column per CTA
+//   k_col_sums   S[c][d] = chunk sums (first pass only)
+//   k_col_prefix S[c][d] -> exclusive prefix over chunks, T[d] = digit totals;
+//                the last CTA to finish turns T into the digit bases base(d)
+//   k_col_apply  counts[t][d] -> base(d) + S[c][d] + prefix within the chunk,
+//                and clears S, ready for the adds of the next counts
 
 __global__ void __launch_bounds__(kColThreads) k_col_sums(const unsigned* __restrict__ counts, int tiles, int radix,
                                                           unsigned* __restrict__ S) {
@@ -263,8 +269,10 @@ __global__ void __launch_bounds__(kColThreads) k_col_sums(const unsigned* __rest
 // CTA per 32-digit slab: thread (seg, lane) owns digit slab*32 + lane and a
 // contiguous run of chunks; two sweeps (sum, rewrite) around a scan of the runs.
 __global__ void __launch_bounds__(kColThreads) k_col_prefix(unsigned* __restrict__ S, int chunks, int radix,
-                                                            unsigned* __restrict__ T) {
+                                                            unsigned* __restrict__ T, unsigned* __restrict__ done) {
     __shared__ unsigned seg_sum[kColSegs][32];
+    __shared__ unsigned scan_tmp[33];
+    __shared__ bool last;
     const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
     const int d = blockIdx.x * 32 + lane;
     const int per = (chunks + kColSegs - 1) / kColSegs;
@@ -295,20 +303,36 @@ __global__ void __launch_bounds__(kColThreads) k_col_prefix(unsigned* __restrict
         }
         if (seg == 0) T[d] = tot;
     }
-}
-
-__global__ void __launch_bounds__(1024) k_col_bases(unsigned* __restrict__ T, int radix) {
-    __shared__ unsigned tmp[33];
-    const int d = threadIdx.x;
-    const unsigned v = (d < radix) ? T[d] : 0u;
-    const unsigned base = block_exclusive(v, tmp, nullptr);
-    if (d < radix) T[d] = base;
+    // The last CTA to finish (counted on `done`, which it resets) sees every
+    // total and replaces them by their exclusive scan over the digits.
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    constexpr int kPer = (1 << kMaxRadixBits) / kColThreads;
+    unsigned v[kPer], mine = 0u;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        const int dd = threadIdx.x * kPer + j;
+        v[j] = (dd < radix) ? __ldcg(T + dd) : 0u;
+        mine += v[j];
+    }
+    unsigned ex = block_exclusive(mine, scan_tmp, nullptr);
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        const int dd = threadIdx.x * kPer + j;
+        if (dd < radix) T[dd] = ex;
+        ex += v[j];
+    }
+    if (threadIdx.x == 0) *done = 0u;
 }
 
 // CTA per (chunk, 32-digit slab): the chunk's 64 x 32 counts staged in shared
 // memory, scanned down each column in 8 segments of 8 tiles.
 __global__ void __launch_bounds__(kColThreads) k_col_apply(unsigned* __restrict__ counts, int tiles, int radix,
-                                                           const unsigned* __restrict__ S,
+                                                           unsigned* __restrict__ S,
                                                            const unsigned* __restrict__ T) {
     __shared__ unsigned tile[kColChunk][33];
     __shared__ unsigned seg_sum[kColSegs][32];
@@ -329,6 +353,8 @@ __global__ void __launch_bounds__(kColThreads) k_col_apply(unsigned* __restrict_
     __syncthreads();
     unsigned run = (d < radix) ? T[d] + S[(size_t)c * radix + d] : 0u;
     for (int j = 0; j < seg; ++j) run += seg_sum[j][lane];
+    __syncthreads();  // every segment has read S[c][d]
+    if (seg == 0 && d < radix) S[(size_t)c * radix + d] = 0u;
 #pragma unroll
     for (int j = 0; j < kRowsPerSeg; ++j) {
         const int r = seg * kRowsPerSeg + j;
@@ -410,31 +436,56 @@ int launch_cell_keys(const float4* pos, int n, int G, int order, uint32_t* keys,
 
 static int col_chunks(int tiles) { return (tiles + kColChunk - 1) / kColChunk; }
 
-// Two count buffers of tiles x radix (the pass being scattered and the next
-// pass's counts), then the column-scan sums.
+// Workspace: two count buffers of tiles x radix (the pass being scattered and
+// the next pass's counts), the chunk sums S[chunks][radix], the digit totals /
+// bases T[radix] and the column scan's finish counter.
+struct SortWs {
+    unsigned* cnt[2];
+    unsigned* S;
+    unsigned* T;
+    unsigned* done;
+};
+
 static size_t counts_bytes(int tiles) {
     return align_up(((size_t)1 << kMaxRadixBits) * tiles * sizeof(unsigned), 256);
+}
+static size_t sums_bytes(int tiles) {
+    return align_up(((size_t)1 << kMaxRadixBits) * col_chunks(tiles) * sizeof(unsigned), 256);
+}
+
+static SortWs sort_ws_layout(void* ws, int n) {
+    const int tiles = std::max(1, (n + kSortTile - 1) / kSortTile);
+    char* b = (char*)ws;
+    SortWs w;
+    w.cnt[0] = (unsigned*)b;
+    w.cnt[1] = (unsigned*)(b + counts_bytes(tiles));
+    w.S = (unsigned*)(b + 2 * counts_bytes(tiles));
+    w.T = (unsigned*)(b + 2 * counts_bytes(tiles) + sums_bytes(tiles));
+    w.done = w.T + ((size_t)1 << kMaxRadixBits);
+    return w;
 }
 
 size_t sort_workspace_bytes(int n) {
     const int tiles = std::max(1, (n + kSortTile - 1) / kSortTile);
-    const size_t radix = (size_t)1 << kMaxRadixBits;
-    return 2 * counts_bytes(tiles) + align_up(radix * (col_chunks(tiles) + 1) * sizeof(unsigned), 256);
+    return 2 * counts_bytes(tiles) + sums_bytes(tiles) +
+           align_up(((size_t)1 << kMaxRadixBits) * sizeof(unsigned) + sizeof(unsigned), 256);
 }
 
-// counts[tiles][radix] (tile-major) -> exclusive global offsets, in place;
-// S holds chunks * radix chunk prefixes followed by the radix digit bases
-static int scan_offsets(unsigned* counts, int tiles, int radix, unsigned* S, cudaStream_t s) {
+static int col_sums(const unsigned* counts, int tiles, int radix, unsigned* S, cudaStream_t s) {
+    k_col_sums<<<dim3(col_chunks(tiles), (radix + kColThreads - 1) / kColThreads), kColThreads, 0, s>>>(counts, tiles,
+                                                                                                     radix, S);
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
+
+// counts[tiles][radix] (tile-major) with their chunk sums in w.S -> exclusive
+// global offsets, in place; leaves w.S zero.
+static int scan_offsets(unsigned* counts, int tiles, int radix, const SortWs& w, cudaStream_t s) {
     const int chunks = col_chunks(tiles);
-    unsigned* T = S + (size_t)chunks * radix;
     const int slabs = (radix + 31) / 32;
-    k_col_sums<<<dim3(chunks, (radix + kColThreads - 1) / kColThreads), kColThreads, 0, s>>>(counts, tiles, radix, S);
+    k_col_prefix<<<slabs, kColThreads, 0, s>>>(w.S, chunks, radix, w.T, w.done);
     SD_LAUNCHED(s);
-    k_col_prefix<<<slabs, kColThreads, 0, s>>>(S, chunks, radix, T);
-    SD_LAUNCHED(s);
-    k_col_bases<<<1, 1024, 0, s>>>(T, radix);
-    SD_LAUNCHED(s);
-    k_col_apply<<<dim3(chunks, slabs), kColThreads, 0, s>>>(counts, tiles, radix, S, T);
+    k_col_apply<<<dim3(chunks, slabs), kColThreads, 0, s>>>(counts, tiles, radix, w.S, w.T);
     SD_LAUNCHED(s);
     return SD_OK;
 }
@@ -454,11 +505,11 @@ int launch_sort_first_counts(const uint32_t* keys, int n, int key_bits, void* ws
     if (n <= 0 || bits == 0) return SD_OK;
     if (!keys || !ws || ws_bytes < sort_workspace_bytes(n)) return fail(SD_E_ARG, "sort counts: bad workspace");
     const int tiles = (n + kSortTile - 1) / kSortTile;
-    unsigned* counts = sort_first_counts(ws);
+    const SortWs w = sort_ws_layout(ws, n);
     switch (bits) {
-        case 8: k_digit_counts<8><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, counts, tiles); break;
-        case 9: k_digit_counts<9><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, counts, tiles); break;
-        default: k_digit_counts<10><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, counts, tiles); break;
+        case 8: k_digit_counts<8><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, w.cnt[0], tiles); break;
+        case 9: k_digit_counts<9><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, w.cnt[0], tiles); break;
+        default: k_digit_counts<10><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, w.cnt[0], tiles); break;
     }
     SD_LAUNCHED(s);
     return SD_OK;
@@ -483,13 +534,13 @@ int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t*
     }
     const int bits = sort_digit_bits(key_bits);
     const int tiles = (n + kSortTile - 1) / kSortTile;
-    unsigned* cnt[2] = {(unsigned*)ws, (unsigned*)((char*)ws + counts_bytes(tiles))};
-    unsigned* sums = (unsigned*)((char*)ws + 2 * counts_bytes(tiles));
+    const SortWs w = sort_ws_layout(ws, n);
+    unsigned* const* cnt = w.cnt;
     // The scatters add the next pass's counts into the second buffer, which must
-    // start at zero; a sort leaves both buffers zero, so a workspace that only
-    // ever serves this sort is cleared once.
-    if (passes > 1 && !ws_zeroed &&
-        SD_CUDA(cudaMemsetAsync(cnt[1], 0, sizeof(unsigned) * ((size_t)tiles << bits), s)))
+    // start at zero, and the column scan counts its CTAs on w.done; a sort leaves
+    // both zero, so a workspace that only ever serves this sort is cleared once.
+    if (!ws_zeroed && (SD_CUDA(cudaMemsetAsync(cnt[1], 0, sizeof(unsigned) * ((size_t)tiles << bits), s)) ||
+                       SD_CUDA(cudaMemsetAsync(w.done, 0, sizeof(unsigned), s))))
         return SD_E_CUDA;
 
     const uint32_t* kin = keys_in;
@@ -500,6 +551,7 @@ int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t*
         const bool to_out = ((passes - 1 - p) % 2) == 0;
         uint32_t* kout = to_out ? keys_out : keys_tmp;
         int32_t* vout = to_out ? vals_out : vals_tmp;
+        int rc = SD_OK;
         unsigned* counts = cnt[p & 1];
         unsigned* next = (p + 1 < passes) ? cnt[(p + 1) & 1] : nullptr;
         const int next_shift = (p + 1) * bits;
@@ -512,20 +564,22 @@ int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t*
             }
             SD_LAUNCHED(s);
         }
-        int rc = scan_offsets(counts, tiles, 1 << bits, sums, s);
-        if (rc != SD_OK) return rc;
+        // first-pass counts, however they were made, still need their chunk sums;
+        // later passes got theirs from the scatter's adds
+        if (p == 0 && (rc = col_sums(counts, tiles, 1 << bits, w.S, s))) return rc;
+        if ((rc = scan_offsets(counts, tiles, 1 << bits, w, s))) return rc;
         switch (bits) {
             case 8:
                 k_digit_scatter<8><<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, next,
-                                                                   next_shift);
+                                                                   w.S, next_shift);
                 break;
             case 9:
                 k_digit_scatter<9><<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, next,
-                                                                   next_shift);
+                                                                   w.S, next_shift);
                 break;
             default:
                 k_digit_scatter<10><<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, next,
-                                                                    next_shift);
+                                                                    w.S, next_shift);
                 break;
         }
         SD_LAUNCHED(s);
