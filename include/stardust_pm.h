@@ -263,7 +263,8 @@ int sd_poisson_noalloc(const float* rho, int grid_size, float softening_cells, f
  * floats, device, may be NULL) is subtracted from each loaded velocity (the
  * deferred momentum zeroing of the previous step). mom_out (device, 4 doubles,
  * may be NULL) receives sum vx, vy, vz and the live count of the new
- * velocities, in a fixed summation order. */
+ * velocities, in a fixed summation order. pos and vel must be 16-byte aligned
+ * (SD_E_ARG otherwise). */
 int sd_gather_kick_drift(const float* phi, int grid_size, float pot_scale, float* pos, float* vel, int n,
                          float dt_kick, float dt_drift, float c2, const float* mean_vel, double* mom_out,
                          void* workspace, size_t workspace_bytes, void* stream);

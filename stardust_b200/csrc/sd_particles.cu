@@ -597,6 +597,9 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
                              int max_blocks, const DiagRecord* diag, int iso_S, unsigned* tile_counts,
                              int count_bits) {
     if (n <= 0) return SD_OK;
+    // particle records are read and written as float4
+    if (((uintptr_t)pos_in | (uintptr_t)vel_in | (uintptr_t)pos_out | (uintptr_t)vel_out) & 15u)
+        return fail(SD_E_ARG, "gather: pos and vel must be 16-byte aligned");
     const float h = (0.5f * (float)G) * pot_scale;  // Sim.cu:604
     int blocks = (int)gather_partials(n);
     const int cap = max_blocks > 0 ? max_blocks : gather_wave();
