@@ -84,8 +84,18 @@ typedef struct sd_config {
     int32_t units;            /* SD_UNITS_* */
     int32_t diagnostics;      /* 1 = FP64 energy and momentum of every step (sd_diagnostics_history) */
     int32_t keep_density;     /* 1 = keep the step-start density for sd_density_device_ptr (4 B/cell more traffic) */
-    int32_t reserved[6];
+    /* Initial conditions laid down by sd_init (structural changes) and sd_reset
+     * (Sim::reset, Sim.cu:4160-4238). */
+    int32_t preset;              /* SimConfig::preset (Sim.h:277): SD_PRESET_FILAMENT (default) or SD_PRESET_EMPTY */
+    float dark_matter_fraction;  /* SimConfig::darkMatterFraction (Sim.h:536): hashed share with vel.w = -100 */
+    float big_bang_shrink;       /* SimConfig::bigBangShrink (Sim.h:214): Filament ball scaled about the centre if > 0 */
+    float spin;                  /* SimConfig::spin (Sim.h:766): rigid rotation about z, v += spin * (-dy, dx, 0) */
+    float hubble;                /* SimConfig::hubble (Sim.h:196): radial flow, v += hubble * (p - 0.5) */
+    float vel_dispersion;        /* SimConfig::velDispersion (Sim.h:263): isotropic random speed of mean size */
 } sd_config;
+
+/* SimConfig::preset (Preset, Sim.h:14-17) */
+enum { SD_PRESET_FILAMENT = 0, SD_PRESET_EMPTY = 1 };
 
 /* Per-step timings (SimTimings, Sim.h:844-852), milliseconds of device time. */
 typedef struct sd_timings {
@@ -141,9 +151,13 @@ int sd_set_stream(sd_sim* sim, void* cuda_stream);
 /* ---- configuration (Sim::init / reconfigure / reset, Sim.cu:4068-4238) ------ */
 int sd_init(sd_sim* sim, const sd_config* cfg);
 int sd_reconfigure(sd_sim* sim, const sd_config* cfg);
-/* Sim::reset: zero time and step count, empty all slots (the reference's
- * Filament preset is not part of this path; scenes are loaded with
- * sd_set_particles / sd_load_state). */
+/* Sim::reset (Sim.cu:4160-4238): zero time and step count and lay down the
+ * configured preset -- kPlace's Filament ball (Sim.cu:281-407; all slots live)
+ * or Empty (all slots empty but a dark-matter halo, active count 0) -- then
+ * spin, Hubble flow and velocity dispersion, then stop the centre of mass
+ * (Filament only, as the reference divides by the active count). sd_init and
+ * structural sd_reconfigure calls do the same, as the reference's init does.
+ * Other scenes are loaded with sd_set_particles / sd_load_state. */
 int sd_reset(sd_sim* sim);
 int sd_get_config(const sd_sim* sim, sd_config* out);
 

@@ -5,9 +5,10 @@
 // SimTimings fields, no exceptions, and a sticky process-wide failure flag
 // (Sim::failed / Sim::failMessage, Sim.cu:52-75).
 //
-// What the reference has and this facade does not: presets, shapes, gas
-// physics, stars, black holes (not part of the PM path). Scenes are loaded with
-// setParticles (host float4 arrays) or loadState (STARDUST v1/v2 files).
+// What the reference has and this facade does not: shapes, gas physics, stars,
+// black holes (not part of the PM path). init/reset lay down the Filament or
+// Empty preset as the reference's do; other scenes are loaded with setParticles
+// (host float4 arrays) or loadState (STARDUST v1/v2 files).
 //
 // Link with -lstardust_pm (stardust_b200/libstardust_pm.so).
 #pragma once
@@ -20,6 +21,7 @@
 namespace stardust {
 
 enum class Boundary { Isolated = SD_BOUNDARY_ISOLATED, Periodic = SD_BOUNDARY_PERIODIC };
+enum class Preset { Filament = SD_PRESET_FILAMENT, Empty = SD_PRESET_EMPTY };  // Sim.h:14-17
 
 // The plain-PM fields of the reference's SimConfig (Sim.h:157-796), with its
 // defaults, plus this build's options.
@@ -33,6 +35,12 @@ struct SimConfig {
     int sortInterval = 1;              // Sim.h:317
     float lengthScale = 1.0f;          // Sim.h:172
     float timeUnitScale = 1.0f;        // Sim.h:180
+    Preset preset = Preset::Filament;  // Sim.h:277
+    float darkMatterFraction = 0.0f;   // Sim.h:536
+    float bigBangShrink = 0.0f;        // Sim.h:214
+    float spin = 0.0f;                 // Sim.h:766
+    float hubble = 0.0f;               // Sim.h:196
+    float velDispersion = 0.0f;        // Sim.h:263
     // options of this build (no reference counterpart)
     int order = SD_ORDER_ROWMAJOR;     // SD_ORDER_TILED enables the fused deposit
     int integrator = SD_INT_KD;
@@ -57,6 +65,12 @@ struct SimConfig {
         c.units = units;
         c.diagnostics = diagnostics ? 1 : 0;
         c.keep_density = keepDensity ? 1 : 0;
+        c.preset = static_cast<int>(preset);
+        c.dark_matter_fraction = darkMatterFraction;
+        c.big_bang_shrink = bigBangShrink;
+        c.spin = spin;
+        c.hubble = hubble;
+        c.vel_dispersion = velDispersion;
         return c;
     }
 };

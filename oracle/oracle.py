@@ -497,6 +497,116 @@ _ASTRO_C = np.array([[0.00, 0.00, 0.00], [0.05, 0.06, 0.19], [0.16, 0.14, 0.47],
 _ASTRO_S = np.array([0.00, 0.18, 0.38, 0.58, 0.76, 0.90, 1.00])
 
 
+# ---- initial conditions of Sim::reset (Sim.cu:4160-4238) -------------------------
+
+PRESET_FILAMENT, PRESET_EMPTY = 0, 1
+_U32 = np.uint32
+
+
+def pcg_hash(v) -> np.ndarray:
+    """pcgHash (Sim.cu:78-82), uint32 arithmetic modulo 2^32."""
+    with np.errstate(over="ignore"):
+        s = np.asarray(v, _U32) * _U32(747796405) + _U32(2891336453)
+        w = ((s >> ((s >> _U32(28)) + _U32(4))) ^ s) * _U32(277803737)
+        return (w >> _U32(22)) ^ w
+
+
+def rnd01(s) -> np.ndarray:
+    """rnd01 (Sim.cu:84-86): the hash rounded to float32 times 2^-32."""
+    return pcg_hash(s).astype(np.float32) * np.float32(2.3283064365386963e-10)
+
+
+def _mul(s, a: int, b: int):
+    with np.errstate(over="ignore"):
+        return np.asarray(s, _U32) * _U32(a) + _U32(b)
+
+
+def _sphere_dir(s):
+    f = np.float32
+    cz = rnd01(_mul(s, 3, 1)) * f(2.0) - f(1.0)
+    sz = np.sqrt(np.maximum(f(1.0) - cz * cz, f(0.0))).astype(f)
+    ph = rnd01(_mul(s, 7, 5)) * f(6.2831853)
+    return cz, sz, ph
+
+
+def _at_radius(r, cz, sz, ph):
+    f = np.float32
+    return (r * sz * np.cos(ph).astype(f), r * sz * np.sin(ph).astype(f), r * cz)
+
+
+def place_preset(n: int, preset: int = PRESET_FILAMENT, dark_frac: float = 0.0, shrink: float = 0.0,
+                 spin: float = 0.0, hubble: float = 0.0, vrms: float = 0.0):
+    """Sim::reset's particles in float32: kPlace (Sim.cu:281-407) with seed 12345
+    (Sim.cu:3642) for the Filament / Empty presets, then kAddSpin, kAddHubble and
+    kAddDispersion (Sim.cu:2406-2476, seed 24680) and, for Filament, the
+    centre-of-mass stop over all n slots (Sim.cu:4218-4235). Angles use libm
+    sin/cos where the reference uses the fast intrinsics, so positions agree with
+    it to a few 1e-7."""
+    f = np.float32
+    i = np.arange(n, dtype=_U32)
+    s = _mul(i, 2654435761, 12345)
+    pos = np.zeros((n, 4), f)
+    vel = np.zeros((n, 4), f)
+    dark = (rnd01(_mul(s, 13, 7)) < f(dark_frac)) if dark_frac > 0 else np.zeros(n, bool)
+    if preset == PRESET_FILAMENT:
+        cz, sz, ph = _sphere_dir(s ^ _U32(0x6C8E9CF5))
+        r = f(0.5) * np.cbrt(np.maximum(rnd01(s ^ _U32(0x6C8E9CF5)), f(1e-9))).astype(f)
+        bx, by, bz = _at_radius(r, cz, sz, ph)
+        x, y, z = f(0.5) + bx, f(0.5) + by, f(0.5) + bz
+        dx = np.zeros(n, f)
+        dy = np.zeros(n, f)
+        dz = np.zeros(n, f)
+        for m in range(3):
+            fm = f(m)
+            k = f(6.2831853) * (f(2.0) + fm * f(2.0))
+            amp = f(0.16) / (f(1.0) + fm)
+            dx = dx + amp * np.sin(k * (y + f(0.13) * fm)).astype(f) * np.cos(k * (z + f(0.29))).astype(f)
+            dy = dy + amp * np.sin(k * (z + f(0.19) * fm)).astype(f) * np.cos(k * (x + f(0.37))).astype(f)
+            dz = dz + amp * np.sin(k * (x + f(0.23) * fm)).astype(f) * np.cos(k * (y + f(0.11))).astype(f)
+        px, py, pz = x + dx, y + dy, z + dz
+        rx, ry, rz = px - f(0.5), py - f(0.5), pz - f(0.5)
+        rr = np.sqrt(rx * rx + ry * ry + rz * rz).astype(f)
+        out = rr > f(0.5)
+        q = np.where(out, f(0.5) / np.where(out, rr, f(1.0)), f(1.0)).astype(f)
+        px = np.where(out, f(0.5) + rx * q, px)
+        py = np.where(out, f(0.5) + ry * q, py)
+        pz = np.where(out, f(0.5) + rz * q, pz)
+        if shrink > 0:
+            sh = f(shrink)
+            px, py, pz = f(0.5) + (px - f(0.5)) * sh, f(0.5) + (py - f(0.5)) * sh, f(0.5) + (pz - f(0.5)) * sh
+        pos[:, 0], pos[:, 1], pos[:, 2] = px, py, pz
+        vel[:, 3] = np.where(dark, f(-100.0), f(0.0))
+    else:
+        pos[:, :3] = -1.0
+        if dark.any():  # the dark fraction still lands in a halo (bulgePoint, Sim.cu:228-236)
+            sd = s[dark] ^ _U32(0x2545F491)
+            u = rnd01(sd)
+            cz, sz, ph = _sphere_dir(sd)
+            hx, hy, hz = _at_radius(f(0.42) * u * u, cz, sz, ph)
+            pos[dark, 0], pos[dark, 1], pos[dark, 2] = f(0.5) + hx, f(0.5) + hy, f(0.5) + hz
+            vel[dark, 3] = -100.0
+    live = pos[:, 0] >= 0
+    v = vel[:, :3]
+    if spin != 0:
+        om = f(spin)
+        ry, rx = pos[:, 1] - f(0.5), pos[:, 0] - f(0.5)
+        v[live, 0] += -om * ry[live]
+        v[live, 1] += om * rx[live]
+    if hubble != 0:
+        v[live] += f(hubble) * (pos[live, :3] - f(0.5))
+    if vrms > 0:
+        sd = _mul(i, 2654435761, 24680)
+        cz, sz, ph = _sphere_dir(sd)
+        g = (rnd01(_mul(sd, 11, 3)) + rnd01(_mul(sd, 13, 7)) + rnd01(_mul(sd, 17, 9))) / f(1.5)
+        a = f(vrms) * g
+        add = np.stack([a * sz * np.cos(ph).astype(f), a * sz * np.sin(ph).astype(f), a * cz], axis=1)
+        v[live] += add[live]
+    if preset == PRESET_FILAMENT and n > 0:
+        mean = (v[live].astype(np.float64).sum(axis=0) / n).astype(f)
+        v[live] -= mean
+    return pos, vel
+
+
 def _cmap(kind: int, t: np.ndarray) -> np.ndarray:
     t = np.clip(np.asarray(t, np.float64), 0.0, 1.0)
     if kind == 1:

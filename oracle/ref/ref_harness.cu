@@ -115,6 +115,25 @@ int ref_load(void* h, const float* pos, const float* vel, int n, int G, float gr
     return ref_load_b(h, pos, vel, n, G, gravity, soft, time_scale, sort_interval, 1, tmp_path);
 }
 
+// Sim::init with the plain-PM settings and the given initial conditions; init
+// ends in reset(), which lays the preset down (placeInitial, spin, Hubble flow,
+// dispersion, centre-of-mass stop). preset 0 Filament, 1 Empty (Sim.h:14-17).
+int ref_init_preset(void* h, int n, int G, int boundary, int preset, float dark_frac, float shrink, float spin,
+                    float hubble, float disp) {
+    const Boundary b = boundary == 0 ? Boundary::Isolated : Boundary::Periodic;
+    SimConfig c = plain_pm(n, G, 1.f, 1.f, 1.f, 1, b);
+    c.preset = preset == 0 ? Preset::Filament : Preset::Empty;
+    c.darkMatterFraction = dark_frac;
+    c.bigBangShrink = shrink;
+    c.spin = spin;
+    c.hubble = hubble;
+    c.velDispersion = disp;
+    Sim* s = static_cast<Sim*>(h);
+    s->init(c);
+    cudaDeviceSynchronize();
+    return Sim::failed() ? -2 : 0;
+}
+
 int ref_step(void* h) {
     static_cast<Sim*>(h)->step();
     return Sim::failed() ? -2 : 0;

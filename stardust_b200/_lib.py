@@ -18,6 +18,7 @@ SD_ORDER_ROWMAJOR, SD_ORDER_MORTON, SD_ORDER_TILED = 0, 1, 2
 SD_INT_KD, SD_INT_KDK = 0, 1
 SD_UNITS_REFERENCE, SD_UNITS_NEWTON = 0, 1
 SD_HOST, SD_DEVICE = 0, 1
+SD_PRESET_FILAMENT, SD_PRESET_EMPTY = 0, 1
 
 
 class SdConfig(ctypes.Structure):
@@ -36,7 +37,12 @@ class SdConfig(ctypes.Structure):
         ("units", ctypes.c_int32),
         ("diagnostics", ctypes.c_int32),
         ("keep_density", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 6),
+        ("preset", ctypes.c_int32),
+        ("dark_matter_fraction", ctypes.c_float),
+        ("big_bang_shrink", ctypes.c_float),
+        ("spin", ctypes.c_float),
+        ("hubble", ctypes.c_float),
+        ("vel_dispersion", ctypes.c_float),
     ]
 
 

@@ -121,6 +121,9 @@ int launch_max_speed(const float4* pos, const float4* vel, int n, const float* m
 int launch_energy(const float* phi, int G, const float4* pos, const float4* vel, int n, const float* mean_vel,
                   double* partials, double* out8, cudaStream_t s, int iso_S = 0);
 int launch_reduce_grid(const float* rho, size_t cells, int op, double* partials, double* out, cudaStream_t s);
+// Sim::reset's placement (sd_scene.cu): preset, initial velocities, centre-of-mass stop.
+int launch_place_preset(float4* pos, float4* vel, int n, const sd_config& cfg, double* partials, double* out8,
+                        float* mean, cudaStream_t s);
 int launch_hide_range(float4* pos, float4* vel, int from, int to, cudaStream_t s);
 
 }  // namespace sd

@@ -252,7 +252,21 @@ int validate_config(const sd_config* c) {
     if (c->order < SD_ORDER_ROWMAJOR || c->order > SD_ORDER_TILED) return fail(SD_E_ARG, "config: bad order");
     if (c->integrator != SD_INT_KD && c->integrator != SD_INT_KDK) return fail(SD_E_ARG, "config: bad integrator");
     if (c->units != SD_UNITS_REFERENCE && c->units != SD_UNITS_NEWTON) return fail(SD_E_ARG, "config: bad units");
+    if (c->preset != SD_PRESET_FILAMENT && c->preset != SD_PRESET_EMPTY) return fail(SD_E_ARG, "config: bad preset");
     return SD_OK;
+}
+
+// placeInitial + reset's velocity and centre-of-mass passes (Sim.cu:3635-3649,
+// 4160-4238): the configured preset in every slot. The mean buffer serves as
+// scratch and is left zero (no correction pending).
+int place_initial(sd_sim* s) {
+    int rc = launch_place_preset(s->pos, s->vel, s->N, s->cfg, s->partials, s->mom, s->mean, s->stream);
+    if (!rc && SD_CUDA(cudaMemsetAsync(s->mean, 0, sizeof(float) * 4, s->stream))) rc = SD_E_CUDA;
+    s->active = (s->cfg.preset == SD_PRESET_FILAMENT) ? s->N : 0;
+    s->mean_pending = false;
+    s->rho_valid = false;
+    s->keys_valid = false;
+    return rc;
 }
 
 int sim_error(sd_sim* s, int rc) {
@@ -454,7 +468,8 @@ int reconfigure(sd_sim* s, const sd_config* c) {
     s->G = G;
     rc = allocate(s);
     if (rc) return rc;
-    s->active = 0;
+    // the reference's init / structural reconfigure ends in reset() (Sim.cu:4151)
+    if ((rc = place_initial(s))) return sim_error(s, rc);
     s->sim_time = 0.0;
     s->step_count = 0;
     s->mean_pending = false;
@@ -532,6 +547,7 @@ int sd_config_default(sd_config* c) {
     c->units = SD_UNITS_REFERENCE;
     c->diagnostics = 0;
     c->keep_density = 1;
+    c->preset = SD_PRESET_FILAMENT;  // Sim.h:277
     return SD_OK;
 }
 
@@ -613,15 +629,10 @@ int sd_reset(sd_sim* s) {
     DeviceGuard g(s->device);
     s->sim_time = 0.0;
     s->step_count = 0;
-    s->active = 0;
-    s->mean_pending = false;
     s->lf_open = false;
-    s->rho_valid = false;
-    s->keys_valid = false;
-    if (SD_CUDA(cudaMemsetAsync(s->mean, 0, sizeof(float) * 4, s->stream)) ||
-        SD_CUDA(cudaMemsetAsync(s->diag_count, 0, sizeof(unsigned long long), s->stream)))
-        return SD_E_CUDA;
-    return launch_hide_range(s->pos, s->vel, 0, s->N, s->stream);
+    if (SD_CUDA(cudaMemsetAsync(s->diag_count, 0, sizeof(unsigned long long), s->stream))) return SD_E_CUDA;
+    const int rc = place_initial(s);
+    return rc ? sim_error(s, rc) : SD_OK;
 }
 
 int sd_get_config(const sd_sim* s, sd_config* out) {
@@ -906,7 +917,7 @@ int sd_save_state(sd_sim* s, const char* path) {
     h.version = 2;
     h.count = n;
     h.gridSize = s->G;
-    h.preset = 1;  // Preset::Empty: the particles are the scene
+    h.preset = s->cfg.preset;  // Sim.cu:5017
     h.boundary = s->cfg.boundary;
     h.gravity = s->cfg.gravity;
     h.simTime = (float)s->sim_time;
@@ -947,6 +958,8 @@ int sd_load_state(sd_sim* s, const char* path) {
     c.grid_size = h.gridSize;
     c.boundary = h.boundary;
     c.gravity = h.gravity;
+    // (Preset)h.preset (Sim.cu:5082); presets other than Filament place as Empty
+    c.preset = (h.preset == SD_PRESET_FILAMENT) ? SD_PRESET_FILAMENT : SD_PRESET_EMPTY;
     int rc = reconfigure(s, &c);
     if (rc) {
         fclose(f);

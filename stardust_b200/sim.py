@@ -39,6 +39,13 @@ class SimConfig:
     units: int = L.SD_UNITS_REFERENCE
     diagnostics: int = 0
     keep_density: int = 1
+    # initial conditions of init / reset (Sim::reset, Sim.cu:4160-4238)
+    preset: int = L.SD_PRESET_FILAMENT   # Sim.h:277
+    dark_matter_fraction: float = 0.0    # Sim.h:536
+    big_bang_shrink: float = 0.0         # Sim.h:214
+    spin: float = 0.0                    # Sim.h:766
+    hubble: float = 0.0                  # Sim.h:196
+    vel_dispersion: float = 0.0          # Sim.h:263
 
     def to_c(self) -> L.SdConfig:
         c = L.SdConfig()

@@ -3,13 +3,15 @@
 Usage (on a machine with a CUDA GPU and the prebuilt oracle/_ref/libsimref.so):
     python tests/golden/make_reference_fixtures.py OUTDIR
 
-For each case it writes ``reference_<name>.npz`` holding the seeded input
+For each step case it writes ``reference_<name>.npz`` holding the seeded input
 particles, the reference's density after Sim::loadState (deposit of the loaded
 positions), and the particles after one Sim::step() (sort + deposit + cuFFT
 Poisson + gradient + kick/drift + momentum zeroing). Velocities carry a particle
 id in ``w`` (the reference copies w through the sort and the integrator), so the
-reference's sort permutation can be read back. The cases are small so the
-committed files stay small.
+reference's sort permutation can be read back. For each preset case it writes
+``reference_preset_<name>.npz``: the particles Sim::init lays down (reset():
+kPlace, spin, Hubble flow, dispersion, centre-of-mass stop) for the given
+settings. The cases are small so the committed files stay small.
 """
 from __future__ import annotations
 
@@ -40,6 +42,7 @@ def load_ref():
     L.ref_get.argtypes = [P, P, P, I]
     L.ref_density.argtypes = [P, P, I]
     L.ref_timings.argtypes = [P, P]
+    L.ref_init_preset.argtypes = [P, I, I, I, I, F, F, F, F, F]
     L.ref_fail_message.restype = ctypes.c_char_p
     L.ref_sim_time.argtypes = [P]
     L.ref_sim_time.restype = ctypes.c_double
@@ -95,9 +98,31 @@ def cases():
     yield "isolated_g32", p, v, 32, 32.0, 1.5, 1e-3, 0
 
 
+def preset_cases():
+    # name, n, G, preset, dark fraction, shrink, spin, hubble, dispersion
+    yield "filament_all", 6000, 32, 0, 0.25, 0.9, 0.7, 0.4, 0.05
+    yield "filament_plain", 4096, 16, 0, 0.0, 0.0, 0.0, 0.0, 0.0
+    yield "empty_dark", 3000, 16, 1, 0.3, 0.0, 0.5, 0.0, 0.1
+
+
 def main(outdir: str) -> int:
     os.makedirs(outdir, exist_ok=True)
     L = load_ref()
+    for name, n, G, preset, dark, shrink, spin, hubble, disp in preset_cases():
+        h = L.ref_create()
+        try:
+            rc = L.ref_init_preset(h, n, G, 1, preset, dark, shrink, spin, hubble, disp)
+            if rc != 0:
+                raise RuntimeError(f"ref_init_preset failed: {rc} {L.ref_fail_message()}")
+            p = np.empty((n, 4), np.float32)
+            v = np.empty((n, 4), np.float32)
+            L.ref_get(h, p.ctypes.data, v.ctypes.data, n)
+        finally:
+            L.ref_destroy(h)
+        np.savez_compressed(os.path.join(outdir, f"reference_preset_{name}.npz"), pos=p, vel=v, n=n, grid=G,
+                            preset=preset, dark_matter_fraction=np.float32(dark), big_bang_shrink=np.float32(shrink),
+                            spin=np.float32(spin), hubble=np.float32(hubble), vel_dispersion=np.float32(disp))
+        print(name, "live", int((p[:, 0] >= 0).sum()), "dark", int((v[:, 3] == -100).sum()))
     with tempfile.TemporaryDirectory() as tmp:
         for name, pos, vel, G, grav, soft, dt, boundary in cases():
             pos = np.ascontiguousarray(pos, np.float32)

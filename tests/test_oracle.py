@@ -93,8 +93,28 @@ def test_pm_accel_f64_two_particles_antisymmetric(oracle):
 
 
 def _golden_files(isolated=False):
+    """One-step fixtures (the preset fixtures hold initial conditions only)."""
     files = sorted(glob.glob(os.path.join(GOLDEN, "reference_*.npz")))
+    files = [f for f in files if not os.path.basename(f).startswith("reference_preset_")]
     return [f for f in files if ("isolated" in os.path.basename(f)) == isolated]
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "reference_preset_*.npz"))),
+                         ids=lambda p: os.path.basename(p)[17:-4])
+def test_preset_oracle_against_reference_fixtures(oracle, path):
+    """place_preset reproduces the particles the unmodified reference's Sim::init
+    lays down (kPlace, spin, Hubble flow, dispersion, centre-of-mass stop): the
+    same hashes pick the same slots and dark-matter marks; positions differ only
+    by libm sin/cos against the reference's fast intrinsics (arguments up to ~50)."""
+    f = np.load(path)
+    po, vo = oracle.place_preset(int(f["n"]), int(f["preset"]), float(f["dark_matter_fraction"]),
+                                 float(f["big_bang_shrink"]), float(f["spin"]), float(f["hubble"]),
+                                 float(f["vel_dispersion"]))
+    live = f["pos"][:, 0] >= 0
+    assert np.array_equal(po[:, 0] >= 0, live)
+    assert np.array_equal(vo[:, 3], f["vel"][:, 3])
+    assert np.abs(po[live, :3] - f["pos"][live, :3]).max() < 4e-6
+    assert np.abs(vo[:, :3] - f["vel"][:, :3]).max() < 4e-6
 
 
 @pytest.mark.skipif(not _golden_files(), reason="no reference fixtures committed")
