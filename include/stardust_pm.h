@@ -28,7 +28,9 @@
 extern "C" {
 #endif
 
-#define SD_ABI_VERSION 1
+/* 2: sd_config's last six words carry the initial conditions (preset, ...) and
+ * sd_init / sd_reset lay the preset down, as the reference's init / reset do. */
+#define SD_ABI_VERSION 2
 
 /* ---- status codes ---------------------------------------------------------- */
 enum {

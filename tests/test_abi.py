@@ -43,7 +43,7 @@ def test_defaults_follow_reference_simconfig(lib):
 
 
 def test_static_queries(lib):
-    assert lib.sd_abi_version() == 1
+    assert lib.sd_abi_version() == 2
     assert lib.sd_max_grid_size(L.SD_BOUNDARY_PERIODIC) == 512       # Sim.cu:4158
     assert lib.sd_max_grid_size(L.SD_BOUNDARY_ISOLATED) == 256
     # key bits of key+1: G^3 + 1 values for row-major / Morton; tile rows: G^2 values
