@@ -358,17 +358,30 @@ typedef struct sd_view {
     float zoom, pan_x, pan_y;
     float size_px;       /* particle footprint before the visibility cap */
     int32_t color_by;    /* 0 density, 2 speed */
-    int32_t cmap;        /* 0 astro, 1 gray, 2 thermal */
+    int32_t cmap;        /* 0 astro, 1 gray, 2 thermal, 3 black body */
     float bright, inv_gamma;
     int32_t use_cmap;    /* 1: accumulated brightness through the colour map */
     int32_t reinhard;    /* 1: x / (1 + x) tone curve when use_cmap is 0 */
-    int32_t reserved[4];
+    int32_t rot_on;      /* ViewRot.on: grid views project through rot (0: straight down z) */
+    int32_t reserved[3];
 } sd_view;
 void sd_view_default(sd_view* view); /* top-down, zoom 1, density, astro map */
 size_t sd_render_workspace_bytes(int width, int height);
 /* pos, vel: device float4[n]; rgba_out: device uchar4[width * height] */
 int sd_render_points(const float* pos, const float* vel, int n, const sd_view* view, int width, int height,
                      void* workspace, size_t workspace_bytes, void* rgba_out, void* stream);
+/* Grid view of a field (Sim::fieldDevicePtr, Sim.cu:5229-5296, drawn by kShade,
+ * RenderField.cu:158-316): SD_FIELD_DENSITY projects the density grid
+ * (device float[G^3], z-major) along z -- or through view->rot when
+ * view->rot_on -- and scales brightness by the value 5 % from the top of its
+ * log histogram (n / G^2 when empty); SD_FIELD_DISPERSION is the rms speed of
+ * the particles (device float4[n]) under each screen cell. Zoom, pan, bright,
+ * inv_gamma and cmap come from view; rows are bottom-up like the points image. */
+enum { SD_FIELD_DENSITY = 0, SD_FIELD_DISPERSION = 1 };
+size_t sd_render_field_workspace_bytes(int grid_size);
+int sd_render_field(int field, const float* density, int grid_size, const float* pos, const float* vel, int n,
+                    const sd_view* view, int width, int height, void* workspace, size_t workspace_bytes,
+                    void* rgba_out, void* stream);
 
 /* ---- FP64 reference forces (force-error judge; not on the step) ------------
  * Periodic Newtonian accelerations (G = 1, each source of mass 1/n_src, mean

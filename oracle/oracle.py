@@ -614,7 +614,130 @@ def _cmap(kind: int, t: np.ndarray) -> np.ndarray:
     if kind == 2:
         return np.stack([np.minimum(t * 2.2, 1.0), np.clip((t - 0.32) * 1.9, 0.0, 1.0),
                          np.clip((t - 0.70) * 3.2, 0.0, 1.0)], axis=-1)
+    if kind == 3:  # cmapBlackbody (RenderField.cu:60-82)
+        u = np.where(t < 0.5, t * 2.0, (t - 0.5) * 2.0)
+        r = np.where(t < 0.5, 1.0, 1.0 - 0.38 * u)
+        g = np.where(t < 0.5, 0.32 + 0.68 * u, 1.0 - 0.30 * u)
+        b = np.where(t < 0.5, 0.08 + 0.80 * u * u, 1.0)
+        dim = np.minimum(t * 3.2, 1.0)
+        return np.stack([r * dim, g * dim, b * dim], axis=-1)
     return np.stack([np.interp(t, _ASTRO_S, _ASTRO_C[:, j]) for j in range(3)], axis=-1)
+
+
+def project_field(rho: np.ndarray, view: dict) -> np.ndarray:
+    """kProjectXY (Sim.cu:2526-2537): the G^3 density summed along z (view off) or
+    each cell's centre through the view rotation into its screen cell; (G, G)
+    indexed [y, x]."""
+    rho = np.asarray(rho, np.float64)
+    G = rho.shape[0]
+    if not view.get("rot_on", 0):
+        return rho.sum(axis=0)
+    z, y, x = np.nonzero(rho)
+    c = (np.stack([x, y, z], axis=1) + 0.5) / G - np.asarray(view["center"], np.float64)
+    R = np.asarray(view["rot"], np.float64).reshape(3, 3)
+    ox, oy = c @ R[0] + 0.5, c @ R[1] + 0.5
+    ok = (ox >= 0) & (ox < 1) & (oy >= 0) & (oy < 1)
+    sx, sy = (ox[ok] * G).astype(np.int64), (oy[ok] * G).astype(np.int64)
+    out = np.zeros((G, G))
+    np.add.at(out, (sy, sx), rho[z[ok], y[ok], x[ok]])
+    return out
+
+
+def dispersion_field(pos, vel, G: int, view: dict) -> np.ndarray:
+    """kScatterDispersion + kDivideInto (Sim.cu:2548-2570, 2701-2707): the rms
+    speed under each screen cell, bilinear weights with edge clamping."""
+    pos = np.asarray(pos, np.float64)
+    vel = np.asarray(vel, np.float64)
+    live = pos[:, 0] >= 0
+    p, v = pos[live], vel[live]
+    v2 = np.sum(v[:, :3] ** 2, axis=1)
+    if view.get("rot_on", 0):
+        c = p[:, :3] - np.asarray(view["center"], np.float64)
+        R = np.asarray(view["rot"], np.float64).reshape(3, 3)
+        ux, uy = c @ R[0] + 0.5, c @ R[1] + 0.5
+        ok = (ux >= 0) & (ux < 1) & (uy >= 0) & (uy < 1)
+        ux, uy, v2 = ux[ok], uy[ok], v2[ok]
+    else:
+        ux, uy = p[:, 0], p[:, 1]
+    gx, gy = ux * G - 0.5, uy * G - 0.5
+    ix, iy = np.floor(gx).astype(np.int64), np.floor(gy).astype(np.int64)
+    fx, fy = gx - ix, gy - iy
+    num = np.zeros((G, G))
+    den = np.zeros((G, G))
+    for ox in (0, 1):
+        for oy in (0, 1):
+            cx, cy = np.clip(ix + ox, 0, G - 1), np.clip(iy + oy, 0, G - 1)
+            w = (fx if ox else 1 - fx) * (fy if oy else 1 - fy)
+            np.add.at(num, (cy, cx), w * v2)
+            np.add.at(den, (cy, cx), w)
+    return np.where(den > 1e-6, np.sqrt(np.maximum(num / np.where(den > 1e-6, den, 1.0), 0.0)), 0.0)
+
+
+def field_brightness(g: np.ndarray, n: int, brightness: float) -> float:
+    """The density view's brightness factor (RenderField.cu:125-137, 930-1000):
+    brightness over the value 5 % from the top of a 64-bin log histogram of the
+    positive cells, interpolated in its bin (n / G^2 when nothing is positive)."""
+    G = g.shape[0]
+    norm = n / (G * G)
+    vals = g[g > 0]
+    if len(vals):
+        b = np.clip(((np.log(vals) + 9.21) / (18.42 + 9.21) * 64).astype(np.int64), 0, 63)
+        h = np.bincount(b, minlength=64)
+        total = int(h.sum())
+        want = int(total * 0.05) + 1
+        acc, hit = 0, 63
+        for k in range(63, -1, -1):
+            acc += int(h[k])
+            if acc >= want:
+                hit = k
+                break
+        below = acc - int(h[hit])
+        frac = min(max((want - below) / h[hit], 0.0), 1.0) if h[hit] > 0 else 0.5
+        m = float(np.exp((hit + 1.0 - frac) / 64 * (18.42 + 9.21) - 9.21))
+        if m > 1e-6:
+            norm = m
+    return brightness / max(norm, 1e-6)
+
+
+def shade(g: np.ndarray, bright: float, view: dict, W: int, H: int) -> np.ndarray:
+    """kShade (RenderField.cu:158-316) over a (G, G) field; rows bottom-up."""
+    G = g.shape[0]
+    y, x = np.mgrid[0:H, 0:W]
+    u, v = (x + 0.5) / W, (y + 0.5) / H
+    aspect = W / H
+    if aspect > 1:
+        u = (u - 0.5) * aspect + 0.5
+    else:
+        v = (v - 0.5) / aspect + 0.5
+    u = (u - 0.5) / view["zoom"] + 0.5 - view["pan_x"]
+    v = (v - 0.5) / view["zoom"] + 0.5 - view["pan_y"]
+    inside = (u >= 0) & (u < 1) & (v >= 0) & (v < 1)
+    gfx, gfy = u * G - 0.5, v * G - 0.5
+    x0, y0 = np.floor(gfx).astype(np.int64), np.floor(gfy).astype(np.int64)
+    tx, ty = gfx - x0, gfy - y0
+    x1, y1 = np.clip(x0 + 1, 0, G - 1), np.clip(y0 + 1, 0, G - 1)
+    x0, y0 = np.clip(x0, 0, G - 1), np.clip(y0, 0, G - 1)
+    d = (g[y0, x0] * (1 - tx) * (1 - ty) + g[y0, x1] * tx * (1 - ty) + g[y1, x0] * (1 - tx) * ty +
+         g[y1, x1] * tx * ty)
+    xl = np.maximum(np.log1p(d * bright) * 0.60, 0.0)
+    t = np.power(xl / (1 + xl), view["inv_gamma"])
+    rgb = (_cmap(view["cmap"], t) * 255.0).astype(np.uint8)
+    out = np.zeros((H, W, 4), np.uint8)
+    out[..., 3] = 255
+    out[..., :3] = np.where(inside[..., None], rgb, 0)
+    return out[::-1]
+
+
+def render_field(field: int, rho, pos, vel, G: int, view: dict, W: int, H: int) -> np.ndarray:
+    """(H, W, 4) uint8 grid view: field 0 the density (rho, G^3 z-major), 1 the
+    velocity dispersion of the particles."""
+    if field == 0:
+        g = project_field(np.asarray(rho).reshape(G, G, G), view)
+        bright = field_brightness(g, len(pos) if pos is not None else 0, view["bright"])
+    else:
+        g = dispersion_field(pos, vel, G, view)
+        bright = view["bright"] * 60.0
+    return shade(g, bright, view, W, H)
 
 
 def render_points(pos, vel, view: dict, W: int, H: int) -> np.ndarray:

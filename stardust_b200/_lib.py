@@ -19,6 +19,7 @@ SD_INT_KD, SD_INT_KDK = 0, 1
 SD_UNITS_REFERENCE, SD_UNITS_NEWTON = 0, 1
 SD_HOST, SD_DEVICE = 0, 1
 SD_PRESET_FILAMENT, SD_PRESET_EMPTY = 0, 1
+SD_FIELD_DENSITY, SD_FIELD_DISPERSION = 0, 1
 
 
 class SdConfig(ctypes.Structure):
@@ -65,7 +66,8 @@ class SdView(ctypes.Structure):
                 ("tan_half_fov", ctypes.c_float), ("zoom", ctypes.c_float), ("pan_x", ctypes.c_float),
                 ("pan_y", ctypes.c_float), ("size_px", ctypes.c_float), ("color_by", ctypes.c_int32),
                 ("cmap", ctypes.c_int32), ("bright", ctypes.c_float), ("inv_gamma", ctypes.c_float),
-                ("use_cmap", ctypes.c_int32), ("reinhard", ctypes.c_int32), ("reserved", ctypes.c_int32 * 4)]
+                ("use_cmap", ctypes.c_int32), ("reinhard", ctypes.c_int32), ("rot_on", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 3)]
 
 
 class SdSceneTuning(ctypes.Structure):
@@ -163,6 +165,8 @@ SIGNATURES = [
     ("sd_view_default", None, [_P]),
     ("sd_render_workspace_bytes", _S, [_I, _I]),
     ("sd_render_points", _I, [_P, _P, _I, _P, _I, _I, _P, _S, _P, _P]),
+    ("sd_render_field_workspace_bytes", _S, [_I]),
+    ("sd_render_field", _I, [_I, _P, _I, _P, _P, _I, _P, _I, _I, _P, _S, _P, _P]),
     ("sd_ewald_modes", _I, [_I]),
     ("sd_ewald_workspace_bytes", _S, [_I]),
     ("sd_ewald_forces", _I, [_P, _I, _P, _I, _D, _D, _I, _P, _P, _S, _P]),

@@ -1,7 +1,8 @@
-"""Headless point render of a simulation's particles into an RGBA image
-(sd_render_points): the reference's kSplatPoints -> kAccumToRGBA path without
-OpenGL. ``render(sim, width, height, **view)`` returns an (H, W, 4) uint8 array;
-``view_default()`` gives the top-down density view."""
+"""Headless renders into RGBA images without OpenGL: the point view
+(sd_render_points, the reference's kSplatPoints -> kAccumToRGBA) and the grid
+view (sd_render_field, its field projections -> kShade). ``render(sim, width,
+height, **view)`` and ``render_field(sim, width, height, field, **view)`` return
+(H, W, 4) uint8 arrays; ``view_default()`` gives the top-down density view."""
 from __future__ import annotations
 
 import ctypes
@@ -37,6 +38,37 @@ def render_device(pos_ptr: int, vel_ptr: int, n: int, view: L.SdView, width: int
     L.check(lib.sd_render_points(pos_ptr, vel_ptr, n, ctypes.byref(view), width, height, ws.data_ptr(), ws.numel(),
                                  out.data_ptr(), stream), "sd_render_points")
     return out
+
+
+def render_field_device(field: int, density_ptr: int, G: int, pos_ptr: int, vel_ptr: int, n: int, view: L.SdView,
+                        width: int, height: int, stream=None):
+    """Grid view of a device density grid (float[G^3]) or of device particles
+    (dispersion); returns a CUDA uint8 tensor (H, W, 4)."""
+    import torch
+
+    lib = L.lib()
+    ws = torch.empty(int(lib.sd_render_field_workspace_bytes(G)), dtype=torch.uint8, device="cuda")
+    out = torch.empty((height, width, 4), dtype=torch.uint8, device="cuda")
+    L.check(lib.sd_render_field(field, density_ptr, G, pos_ptr, vel_ptr, n, ctypes.byref(view), width, height,
+                                ws.data_ptr(), ws.numel(), out.data_ptr(), stream), "sd_render_field")
+    return out
+
+
+def render_field(sim, width: int, height: int, field: int = L.SD_FIELD_DENSITY, **view) -> np.ndarray:
+    """Grid view of a Sim: its density of the step-start positions (of the
+    current positions before any step) or the velocity dispersion."""
+    import torch
+
+    n, G = sim.particle_count(), sim.grid_size()
+    pos = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    vel = torch.empty_like(pos)
+    sim.get_particles_into(pos, vel)
+    rho = torch.from_numpy(np.ascontiguousarray(sim.density(), np.float32)).cuda() if field == L.SD_FIELD_DENSITY \
+        else torch.empty(1, device="cuda")
+    torch.cuda.synchronize()
+    img = render_field_device(field, rho.data_ptr(), G, pos.data_ptr(), vel.data_ptr(), n, view_default(**view),
+                              width, height)
+    return img.cpu().numpy()
 
 
 def render(sim, width: int, height: int, **view) -> np.ndarray:
