@@ -28,8 +28,9 @@
 extern "C" {
 #endif
 
-/* 2: sd_config's last six words carry the initial conditions (preset, ...) and
- * sd_init / sd_reset lay the preset down, as the reference's init / reset do. */
+/* 2: sd_config carries the initial conditions (preset, ...), which sd_init /
+ * sd_reset lay down as the reference's init / reset do, and the hydro add-ons;
+ * it grew to 32 words. */
 #define SD_ABI_VERSION 2
 
 /* ---- status codes ---------------------------------------------------------- */
@@ -94,6 +95,15 @@ typedef struct sd_config {
     float spin;                  /* SimConfig::spin (Sim.h:766): rigid rotation about z, v += spin * (-dy, dx, 0) */
     float hubble;                /* SimConfig::hubble (Sim.h:196): radial flow, v += hubble * (p - 0.5) */
     float vel_dispersion;        /* SimConfig::velDispersion (Sim.h:263): isotropic random speed of mean size */
+    /* Grid hydrodynamics add-ons (doCooling / kPressure, Sim.cu:3605-3868). The
+     * reference enables both by default; here they are off unless set, as the PM
+     * path is the product. A cooling step runs every 2 steps with pressure, every
+     * 8 without (then sd_steps runs eagerly and ensembles reject the scene). */
+    int32_t pressure_enabled;    /* SimConfig::pressureEnabled (Sim.h:319) */
+    float pressure_k;            /* SimConfig::pressureK (Sim.h:320), default 0.45 */
+    int32_t cooling_enabled;     /* SimConfig::coolingEnabled (Sim.h:327) */
+    float cooling_rate;          /* SimConfig::coolingRate (Sim.h:345), default 0.08 */
+    int32_t reserved[8];
 } sd_config;
 
 /* SimConfig::preset (Preset, Sim.h:14-17) */

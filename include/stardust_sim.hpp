@@ -41,6 +41,11 @@ struct SimConfig {
     float spin = 0.0f;                 // Sim.h:766
     float hubble = 0.0f;               // Sim.h:196
     float velDispersion = 0.0f;        // Sim.h:263
+    // grid hydrodynamics (the reference's defaults are on; off here unless set)
+    bool pressureEnabled = false;      // Sim.h:319
+    float pressureK = 0.45f;           // Sim.h:320
+    bool coolingEnabled = false;       // Sim.h:327
+    float coolingRate = 0.08f;         // Sim.h:345
     // options of this build (no reference counterpart)
     int order = SD_ORDER_ROWMAJOR;     // SD_ORDER_TILED enables the fused deposit
     int integrator = SD_INT_KD;
@@ -71,6 +76,10 @@ struct SimConfig {
         c.spin = spin;
         c.hubble = hubble;
         c.vel_dispersion = velDispersion;
+        c.pressure_enabled = pressureEnabled ? 1 : 0;
+        c.pressure_k = pressureK;
+        c.cooling_enabled = coolingEnabled ? 1 : 0;
+        c.cooling_rate = coolingRate;
         return c;
     }
 };

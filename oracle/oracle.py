@@ -497,6 +497,83 @@ _ASTRO_C = np.array([[0.00, 0.00, 0.00], [0.05, 0.06, 0.19], [0.16, 0.14, 0.47],
 _ASTRO_S = np.array([0.00, 0.18, 0.38, 0.58, 0.76, 0.90, 1.00])
 
 
+# ---- grid hydrodynamics add-ons (doCooling, kPressure; Sim.cu:1212-1415, 3605-3868) ----
+
+def containing_cell(pos, G: int) -> np.ndarray:
+    """Flat index (z G + y) G + x of the containing cell, clamp((int)(p G), 0, G-1)
+    (kAccumCellVel, Sim.cu:1227-1230)."""
+    c = np.clip((np.asarray(pos, np.float32)[:, :3] * np.float32(G)).astype(np.int64), 0, G - 1)
+    return (c[:, 2] * G + c[:, 1]) * G + c[:, 0]
+
+
+def hydro_cool(pos, vel, G: int, k: float, pressure: bool):
+    """One cooling pass (kAccumCellVel + kCoolCell, Sim.cu:1212-1310) with sums in
+    float64: returns the cooled float32 velocities and, with pressure, the
+    dispersion grids (3, G^3) and their counts (G^3)."""
+    pos = np.asarray(pos, np.float32)
+    vel = np.array(vel, np.float32)
+    cells = G ** 3
+    live = (pos[:, 0] >= 0) & np.isfinite(vel[:, :3]).all(axis=1) & (vel[:, 3] >= -50)
+    c = containing_cell(pos, G)
+    sums = np.zeros((3, cells))
+    cnt = np.zeros(cells, np.int64)
+    for d in range(3):
+        np.add.at(sums[d], c[live], vel[live, d].astype(np.float64))
+    np.add.at(cnt, c[live], 1)
+    act = live & (cnt[c] >= 2)
+    inv = (np.float32(1.0) / cnt[c[act]].astype(np.float32))
+    dv = np.stack([sums[d][c[act]].astype(np.float32) * inv - vel[act, d] for d in range(3)], axis=1)
+    disp = np.zeros((3, cells))
+    dcnt = np.zeros(cells, np.int64)
+    if pressure:
+        for d in range(3):
+            np.add.at(disp[d], c[act], (dv[:, d] * dv[:, d]).astype(np.float64))
+        np.add.at(dcnt, c[act], 1)
+    gas = pos[act, 3] <= 0
+    idx = np.nonzero(act)[0][gas]
+    vel[idx, :3] = vel[idx, :3] + np.float32(k) * dv[gas]
+    return vel, disp, dcnt
+
+
+def pressure_field(disp, dcnt, G: int, pressure_k: float, periodic: bool = True) -> np.ndarray:
+    """kPressure (Sim.cu:1368-1400): -(disp_d[+1] - disp_d[-1]) G/2 k / count per
+    axis, clamped to +-5, zero where the count is zero; (G^3, 3) float32."""
+    d = np.asarray(disp, np.float64).reshape(3, G, G, G).astype(np.float32)
+    rho = np.asarray(dcnt).reshape(G, G, G).astype(np.float32)
+
+    def shift(a, axis, s):
+        if periodic:
+            return np.roll(a, -s, axis=axis)
+        idx = np.clip(np.arange(G) + s, 0, G - 1)
+        return np.take(a, idx, axis=axis)
+
+    h = np.where(rho > 0, np.float32(0.5) * np.float32(G) * np.float32(pressure_k) / np.where(rho > 0, rho, 1),
+                 0).astype(np.float32)
+    out = np.zeros((G, G, G, 3), np.float32)
+    for ax, axis in ((0, 2), (1, 1), (2, 0)):  # x is the last array axis
+        g = -(shift(d[ax], axis, 1) - shift(d[ax], axis, -1)) * h
+        out[..., ax] = np.clip(g, -5.0, 5.0)
+    out[rho < 1e-6] = 0
+    return out.reshape(-1, 3)
+
+
+def sample_field(field, pos, G: int, periodic: bool = True) -> np.ndarray:
+    """CIC sample of a (G^3, 3) field at the positions (sampleAcc, Sim.cu:614-629)."""
+    pos = np.asarray(pos, np.float64)
+    f = np.asarray(field, np.float64)
+    g = pos[:, :3] * G - 0.5
+    i0 = np.floor(g).astype(np.int64)
+    fr = g - i0
+    a = np.zeros((len(pos), 3))
+    for k in range(8):
+        o = np.array([k & 1, (k >> 1) & 1, (k >> 2) & 1])
+        c = i0 + o
+        c = (c & (G - 1)) if periodic else np.clip(c, 0, G - 1)
+        w = np.prod(np.where(o == 1, fr, 1 - fr), axis=1)
+        a += w[:, None] * f[(c[:, 2] * G + c[:, 1]) * G + c[:, 0]]
+    return a
+
+
 # ---- initial conditions of Sim::reset (Sim.cu:4160-4238) -------------------------
 
 PRESET_FILAMENT, PRESET_EMPTY = 0, 1

@@ -134,6 +134,21 @@ int ref_init_preset(void* h, int n, int G, int boundary, int preset, float dark_
     return Sim::failed() ? -2 : 0;
 }
 
+// Switch the grid hydrodynamics add-ons of a configured sim (a non-structural
+// reconfigure: the particles stay). Star ionisation is zeroed so pressure runs
+// alone, as star formation is off.
+int ref_set_hydro(void* h, int pressure, float pressure_k, int cooling, float cooling_rate) {
+    Sim* s = static_cast<Sim*>(h);
+    SimConfig c = s->config();
+    c.pressureEnabled = pressure != 0;
+    c.pressureK = pressure_k;
+    c.coolingEnabled = cooling != 0;
+    c.coolingRate = cooling_rate;
+    c.starIonizeK = 0.f;
+    s->reconfigure(c);
+    return Sim::failed() ? -2 : 0;
+}
+
 int ref_step(void* h) {
     static_cast<Sim*>(h)->step();
     return Sim::failed() ? -2 : 0;

@@ -44,6 +44,11 @@ class SdConfig(ctypes.Structure):
         ("spin", ctypes.c_float),
         ("hubble", ctypes.c_float),
         ("vel_dispersion", ctypes.c_float),
+        ("pressure_enabled", ctypes.c_int32),
+        ("pressure_k", ctypes.c_float),
+        ("cooling_enabled", ctypes.c_int32),
+        ("cooling_rate", ctypes.c_float),
+        ("reserved", ctypes.c_int32 * 8),
     ]
 
 

@@ -68,8 +68,10 @@ void drop_graphs(sd_ensemble* e) {
     e->graph[0] = e->graph[1] = nullptr;
 }
 
+// Scenes with the hydro add-ons (a cooling schedule tied to the step count) run
+// as solo simulations.
 bool graphable(const sd_sim* s) {
-    return s->configured && (s->cfg.sort_interval == 0 || s->cfg.sort_interval == 1);
+    return s->configured && (s->cfg.sort_interval == 0 || s->cfg.sort_interval == 1) && !hydro_on(s);
 }
 
 struct HostCounters {
@@ -102,7 +104,7 @@ int prepare_scenes(sd_ensemble* e, float dt) {
     for (auto& sl : e->scenes) {
         sd_sim* s = sl.sim;
         if (!graphable(s))
-            return fail(SD_E_STATE, "ensemble: scenes must sort every step or never");
+            return fail(SD_E_STATE, "ensemble: scenes must sort every step or never, without hydro add-ons");
         if (s->cfg.integrator == SD_INT_KDK && !s->lf_open) {
             if (int rc = do_step(s, dt, sort_due(s), false)) return rc;
         }

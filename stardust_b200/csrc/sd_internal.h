@@ -105,7 +105,7 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
                              double* mom_out, float* mean_out, cudaStream_t s, const float4* extra = nullptr,
                              int max_blocks = 0, const DiagRecord* diag = nullptr, int iso_S = 0,
-                             unsigned* tile_counts = nullptr, int count_bits = 0);
+                             unsigned* tile_counts = nullptr, int count_bits = 0, const float4* press = nullptr);
 // tile_counts: zeroed first-pass sort counts; the gather adds the digit (low
 // count_bits bits) of every key it writes to the row of the key's sort tile.
 // iso_S > 0: isolated boundary, potential box of side iso_S (= 2G), clamped sampling
@@ -121,6 +121,24 @@ int launch_max_speed(const float4* pos, const float4* vel, int n, const float* m
 int launch_energy(const float* phi, int G, const float4* pos, const float4* vel, int n, const float* mean_vel,
                   double* partials, double* out8, cudaStream_t s, int iso_S = 0);
 int launch_reduce_grid(const float* rho, size_t cells, int op, double* partials, double* out, cudaStream_t s);
+// Grid hydrodynamics add-ons (sd_hydro.cu): per-cell fixed-point sums for cooling
+// and the velocity dispersion, and the pressure acceleration grid (G^3 each).
+struct HydroGrids {
+    void* base = nullptr;
+    float4* acc = nullptr;              // pressure acceleration
+    long long* vsum[3] = {nullptr, nullptr, nullptr};
+    long long* disp[3] = {nullptr, nullptr, nullptr};
+    unsigned* cnt = nullptr;            // members of each cell
+    unsigned* dcnt = nullptr;           // members that entered the dispersion
+    int G = 0;
+};
+size_t hydro_bytes(int G);
+int hydro_alloc(HydroGrids& h, int G);
+void hydro_free(HydroGrids& h);
+int launch_pressure(const HydroGrids& h, int periodic, float pressure_k, cudaStream_t s);
+int launch_cooling(const HydroGrids& h, const float4* pos, float4* vel, int n, const float* mean, float rate,
+                   float dt, bool pressure, cudaStream_t s);
+
 // Sim::reset's placement (sd_scene.cu): preset, initial velocities, centre-of-mass stop.
 int launch_place_preset(float4* pos, float4* vel, int n, const sd_config& cfg, double* partials, double* out8,
                         float* mean, cudaStream_t s);

@@ -213,12 +213,38 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double* partials) {
 // ISO: isolated boundary (potential box of side S, clamped sampling, and the
 // reference's wall at [0.002, 0.998] that stops a particle and returns a quarter
 // of its speed, Sim.cu:895-903) instead of the periodic wrap.
-template <bool DIAG, bool ISO>
+// CIC sample of a G^3 float4 field at p (sampleAcc, Sim.cu:614-629): cell-centred
+// weights (wx wy) wz, corners wrapped (periodic) or clamped (isolated).
+template <bool ISO>
+__device__ __forceinline__ float3 sample_field(const float4* __restrict__ f, int G, float4 p) {
+    int ix, iy, iz;
+    float fx, fy, fz;
+    cic_axis(p.x, G, ix, fx);
+    cic_axis(p.y, G, iy, fy);
+    cic_axis(p.z, G, iz, fz);
+    float3 a = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int cx = cic_cell(ix + (k & 1), G, !ISO), cy = cic_cell(iy + ((k >> 1) & 1), G, !ISO),
+                  cz = cic_cell(iz + ((k >> 2) & 1), G, !ISO);
+        const float w = cic_weight(k, fx, fy, fz);
+        const float4 g = f[((size_t)cz * G + cy) * G + cx];
+        a.x = __fmaf_rn(g.x, w, a.x);
+        a.y = __fmaf_rn(g.y, w, a.y);
+        a.z = __fmaf_rn(g.z, w, a.z);
+    }
+    return a;
+}
+
+// PRESS: gas particles (pos.w <= 0, not dark matter) also take the CIC sample of
+// the pressure acceleration grid `press` (G^3; kIntegrate, Sim.cu:740-743).
+template <bool DIAG, bool ISO, bool PRESS>
 __global__ void __launch_bounds__(kGatherThreads, 3) k_gather_kick_drift(
     const float* __restrict__ phi, int G, float h, const float4* pos_in, const float4* vel_in,
     const int* __restrict__ perm, float4* pos_out, float4* vel_out, uint32_t* __restrict__ keys_out, int order, int n,
     float dt_kick, float dt_drift, float c2, const float* __restrict__ mean_vel, double* __restrict__ partials,
-    const float4* __restrict__ extra, int S, unsigned* __restrict__ tile_counts, int count_bits) {
+    const float4* __restrict__ extra, int S, unsigned* __restrict__ tile_counts, int count_bits,
+    const float4* __restrict__ press) {
     double sx = 0.0, sy = 0.0, sz = 0.0, cnt = 0.0, sv2 = 0.0, sphi = 0.0;
     const unsigned cmask = (1u << count_bits) - 1u;
     const float mx = mean_vel ? mean_vel[0] : 0.f, my = mean_vel ? mean_vel[1] : 0.f,
@@ -249,6 +275,12 @@ __global__ void __launch_bounds__(kGatherThreads, 3) k_gather_kick_drift(
                 a.x = __fadd_rn(a.x, e.x);
                 a.y = __fadd_rn(a.y, e.y);
                 a.z = __fadd_rn(a.z, e.z);
+            }
+            if (PRESS && p.w <= 0.f && v.w >= -50.f) {
+                const float3 pr = sample_field<ISO>(press, G, p);
+                a.x = __fadd_rn(a.x, pr.x);
+                a.y = __fadd_rn(a.y, pr.y);
+                a.z = __fadd_rn(a.z, pr.z);
             }
             v.x = __fmaf_rn(a.x, dt_kick, v.x);
             v.y = __fmaf_rn(a.y, dt_kick, v.y);
@@ -576,8 +608,8 @@ int gather_prepare(int device) {
     if (g_gather_wave[device] > 0) return SD_OK;
     int sms = 0, per_sm = 0, per_sm_diag = 0;
     if (SD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) ||
-        SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather_kick_drift<false, false>, kGatherThreads, 0)) ||
-        SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_diag, k_gather_kick_drift<true, false>, kGatherThreads, 0)))
+        SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather_kick_drift<false, false, false>, kGatherThreads, 0)) ||
+        SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_diag, k_gather_kick_drift<true, false, false>, kGatherThreads, 0)))
         return SD_E_CUDA;
     const int w = sms * (per_sm < per_sm_diag ? per_sm : per_sm_diag);
     g_gather_wave[device] = w > 0 ? w : kGatherMaxBlocks;
@@ -595,7 +627,7 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
                              double* mom_out, float* mean_out, cudaStream_t s, const float4* extra,
                              int max_blocks, const DiagRecord* diag, int iso_S, unsigned* tile_counts,
-                             int count_bits) {
+                             int count_bits, const float4* press) {
     if (n <= 0) return SD_OK;
     // particle records are read and written as float4
     if (((uintptr_t)pos_in | (uintptr_t)vel_in | (uintptr_t)pos_out | (uintptr_t)vel_out) & 15u)
@@ -605,17 +637,21 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
     const int cap = max_blocks > 0 ? max_blocks : gather_wave();
     if (blocks > cap) blocks = cap;
     const bool dg = diag && partials;
-#define SD_GATHER(D, I)                                                                                            \
-    k_gather_kick_drift<D, I><<<blocks, kGatherThreads, 0, s>>>(phi, G, h, pos_in, vel_in, perm, pos_out, vel_out, \
-                                                                keys_out, order, n, dt_kick, dt_drift, c2, mean_vel,  \
-                                                                partials, extra, iso_S, tile_counts, count_bits)
+#define SD_GATHER(D, I, P)                                                                                 \
+    k_gather_kick_drift<D, I, P><<<blocks, kGatherThreads, 0, s>>>(                                            \
+        phi, G, h, pos_in, vel_in, perm, pos_out, vel_out, keys_out, order, n, dt_kick, dt_drift, c2, mean_vel, \
+        partials, extra, iso_S, tile_counts, count_bits, press)
+#define SD_GATHER_P(D, I)        \
+    if (press) SD_GATHER(D, I, true); \
+    else SD_GATHER(D, I, false)
     if (iso_S) {
-        if (dg) SD_GATHER(true, true);
-        else SD_GATHER(false, true);
+        if (dg) SD_GATHER_P(true, true);
+        else SD_GATHER_P(false, true);
     } else {
-        if (dg) SD_GATHER(true, false);
-        else SD_GATHER(false, false);
+        if (dg) SD_GATHER_P(true, false);
+        else SD_GATHER_P(false, false);
     }
+#undef SD_GATHER_P
 #undef SD_GATHER
     SD_LAUNCHED(s);
     if (dg) {

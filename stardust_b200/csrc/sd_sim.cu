@@ -20,6 +20,7 @@
 #include <string.h>
 
 #include <atomic>
+#include <cmath>
 #include <mutex>
 #include <utility>
 #include <vector>
@@ -146,6 +147,7 @@ void free_buffers(sd_sim* s) {
     s->sort_ws_bytes = 0;
     free_dev(s->acc); free_dev(s->row_start); free_dev(s->spec); free_dev(s->phi); free_dev(s->rho);
     free_dev(s->green);
+    hydro_free(s->hydro);
     free_dev(s->partials); free_dev(s->mom); free_dev(s->mean);
     free_dev(s->mlp_out);
     free_dev(s->diag_rec);
@@ -253,7 +255,26 @@ int validate_config(const sd_config* c) {
     if (c->integrator != SD_INT_KD && c->integrator != SD_INT_KDK) return fail(SD_E_ARG, "config: bad integrator");
     if (c->units != SD_UNITS_REFERENCE && c->units != SD_UNITS_NEWTON) return fail(SD_E_ARG, "config: bad units");
     if (c->preset != SD_PRESET_FILAMENT && c->preset != SD_PRESET_EMPTY) return fail(SD_E_ARG, "config: bad preset");
+    if (!std::isfinite(c->pressure_k) || !std::isfinite(c->cooling_rate))
+        return fail(SD_E_ARG, "config: non-finite pressure_k or cooling_rate");
     return SD_OK;
+}
+
+bool hydro_on(const sd_sim* s) { return s->cfg.pressure_enabled || (s->cfg.cooling_enabled && s->cfg.cooling_rate > 0.f); }
+
+// doCooling's period (Sim.cu:3737): every 2 steps with pressure, every 8 without.
+int cooling_period(const sd_sim* s) { return s->cfg.pressure_enabled ? 2 : 8; }
+
+// The hydro grids exist while either add-on is on (zeroed when made, as the
+// reference's are at allocation); toggling does not touch the particles.
+int ensure_hydro(sd_sim* s) {
+    if (!hydro_on(s)) {
+        hydro_free(s->hydro);
+        return SD_OK;
+    }
+    if (s->hydro.base && s->hydro.G == s->G) return SD_OK;
+    hydro_free(s->hydro);
+    return hydro_alloc(s->hydro, s->G);
 }
 
 // placeInitial + reset's velocity and centre-of-mass passes (Sim.cu:3635-3649,
@@ -396,6 +417,21 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     if (keep) s->rho_valid = true;
     if (timed) cudaEventRecord(s->ev[3], s->stream);
     if (s->mlp_on && (rc = mlp_correction(s, perm))) return sim_error(s, rc);
+    // Grid hydrodynamics (computeAccel's kPressure, then doCooling, Sim.cu:3620-3631,
+    // 3732-3868): the pressure field comes from the dispersion of the last cooling
+    // step; a cooling step then corrects and cools the velocities in place, so the
+    // gather reads them without the pending mean.
+    const float* mean_in = s->mean;
+    const bool press = s->hydro.base && s->cfg.pressure_enabled;
+    if (press && (rc = launch_pressure(s->hydro, isolated(s) ? 0 : 1, s->cfg.pressure_k, s->stream)))
+        return sim_error(s, rc);
+    if (s->hydro.base && (s->step_count % cooling_period(s)) == 0) {
+        const float rate = (s->cfg.cooling_enabled && s->cfg.cooling_rate > 0.f) ? s->cfg.cooling_rate : 0.f;
+        if ((rc = launch_cooling(s->hydro, s->pos, s->vel, s->N, s->mean, rate, dt * (float)cooling_period(s),
+                                 s->cfg.pressure_enabled != 0, s->stream)))
+            return sim_error(s, rc);
+        mean_in = nullptr;
+    }
     const float c2 = light_speed_sq(s->cfg.length_scale, s->cfg.time_unit_scale);
     // The mean written last step is read here as the correction for the loaded
     // velocities; the finalize kernel then overwrites it with this step's mean.
@@ -408,11 +444,11 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     diag.cap = kDiagCap;
     diag.mass = 1.0 / (double)(s->N > 0 ? s->N : 1);
     rc = launch_gather_kick_drift(s->phi, s->G, pot_scale_of(s), s->pos, s->vel, perm, pos_out, vel_out, s->keys,
-                                  s->cfg.order, s->N, dt_kick, dt_drift, c2, s->mean, s->partials, s->mom, s->mean,
+                                  s->cfg.order, s->N, dt_kick, dt_drift, c2, mean_in, s->partials, s->mom, s->mean,
                                   s->stream, s->mlp_on ? s->mlp_out : nullptr, s->gather_blocks,
                                   s->cfg.diagnostics ? &diag : nullptr, isolated(s) ? 2 * s->G : 0,
                                   sort ? sort_first_counts(s->sort_ws) : nullptr,
-                                  sort_digit_bits(key_bits_for(s->G, s->cfg.order)));
+                                  sort_digit_bits(key_bits_for(s->G, s->cfg.order)), press ? s->hydro.acc : nullptr);
     if (rc) return sim_error(s, rc);
     if (perm) {
         std::swap(s->pos, s->pos2);
@@ -458,6 +494,7 @@ int reconfigure(sd_sim* s, const sd_config* c) {
     if (!structural) {
         if (s->graph) cudaGraphExecDestroy(s->graph);
         s->graph = nullptr;
+        if ((rc = ensure_hydro(s))) return rc;
         if (!soft_changed) return SD_OK;
         rc = poisson_plan_build(s->plan, box_of(s->G, s->cfg.boundary), s->cfg.softening_cells);
         if (!rc && isolated(s))
@@ -468,6 +505,7 @@ int reconfigure(sd_sim* s, const sd_config* c) {
     s->G = G;
     rc = allocate(s);
     if (rc) return rc;
+    if ((rc = ensure_hydro(s))) return rc;
     // the reference's init / structural reconfigure ends in reset() (Sim.cu:4151)
     if ((rc = place_initial(s))) return sim_error(s, rc);
     s->sim_time = 0.0;
@@ -548,6 +586,8 @@ int sd_config_default(sd_config* c) {
     c->diagnostics = 0;
     c->keep_density = 1;
     c->preset = SD_PRESET_FILAMENT;  // Sim.h:277
+    c->pressure_k = 0.45f;           // Sim.h:320 (pressure itself off: the PM path)
+    c->cooling_rate = 0.08f;         // Sim.h:345 (cooling itself off)
     return SD_OK;
 }
 
@@ -790,7 +830,10 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
     if (!s || !s->configured) return fail(SD_E_STATE, "steps: not initialised");
     if (nsteps < 0) return fail(SD_E_ARG, "steps: negative count");
     DeviceGuard g(s->device);
-    const bool graphable = s->cfg.sort_interval == 0 || s->cfg.sort_interval == 1;
+    // A two-step graph repeats the cooling schedule only when its period is 2.
+    const bool graphable = (s->cfg.sort_interval == 0 || s->cfg.sort_interval == 1) &&
+                           (!hydro_on(s) || cooling_period(s) == 2);
+    const int phase = hydro_on(s) ? (s->step_count & 1) : 0;
     int done = 0;
     // leapfrog opening kick and odd counts run eagerly
     while (done < nsteps && (!graphable || (s->cfg.integrator == SD_INT_KDK && !s->lf_open))) {
@@ -809,7 +852,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
     // A captured graph covers two steps so the pos/pos2 ping-pong returns to the
     // same buffers; it is rebuilt when dt changes or the particles sit in the
     // other buffer of the pair.
-    if (!s->graph || s->graph_dt != dt || s->graph_pos != s->pos) {
+    if (!s->graph || s->graph_dt != dt || s->graph_pos != s->pos || s->graph_phase != phase) {
         if (s->graph) cudaGraphExecDestroy(s->graph);
         s->graph = nullptr;
         cudaGraph_t graph = nullptr;
@@ -846,6 +889,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
         if (SD_CUDA(e)) return sim_error(s, SD_E_CUDA);
         s->graph_dt = dt;
         s->graph_pos = s->pos;
+        s->graph_phase = phase;
     }
     while (nsteps - done >= 2) {
         if (SD_CUDA(cudaGraphLaunch(s->graph, s->stream))) return sim_error(s, SD_E_CUDA);

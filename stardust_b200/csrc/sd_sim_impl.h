@@ -31,6 +31,8 @@ struct sd_sim {
     float* phi = nullptr;
     float* rho = nullptr;        // kept density (keep_density)
     float* green = nullptr;      // isolated boundary: real Green spectrum of the 2G box
+    sd::HydroGrids hydro;        // pressure / cooling grids, allocated while either is on
+    int graph_phase = 0;         // step count parity the captured graph was made at (hydro)
     double* partials = nullptr;  // gather / energy / reduction partials
     size_t partials_count = 0;
     double* mom = nullptr;       // 8 doubles: momentum sums of the last step, energy results
@@ -86,6 +88,8 @@ struct DeviceGuard {
 int sim_error(sd_sim* s, int rc);
 bool sort_due(const sd_sim* s);
 int ensure_sort_inputs(sd_sim* s);
+bool hydro_on(const sd_sim* s);
+int cooling_period(const sd_sim* s);
 int key_bits_for(int G, int order);
 // One step of one scene on s->stream (no host synchronisation; capturable).
 int do_step(sd_sim* s, float dt, bool sort, bool timed);

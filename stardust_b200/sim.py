@@ -46,6 +46,11 @@ class SimConfig:
     spin: float = 0.0                    # Sim.h:766
     hubble: float = 0.0                  # Sim.h:196
     vel_dispersion: float = 0.0          # Sim.h:263
+    # grid hydrodynamics add-ons (off unless set; the reference's defaults are on)
+    pressure_enabled: int = 0            # Sim.h:319
+    pressure_k: float = 0.45             # Sim.h:320
+    cooling_enabled: int = 0             # Sim.h:327
+    cooling_rate: float = 0.08           # Sim.h:345
 
     def to_c(self) -> L.SdConfig:
         c = L.SdConfig()

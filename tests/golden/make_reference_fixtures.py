@@ -43,6 +43,7 @@ def load_ref():
     L.ref_density.argtypes = [P, P, I]
     L.ref_timings.argtypes = [P, P]
     L.ref_init_preset.argtypes = [P, I, I, I, I, F, F, F, F, F]
+    L.ref_set_hydro.argtypes = [P, I, F, I, F]
     L.ref_fail_message.restype = ctypes.c_char_p
     L.ref_sim_time.argtypes = [P]
     L.ref_sim_time.restype = ctypes.c_double
@@ -98,6 +99,21 @@ def cases():
     yield "isolated_g32", p, v, 32, 32.0, 1.5, 1e-3, 0
 
 
+def hydro_cases():
+    """Steps with pressure and cooling on: name, particles, grid, gravity, softening,
+    dt, steps, pressure_k, cooling_rate."""
+    rng = np.random.default_rng(777)
+    n = 6000
+    c = rng.random((5, 3))
+    xyz = (c[rng.integers(0, 5, n)] + rng.normal(scale=0.06, size=(n, 3))) % 1.0
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = xyz
+    pos[:, :3][pos[:, :3] >= 1.0] = 0.0
+    vel = np.zeros((n, 4), np.float32)
+    vel[:, :3] = rng.normal(scale=0.3, size=(n, 3))
+    yield "hydro_g16", pos, vel, 16, float(4 * np.pi * 16 ** 3), 1.0, 1e-3, 3, 0.45, 0.08
+
+
 def preset_cases():
     # name, n, G, preset, dark fraction, shrink, spin, hubble, dispersion
     yield "filament_all", 6000, 32, 0, 0.25, 0.9, 0.7, 0.4, 0.05
@@ -108,6 +124,37 @@ def preset_cases():
 def main(outdir: str) -> int:
     os.makedirs(outdir, exist_ok=True)
     L = load_ref()
+    for name, pos, vel, G, grav, soft, dt, steps, pk, rate in hydro_cases():
+        pos = np.ascontiguousarray(pos, np.float32)
+        vel = np.ascontiguousarray(vel, np.float32)
+        vel[:, 3] = np.arange(len(vel), dtype=np.float32)  # ids (>= 0: gas, not dark matter)
+        n = len(pos)
+        h = L.ref_create()
+        try:
+            with tempfile.TemporaryDirectory() as tmp:
+                path = os.path.join(tmp, "in.stardust").encode()
+                ts = np.float32(dt) / np.float32(0.0016)
+                if L.ref_load_b(h, pos.ctypes.data, vel.ctypes.data, n, G, grav, soft, float(ts), 1, 1, path) != 0:
+                    raise RuntimeError(f"ref_load failed: {L.ref_fail_message()}")
+            if L.ref_set_hydro(h, 1, pk, 1, rate) != 0:
+                raise RuntimeError(f"ref_set_hydro failed: {L.ref_fail_message()}")
+            ps, vs, dts = [], [], []
+            for _ in range(steps):
+                if L.ref_step(h) != 0:
+                    raise RuntimeError(f"ref_step failed: {L.ref_fail_message()}")
+                p1, v1 = np.empty_like(pos), np.empty_like(vel)
+                L.ref_get(h, p1.ctypes.data, v1.ctypes.data, n)
+                t = np.empty(6, np.float32)
+                L.ref_timings(h, t.ctypes.data)
+                ps.append(p1)
+                vs.append(v1)
+                dts.append(t[4])
+        finally:
+            L.ref_destroy(h)
+        np.savez_compressed(os.path.join(outdir, f"reference_{name}.npz"), pos_in=pos, vel_in=vel,
+                            pos_steps=np.stack(ps), vel_steps=np.stack(vs), dt_used=np.array(dts, np.float32),
+                            grid=G, gravity=grav, soft=soft, pressure_k=np.float32(pk), cooling_rate=np.float32(rate))
+        print(name, "dt_used", dts)
     for name, n, G, preset, dark, shrink, spin, hubble, disp in preset_cases():
         h = L.ref_create()
         try:

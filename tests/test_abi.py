@@ -29,7 +29,7 @@ def test_every_declared_symbol_is_exported(lib):
 
 
 def test_struct_sizes_match_header(lib):
-    assert ctypes.sizeof(L.SdConfig) == 20 * 4
+    assert ctypes.sizeof(L.SdConfig) == 32 * 4
     assert ctypes.sizeof(L.SdTimings) == 16 * 4
 
 

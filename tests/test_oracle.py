@@ -93,9 +93,9 @@ def test_pm_accel_f64_two_particles_antisymmetric(oracle):
 
 
 def _golden_files(isolated=False):
-    """One-step fixtures (the preset fixtures hold initial conditions only)."""
+    """One-step plain-PM fixtures (not the preset and hydro fixtures)."""
     files = sorted(glob.glob(os.path.join(GOLDEN, "reference_*.npz")))
-    files = [f for f in files if not os.path.basename(f).startswith("reference_preset_")]
+    files = [f for f in files if not os.path.basename(f).startswith(("reference_preset_", "reference_hydro_"))]
     return [f for f in files if ("isolated" in os.path.basename(f)) == isolated]
 
 
