@@ -226,9 +226,9 @@ def run_ours(args, rank, world):
     e2e_steps = max(2, min(args.steps, 10))
 
     def e2e_step():
-        L.check(lib.sd_set_particles(sim.handle, hp.data_ptr(), hv.data_ptr(), n, L.SD_HOST), "set")
-        L.check(lib.sd_step(sim.handle, float(dt)), "step")
-        L.check(lib.sd_get_particles(sim.handle, op.data_ptr(), ov.data_ptr(), n, L.SD_HOST), "get")
+        # the offload call: host pos/vel in, one step, host pos/vel out (pinned buffers)
+        L.check(lib.sd_step_host(sim.handle, hp.data_ptr(), hv.data_ptr(), n, float(dt), op.data_ptr(),
+                                 ov.data_ptr()), "step_host")
 
     e2e_step()
     barrier()
@@ -282,7 +282,7 @@ def run_ours(args, rank, world):
         "phase_ms": phase_ms,
         "e2e": {"value": world * n / (e2e_ms * 1e-3), "unit": "particle-steps/s",
                 "h2d_bytes_per_step": 2 * 16 * n, "d2h_bytes_per_step": 2 * 16 * n,
-                "path": "sd_set_particles(host) + sd_step + sd_get_particles(host), pinned"},
+                "path": "sd_step_host: pinned host pos/vel in, one step, host pos/vel out"},
         "gpu_launches": int(launches),
         "clocks": clock_info,
         "diagnostics": diag,

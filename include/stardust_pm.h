@@ -199,6 +199,13 @@ int sd_step(sd_sim* sim, float dt);
 /* The reference's step(): dt = 0.0016*dtScaleFor(time_scale) clamped to
  * 0.8*cell/vmax (Sim.cu:4255-4269); blocks for the vmax read like the reference. */
 int sd_step_auto(sd_sim* sim);
+/* One offload step on host buffers: the same as sd_set_particles(pos_in, vel_in,
+ * n, SD_HOST) + sd_step(dt) + sd_get_particles(pos_out, vel_out, n, SD_HOST), with
+ * the velocity upload overlapping the sort, deposit and Poisson solve and the
+ * position download overlapping the momentum correction. Synchronous: returns
+ * when the outputs are written. Use pinned host memory for full copy speed. */
+int sd_step_host(sd_sim* sim, const float* pos_in, const float* vel_in, int n, float dt, float* pos_out,
+                 float* vel_out);
 /* nsteps fixed-dt steps; replays a captured CUDA graph after the first call. */
 int sd_steps(sd_sim* sim, float dt, int nsteps);
 /* Leapfrog: apply the closing half kick so velocities are synchronous with

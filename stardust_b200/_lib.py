@@ -119,6 +119,7 @@ SIGNATURES = [
     ("sd_get_accel", _I, [_P, _P, _I, _I]),
     ("sd_step", _I, [_P, _F]),
     ("sd_step_auto", _I, [_P]),
+    ("sd_step_host", _I, [_P, _P, _P, _I, _F, _P, _P]),
     ("sd_steps", _I, [_P, _F, _I]),
     ("sd_synchronize", _I, [_P]),
     ("sd_sort_only", _I, [_P, _P, _I]),

@@ -423,6 +423,12 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     // gather reads them without the pending mean.
     const float* mean_in = s->mean;
     const bool press = s->hydro.base && s->cfg.pressure_enabled;
+    // velocities still arriving on the offload stream (sd_step_host): nothing
+    // before this point reads them
+    if (s->vel_wait) {
+        if (SD_CUDA(cudaStreamWaitEvent(s->stream, s->vel_wait, 0))) return sim_error(s, SD_E_CUDA);
+        s->vel_wait = nullptr;
+    }
     if (press && (rc = launch_pressure(s->hydro, isolated(s) ? 0 : 1, s->cfg.pressure_k, s->stream)))
         return sim_error(s, rc);
     if (s->hydro.base && (s->step_count % cooling_period(s)) == 0) {
@@ -634,6 +640,12 @@ int sd_destroy(sd_sim* s) {
         if (e) cudaEventDestroy(e);
     for (auto& e : s->pev)
         if (e) cudaEventDestroy(e);
+    for (auto& e : s->io_ev)
+        if (e) cudaEventDestroy(e);
+    if (s->io_stream) {
+        cudaStreamSynchronize(s->io_stream);
+        cudaStreamDestroy(s->io_stream);
+    }
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return SD_OK;
@@ -803,6 +815,57 @@ int sd_step(sd_sim* s, float dt) {
     s->tm.dt_used = dt;
     s->tm.steps = 1;
     return SD_OK;
+}
+
+int sd_step_host(sd_sim* s, const float* pos_in, const float* vel_in, int n, float dt, float* pos_out,
+                 float* vel_out) {
+    if (!s || !s->configured) return fail(SD_E_STATE, "step_host: not initialised");
+    if (!pos_in || !vel_in || !pos_out || !vel_out || n < 0 || n > s->N)
+        return fail(SD_E_ARG, "step_host: bad arguments (n=%d)", n);
+    DeviceGuard g(s->device);
+    if (!s->io_stream) {
+        if (SD_CUDA(cudaStreamCreateWithFlags(&s->io_stream, cudaStreamNonBlocking))) return SD_E_CUDA;
+        for (auto& e : s->io_ev)
+            if (SD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming))) return SD_E_CUDA;
+    }
+    const size_t bytes = sizeof(float4) * (size_t)n;
+    cudaStream_t st = s->stream, io = s->io_stream;
+    // Inputs: the positions first, at the link's full speed, on the handle's
+    // stream; then the velocities on the offload stream while the step's sort,
+    // deposit and Poisson solve run. The first kernel that reads velocities waits.
+    int rc = SD_CUDA(cudaMemcpyAsync(s->pos, pos_in, bytes, cudaMemcpyHostToDevice, st));
+    if (!rc) rc = SD_CUDA(cudaEventRecord(s->io_ev[0], st));
+    if (!rc) rc = SD_CUDA(cudaStreamWaitEvent(io, s->io_ev[0], 0));
+    if (!rc) rc = SD_CUDA(cudaMemcpyAsync(s->vel, vel_in, bytes, cudaMemcpyHostToDevice, io));
+    if (!rc) rc = SD_CUDA(cudaEventRecord(s->io_ev[1], io));
+    if (!rc) rc = launch_hide_range(s->pos, s->vel, n, s->N, st);  // slots >= n: disjoint from the copy
+    if (!rc && SD_CUDA(cudaMemsetAsync(s->mean, 0, sizeof(float) * 4, st))) rc = SD_E_CUDA;
+    if (rc) return sim_error(s, rc);
+    s->active = n;
+    s->mean_pending = false;
+    s->lf_open = false;
+    s->rho_valid = false;
+    s->keys_valid = false;
+    s->vel_wait = s->io_ev[1];
+    rc = do_step(s, dt, sort_due(s), true);
+    if (s->vel_wait) {  // a step that read no velocity still owes the wait
+        if (!rc) rc = SD_CUDA(cudaStreamWaitEvent(st, s->vel_wait, 0));
+        s->vel_wait = nullptr;
+    }
+    if (rc) return rc;
+    s->tm.dt_used = dt;
+    s->tm.steps = 1;
+    // Outputs: the positions leave on the offload stream while the handle's stream
+    // applies the pending momentum correction to the velocities, which follow
+    // (the two downloads share the link).
+    rc = SD_CUDA(cudaEventRecord(s->io_ev[0], st));
+    if (!rc) rc = SD_CUDA(cudaStreamWaitEvent(io, s->io_ev[0], 0));
+    if (!rc) rc = SD_CUDA(cudaMemcpyAsync(pos_out, s->pos, bytes, cudaMemcpyDeviceToHost, io));
+    if (!rc) rc = materialize(s);
+    if (!rc) rc = SD_CUDA(cudaMemcpyAsync(vel_out, s->vel, bytes, cudaMemcpyDeviceToHost, st));
+    if (!rc) rc = SD_CUDA(cudaStreamSynchronize(io));
+    if (!rc) rc = SD_CUDA(cudaStreamSynchronize(st));
+    return rc ? sim_error(s, rc) : SD_OK;
 }
 
 int sd_step_auto(sd_sim* s) {

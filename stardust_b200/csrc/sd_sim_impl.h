@@ -50,6 +50,11 @@ struct sd_sim {
     // timings of the last eager step: ev[0..4] phase bounds, pev[0..3] after Poisson passes A-D
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t pev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // host offload step (sd_step_host): a second stream for the copies that overlap
+    // the step, its two events, and the event the step's first velocity read waits on
+    cudaStream_t io_stream = nullptr;
+    cudaEvent_t io_ev[2] = {nullptr, nullptr};
+    cudaEvent_t vel_wait = nullptr;
     bool ev_valid = false;
     sd_timings tm{};
     sd_diagnostics diag{};

@@ -210,6 +210,20 @@ class Sim:
         set_correction(self, correction)
 
     # ---- stepping -----------------------------------------------------------------
+    def step_host(self, pos, vel, dt: float, out=None):
+        """One offload step on host arrays (sd_step_host): upload, step, download.
+        ``pos``/``vel``: float32 (n, 4) numpy arrays or CPU tensors (pinned for full
+        copy speed); ``out``: optional (pos, vel) arrays to write. Returns them."""
+        def ptr(a):
+            return a.data_ptr() if hasattr(a, "data_ptr") else _host_f4(a).ctypes.data
+
+        n = int(pos.shape[0])
+        if out is None:
+            out = (np.empty((n, 4), np.float32), np.empty((n, 4), np.float32))
+        L.check(L.lib().sd_step_host(self._h, ptr(pos), ptr(vel), n, float(dt), ptr(out[0]), ptr(out[1])),
+                "sd_step_host")
+        return out
+
     def step(self, dt: float | None = None) -> None:
         """``step()`` is the reference's CFL-clamped step; ``step(dt)`` advances by dt."""
         if dt is None:

@@ -307,3 +307,25 @@ def test_per_step_diagnostics_record_energy_and_momentum(cuda):
         assert np.array_equal(h[:, 0], np.arange(11))
         e = h[:, 1] + h[:, 2]
         assert np.abs(e - e[0]).max() <= 1e-2 * abs(h[0, 2])
+
+
+@pytest.mark.parametrize("order,diag", [(L.SD_ORDER_TILED, 1), (L.SD_ORDER_ROWMAJOR, 0)])
+def test_step_host_equals_set_step_get(cuda, order, diag):
+    """sd_step_host overlaps its copies with the step; the result is that of
+    set_particles + step + get_particles, bit for bit (also with n below capacity)."""
+    G, N, n = 32, 70_000, 65_000
+    outs = []
+    for mode in ("separate", "host"):
+        with make_sim(cuda, N, G, gravity=300.0, softening_cells=1.0, order=order, diagnostics=diag) as s:
+            for k in range(3):
+                pos, vel = random_particles(n, 40 + k, clustered=True)
+                if mode == "separate":
+                    s.set_particles(pos, vel)
+                    s.step(1e-3)
+                    p, v = s.get_particles(n)
+                else:
+                    p, v = s.step_host(pos, vel, 1e-3)
+                outs.append((p, v))
+    for (a, b), (c, d) in zip(outs[:3], outs[3:]):
+        assert np.array_equal(a.view(np.int32), c.view(np.int32))
+        assert np.array_equal(b.view(np.int32), d.view(np.int32))
