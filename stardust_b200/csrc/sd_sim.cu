@@ -840,7 +840,13 @@ int sd_step_host(sd_sim* s, const float* pos_in, const float* vel_in, int n, flo
     if (!rc) rc = SD_CUDA(cudaEventRecord(s->io_ev[1], io));
     if (!rc) rc = launch_hide_range(s->pos, s->vel, n, s->N, st);  // slots >= n: disjoint from the copy
     if (!rc && SD_CUDA(cudaMemsetAsync(s->mean, 0, sizeof(float) * 4, st))) rc = SD_E_CUDA;
-    if (rc) return sim_error(s, rc);
+    // on any failure the call returns only after its copies stopped reading the caller's buffers
+    auto drain = [&](int code) {
+        cudaStreamSynchronize(io);
+        cudaStreamSynchronize(st);
+        return sim_error(s, code);
+    };
+    if (rc) return drain(rc);
     s->active = n;
     s->mean_pending = false;
     s->lf_open = false;
@@ -852,7 +858,7 @@ int sd_step_host(sd_sim* s, const float* pos_in, const float* vel_in, int n, flo
         if (!rc) rc = SD_CUDA(cudaStreamWaitEvent(st, s->vel_wait, 0));
         s->vel_wait = nullptr;
     }
-    if (rc) return rc;
+    if (rc) return drain(rc);
     s->tm.dt_used = dt;
     s->tm.steps = 1;
     // Outputs: the positions leave on the offload stream while the handle's stream
@@ -863,9 +869,9 @@ int sd_step_host(sd_sim* s, const float* pos_in, const float* vel_in, int n, flo
     if (!rc) rc = SD_CUDA(cudaMemcpyAsync(pos_out, s->pos, bytes, cudaMemcpyDeviceToHost, io));
     if (!rc) rc = materialize(s);
     if (!rc) rc = SD_CUDA(cudaMemcpyAsync(vel_out, s->vel, bytes, cudaMemcpyDeviceToHost, st));
-    if (!rc) rc = SD_CUDA(cudaStreamSynchronize(io));
-    if (!rc) rc = SD_CUDA(cudaStreamSynchronize(st));
-    return rc ? sim_error(s, rc) : SD_OK;
+    if (rc) return drain(rc);
+    if ((rc = SD_CUDA(cudaStreamSynchronize(io))) || (rc = SD_CUDA(cudaStreamSynchronize(st)))) return drain(rc);
+    return SD_OK;
 }
 
 int sd_step_auto(sd_sim* s) {

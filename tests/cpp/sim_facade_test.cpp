@@ -4,6 +4,7 @@
 // (stardust_sim.hpp) so that App-style code is shown to build and run
 // unchanged. Scenes are generated here (the reference's presets are not part of
 // the PM path) and loaded with setParticles. Exit status 0 = all checks passed.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -176,6 +177,32 @@ static void test_state_round_trip(const std::string& dir) {
           "particles survive a save/load round trip byte for byte", fmt("active %g of %g (%g)", b.activeCount(), cfg.particleCount, 0));
 }
 
+static void test_init_lays_down_the_preset() {
+    std::printf("[7] init / reset lay down the Filament preset (Sim::reset)\n");
+    Sim sim;
+    SimConfig cfg;
+    cfg.particleCount = 30000;
+    cfg.gridSize = 32;
+    cfg.spin = 0.5f;  // the reference's defaults otherwise: Filament, no shrink
+    sim.init(cfg);
+    std::vector<float> p(4 * (size_t)cfg.particleCount), v(p.size());
+    sim.getParticles(p.data(), v.data(), cfg.particleCount);
+    double rmax = 0.0, px = 0.0;
+    for (int i = 0; i < cfg.particleCount; ++i) {
+        const double dx = p[4 * i] - 0.5, dy = p[4 * i + 1] - 0.5, dz = p[4 * i + 2] - 0.5;
+        rmax = std::max(rmax, std::sqrt(dx * dx + dy * dy + dz * dz));
+        px += v[4 * i];
+    }
+    sim.step(1e-3f);
+    sim.reset();
+    std::vector<float> q(p.size()), w(p.size());
+    sim.getParticles(q.data(), w.data(), cfg.particleCount);
+    check(sim.activeCount() == cfg.particleCount && rmax <= 0.5 + 1e-6 && std::fabs(px) < 1e-2 * cfg.particleCount &&
+              q == p && w == v && sim.simTime() == 0.0,
+          "every slot filled inside the ball, momentum stopped, reset repeats it",
+          fmt("active %g  r_max %.6f  sum vx %.3g", (double)sim.activeCount(), rmax, px));
+}
+
 static void test_sticky_failure() {
     std::printf("[6] sticky failure flag\n");
     sd_clear_error();
@@ -201,6 +228,7 @@ int main(int argc, char** argv) {
     test_long_run();
     test_periodic_softening();
     test_state_round_trip(dir);
+    test_init_lays_down_the_preset();
     test_sticky_failure();
     std::printf("%d failure(s)\n", g_failures);
     return g_failures == 0 ? 0 : 1;
