@@ -103,7 +103,9 @@ typedef struct sd_config {
     float pressure_k;            /* SimConfig::pressureK (Sim.h:320), default 0.45 */
     int32_t cooling_enabled;     /* SimConfig::coolingEnabled (Sim.h:327) */
     float cooling_rate;          /* SimConfig::coolingRate (Sim.h:345), default 0.08 */
-    int32_t reserved[8];
+    int32_t full_sort;           /* 1: always the full radix sort; 0: a step after a sorted step merges
+                                    the few keys that changed into the rest (tiled order, periodic) */
+    int32_t reserved[7];
 } sd_config;
 
 /* SimConfig::preset (Preset, Sim.h:14-17) */

@@ -48,7 +48,8 @@ class SdConfig(ctypes.Structure):
         ("pressure_k", ctypes.c_float),
         ("cooling_enabled", ctypes.c_int32),
         ("cooling_rate", ctypes.c_float),
-        ("reserved", ctypes.c_int32 * 8),
+        ("full_sort", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 7),
     ]
 
 

@@ -307,6 +307,7 @@ int sd_ensemble_add(sd_ensemble* e, const sd_config* cfg, const float* pos, cons
     DeviceGuard g(e->device);
     sd_sim* s = nullptr;
     int rc = sd_create(&s, e->device);
+    if (!rc) s->allow_incr = false;  // scenes sort in full: one graph per step, no per-scene merge state
     if (!rc) rc = sd_init(s, cfg);
     if (!rc && pos) rc = sd_set_particles(s, pos, vel, n, where);
     if (!rc && !graphable(s))

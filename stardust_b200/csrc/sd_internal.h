@@ -26,7 +26,10 @@ int launch_cell_keys(const float4* pos, int n, int G, int order, uint32_t* keys,
 size_t sort_workspace_bytes(int n);
 int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t* keys_out, int32_t* vals_out,
                       uint32_t* keys_tmp, int32_t* vals_tmp, int n, int key_bits, void* ws, size_t ws_bytes,
-                      cudaStream_t s, bool ws_zeroed = false, bool first_counts_ready = false);
+                      cudaStream_t s, bool ws_zeroed = false, bool first_counts_ready = false,
+                      const int* n_dev = nullptr);
+// n_dev: the key count lives in device memory (made by an earlier kernel); n is
+// then the capacity the grids are sized for, and keys past the count are ignored.
 // ws_zeroed: the workspace's count buffers are zero, as every sort leaves them.
 // first_counts_ready: the first digit pass's tile counts are already in the
 // workspace (launch_sort_first_counts, or added by the gather that wrote the keys).
@@ -105,7 +108,11 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
                              double* mom_out, float* mean_out, cudaStream_t s, const float4* extra = nullptr,
                              int max_blocks = 0, const DiagRecord* diag = nullptr, int iso_S = 0,
-                             unsigned* tile_counts = nullptr, int count_bits = 0, const float4* press = nullptr);
+                             unsigned* tile_counts = nullptr, int count_bits = 0, const float4* press = nullptr,
+                             unsigned* chg_words = nullptr);
+// chg_words: zeroed change bits (one per output) for the next step's merge sort
+// (sd_resort.cu); a bit is set where the key written differs from the key of the
+// step-start position.
 // tile_counts: zeroed first-pass sort counts; the gather adds the digit (low
 // count_bits bits) of every key it writes to the row of the key's sort tile.
 // iso_S > 0: isolated boundary, potential box of side iso_S (= 2G), clamped sampling
@@ -121,6 +128,28 @@ int launch_max_speed(const float4* pos, const float4* vel, int n, const float* m
 int launch_energy(const float* phi, int G, const float4* pos, const float4* vel, int n, const float* mean_vel,
                   double* partials, double* out8, cudaStream_t s, int iso_S = 0);
 int launch_reduce_grid(const float* rho, size_t cells, int op, double* partials, double* out, cudaStream_t s);
+// The step's sort as a merge of the unchanged and the changed keys (sd_resort.cu).
+struct ResortBufs {
+    unsigned* words = nullptr;      // change bits, one per position (zero between uses)
+    unsigned* word_pre = nullptr;   // changed positions before each word
+    unsigned* chunk_cnt = nullptr;  // changed positions per chunk of words
+    int* c_rows = nullptr;          // row table of the sorted changed keys
+    int* n_changed = nullptr;
+    // the changed keys and positions, compacted, then radix-sorted (capacity n each)
+    uint32_t *ck_in = nullptr, *ck_out = nullptr, *ck_tmp = nullptr;
+    int32_t *ci_in = nullptr, *ci_out = nullptr, *ci_tmp = nullptr;
+};
+size_t resort_bytes(int n, int G);
+size_t resort_words(int n);  // entries of the change-bit buffer (padded; the padding stays zero)
+// Lays out resort_bytes(n, G) at base; ck_in, ci_in and ck_tmp are the three
+// spare arrays of n entries given (scratch of the full sort, idle during a merge).
+ResortBufs resort_layout(void* base, int n, int G, uint32_t* spare_k0, int32_t* spare_v0, uint32_t* spare_k1);
+// keys: the new key of every position, positions sorted by their old keys, whose
+// row table is row_start; writes the stable sort's permutation to vals_out and
+// the new keys' row table over row_start.
+int launch_resort(const ResortBufs& r, const uint32_t* keys, int n, int G, int key_bits, int* row_start,
+                  int32_t* vals_out, void* sort_ws, size_t sort_ws_bytes, cudaStream_t s);
+
 // Grid hydrodynamics add-ons (sd_hydro.cu): per-cell fixed-point sums for cooling
 // and the velocity dispersion, and the pressure acceleration grid (G^3 each).
 struct HydroGrids {

@@ -32,6 +32,7 @@ namespace {
 
 constexpr int kGatherThreads = 256;
 constexpr int kGatherMaxBlocks = 4096;
+constexpr int kKeysPlain = 0, kKeysCounts = 1, kKeysChanged = 2;  // the gather's KEYS modes
 
 __global__ void __launch_bounds__(256) k_deposit_fixed(const float4* __restrict__ pos, int n, int G,
                                                        unsigned long long* __restrict__ acc, int periodic) {
@@ -238,19 +239,32 @@ __device__ __forceinline__ float3 sample_field(const float4* __restrict__ f, int
 
 // PRESS: gas particles (pos.w <= 0, not dark matter) also take the CIC sample of
 // the pressure acceleration grid `press` (G^3; kIntegrate, Sim.cu:740-743).
-template <bool DIAG, bool ISO, bool PRESS>
+//
+// KEYS: what the gather leaves for the next step's sort besides keys_out --
+// kKeysPlain nothing, kKeysCounts the first pass's tile counts (tile_counts),
+// kKeysChanged the change bits (chg_words). Each instantiation holds only its own
+// bookkeeping: the gather runs at its register limit, and code that a launch
+// never executes still costs it.
+template <bool DIAG, bool ISO, bool PRESS, int KEYS>
 __global__ void __launch_bounds__(kGatherThreads, 3) k_gather_kick_drift(
     const float* __restrict__ phi, int G, float h, const float4* pos_in, const float4* vel_in,
     const int* __restrict__ perm, float4* pos_out, float4* vel_out, uint32_t* __restrict__ keys_out, int order, int n,
     float dt_kick, float dt_drift, float c2, const float* __restrict__ mean_vel, double* __restrict__ partials,
     const float4* __restrict__ extra, int S, unsigned* __restrict__ tile_counts, int count_bits,
-    const float4* __restrict__ press) {
-    double sx = 0.0, sy = 0.0, sz = 0.0, cnt = 0.0, sv2 = 0.0, sphi = 0.0;
+    const float4* __restrict__ press, unsigned* __restrict__ chg_words) {
+    // Per-thread FP64 sums (momentum, count; with DIAG |v|^2 and phi), each in the
+    // thread's own shared-memory slot: held in registers they crowd out the stencil's
+    // loads at the kernel's register limit. The summation order is the same.
+    __shared__ double acc[6][kGatherThreads];
+    const int me = threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[q][me] = 0.0;
     const unsigned cmask = (1u << count_bits) - 1u;
     const float mx = mean_vel ? mean_vel[0] : 0.f, my = mean_vel ? mean_vel[1] : 0.f,
                 mz = mean_vel ? mean_vel[2] : 0.f;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t key = 0u;  // the order key written for output i (0: empty or lost)
+        uint32_t key = 0u;      // the order key written for output i (0: empty or lost)
+        uint32_t key_old = 0u;  // the key of the step-start position (the one output i was sorted by)
         do {
             const int j = perm ? perm[i] : i;
             float4 p = pos_in[j];
@@ -294,6 +308,8 @@ __global__ void __launch_bounds__(kGatherThreads, 3) k_gather_kick_drift(
                     v.z = __fmul_rn(v.z, k);
                 }
             }
+            // taken here rather than at the load: nothing holds it across the stencil loads
+            if (KEYS == kKeysChanged) key_old = order_key(p, G, order);
             p.x = __fmaf_rn(v.x, dt_drift, p.x);
             p.y = __fmaf_rn(v.y, dt_drift, p.y);
             p.z = __fmaf_rn(v.z, dt_drift, p.z);
@@ -322,19 +338,26 @@ __global__ void __launch_bounds__(kGatherThreads, 3) k_gather_kick_drift(
                 key = order_key(p, G, order);
                 keys_out[i] = key;
             }
-            sx += v.x;
-            sy += v.y;
-            sz += v.z;
-            cnt += 1.0;
+            acc[0][me] += v.x;
+            acc[1][me] += v.y;
+            acc[2][me] += v.z;
+            acc[3][me] += 1.0;
             if (DIAG) {
-                sv2 += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z;
-                sphi += (double)phi_p;
+                acc[4][me] += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z;
+                acc[5][me] += (double)phi_p;
             }
         } while (0);
+        // The change bit of output i for the next step's merge sort: one word per
+        // warp (a warp's outputs are 32 consecutive, aligned indices).
+        if (KEYS == kKeysChanged) {
+            const unsigned act = __activemask();
+            const unsigned b = __ballot_sync(act, key != key_old);
+            if (b && (int)(threadIdx.x & 31) == __ffs(act) - 1) atomicOr(chg_words + (i >> 5), b);
+        }
         // First sort pass's digit counts of the keys just written: the lanes that
         // share (sort tile, digit) add once. A warp's outputs are consecutive, so
         // they fall in one tile and, the particles being sorted, carry few digits.
-        if (tile_counts) {
+        if (KEYS == kKeysCounts) {
             const unsigned pair = (((unsigned)i >> kSortTileShift) << count_bits) | (key & cmask);
             const unsigned peers = __match_any_sync(__activemask(), pair);
             if ((peers & lanemask_lt()) == 0u) atomicAdd(tile_counts + pair, (unsigned)__popc(peers));
@@ -342,10 +365,10 @@ __global__ void __launch_bounds__(kGatherThreads, 3) k_gather_kick_drift(
     }
     if (partials) {
         if (DIAG) {
-            double v6[6] = {sx, sy, sz, cnt, sv2, sphi};
+            double v6[6] = {acc[0][me], acc[1][me], acc[2][me], acc[3][me], acc[4][me], acc[5][me]};
             block_sum<6>(v6, partials);
         } else {
-            double v4[4] = {sx, sy, sz, cnt};
+            double v4[4] = {acc[0][me], acc[1][me], acc[2][me], acc[3][me]};
             block_sum<4>(v4, partials);
         }
     }
@@ -608,8 +631,10 @@ int gather_prepare(int device) {
     if (g_gather_wave[device] > 0) return SD_OK;
     int sms = 0, per_sm = 0, per_sm_diag = 0;
     if (SD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) ||
-        SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather_kick_drift<false, false, false>, kGatherThreads, 0)) ||
-        SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_diag, k_gather_kick_drift<true, false, false>, kGatherThreads, 0)))
+        SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, k_gather_kick_drift<false, false, false, kKeysChanged>, kGatherThreads, 0)) ||
+        SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm_diag, k_gather_kick_drift<true, false, false, kKeysChanged>, kGatherThreads, 0)))
         return SD_E_CUDA;
     const int w = sms * (per_sm < per_sm_diag ? per_sm : per_sm_diag);
     g_gather_wave[device] = w > 0 ? w : kGatherMaxBlocks;
@@ -627,7 +652,7 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
                              float dt_kick, float dt_drift, float c2, const float* mean_vel, double* partials,
                              double* mom_out, float* mean_out, cudaStream_t s, const float4* extra,
                              int max_blocks, const DiagRecord* diag, int iso_S, unsigned* tile_counts,
-                             int count_bits, const float4* press) {
+                             int count_bits, const float4* press, unsigned* chg_words) {
     if (n <= 0) return SD_OK;
     // particle records are read and written as float4
     if (((uintptr_t)pos_in | (uintptr_t)vel_in | (uintptr_t)pos_out | (uintptr_t)vel_out) & 15u)
@@ -637,21 +662,30 @@ int launch_gather_kick_drift(const float* phi, int G, float pot_scale, const flo
     const int cap = max_blocks > 0 ? max_blocks : gather_wave();
     if (blocks > cap) blocks = cap;
     const bool dg = diag && partials;
-#define SD_GATHER(D, I, P)                                                                                 \
-    k_gather_kick_drift<D, I, P><<<blocks, kGatherThreads, 0, s>>>(                                            \
+    // change bits serve the merge sort of the periodic tiled order only
+    if (chg_words && (iso_S || tile_counts || !keys_out))
+        return fail(SD_E_ARG, "gather: change bits need keys, no tile counts and the periodic box");
+    const int keys_mode = chg_words ? kKeysChanged : (tile_counts ? kKeysCounts : kKeysPlain);
+#define SD_GATHER(D, I, P, K)                                                                              \
+    k_gather_kick_drift<D, I, P, K><<<blocks, kGatherThreads, 0, s>>>(                                         \
         phi, G, h, pos_in, vel_in, perm, pos_out, vel_out, keys_out, order, n, dt_kick, dt_drift, c2, mean_vel, \
-        partials, extra, iso_S, tile_counts, count_bits, press)
-#define SD_GATHER_P(D, I)        \
-    if (press) SD_GATHER(D, I, true); \
-    else SD_GATHER(D, I, false)
+        partials, extra, iso_S, tile_counts, count_bits, press, chg_words)
+#define SD_GATHER_K(D, I, P)                                          \
+    if (keys_mode == kKeysCounts) SD_GATHER(D, I, P, kKeysCounts);    \
+    else if (!I && keys_mode == kKeysChanged) SD_GATHER(D, false, P, kKeysChanged); \
+    else SD_GATHER(D, I, P, kKeysPlain)
+#define SD_GATHER_P(D, I)                \
+    if (press) { SD_GATHER_K(D, I, true); } \
+    else { SD_GATHER_K(D, I, false); }
     if (iso_S) {
-        if (dg) SD_GATHER_P(true, true);
-        else SD_GATHER_P(false, true);
+        if (dg) { SD_GATHER_P(true, true); }
+        else { SD_GATHER_P(false, true); }
     } else {
-        if (dg) SD_GATHER_P(true, false);
-        else SD_GATHER_P(false, false);
+        if (dg) { SD_GATHER_P(true, false); }
+        else { SD_GATHER_P(false, false); }
     }
 #undef SD_GATHER_P
+#undef SD_GATHER_K
 #undef SD_GATHER
     SD_LAUNCHED(s);
     if (dg) {

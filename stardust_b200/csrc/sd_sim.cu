@@ -148,6 +148,8 @@ void free_buffers(sd_sim* s) {
     free_dev(s->acc); free_dev(s->row_start); free_dev(s->spec); free_dev(s->phi); free_dev(s->rho);
     free_dev(s->green);
     hydro_free(s->hydro);
+    if (s->rs_base) cudaFree(s->rs_base);
+    s->rs_base = nullptr;
     free_dev(s->partials); free_dev(s->mom); free_dev(s->mean);
     free_dev(s->mlp_out);
     free_dev(s->diag_rec);
@@ -181,6 +183,7 @@ size_t estimate_bytes(int n, int G, int boundary) {
     b += sizeof(float) * (box + cells);                // phi, kept density
     if (S != G) b += sizeof(float) * green_table_elems(S);
     b += sizeof(double) * 8 * (gather_partials((int)N) + 1024);
+    if (S == G) b += resort_bytes((int)N, G);  // the merge sort (periodic box, tiled order)
     return b;
 }
 
@@ -277,6 +280,39 @@ int ensure_hydro(sd_sim* s) {
     return hydro_alloc(s->hydro, s->G);
 }
 
+// The keys no longer describe the particles (loaded, moved or reordered outside
+// a step): no sort counts, no merge sort until a full one.
+void invalidate_keys(sd_sim* s) {
+    s->keys_valid = false;
+    s->counts_valid = false;
+    s->incr_ready = false;
+}
+
+bool incr_possible(const sd_sim* s) {
+    return s->allow_incr && !s->cfg.full_sort && s->cfg.order == SD_ORDER_TILED && !isolated(s);
+}
+
+// Merge-sort buffers exist while the configuration can merge-sort (zeroed when made).
+int ensure_resort(sd_sim* s) {
+    if (!incr_possible(s)) {
+        if (s->rs_base) cudaFree(s->rs_base);
+        s->rs_base = nullptr;
+        s->incr_ready = s->chg_dirty = false;
+        return SD_OK;
+    }
+    if (s->rs_base) return SD_OK;
+    const size_t b = resort_bytes(s->N, s->G);
+    if (cudaMalloc(&s->rs_base, b) != cudaSuccess) {
+        cudaGetLastError();
+        s->rs_base = nullptr;
+        return fail(SD_E_NOMEM, "cudaMalloc of the merge-sort buffers failed");
+    }
+    // the full sort's scratch (sorted keys, temporaries) is idle while a merge runs
+    s->rs = resort_layout(s->rs_base, s->N, s->G, s->keys2, s->vals2, s->keys3);
+    s->incr_ready = s->chg_dirty = false;
+    return SD_CUDA(cudaMemset(s->rs_base, 0, b));
+}
+
 // placeInitial + reset's velocity and centre-of-mass passes (Sim.cu:3635-3649,
 // 4160-4238): the configured preset in every slot. The mean buffer serves as
 // scratch and is left zero (no correction pending).
@@ -286,7 +322,7 @@ int place_initial(sd_sim* s) {
     s->active = (s->cfg.preset == SD_PRESET_FILAMENT) ? s->N : 0;
     s->mean_pending = false;
     s->rho_valid = false;
-    s->keys_valid = false;
+    invalidate_keys(s);
     return rc;
 }
 
@@ -330,9 +366,9 @@ int ensure_sort_inputs(sd_sim* s) {
     if (!s->keys_valid) {
         if ((rc = launch_cell_keys(s->pos, s->N, s->G, s->cfg.order, s->keys, s->stream))) return rc;
         s->keys_valid = true;
-        s->counts_valid = false;
+        s->counts_valid = s->incr_ready = false;
     }
-    if (!s->counts_valid) {
+    if (!s->counts_valid && !s->incr_ready) {  // a merge sort needs no counts
         if ((rc = launch_sort_first_counts(s->keys, s->N, key_bits_for(s->G, s->cfg.order), s->sort_ws,
                                            s->sort_ws_bytes, s->stream)))
             return rc;
@@ -355,8 +391,7 @@ int do_sort(sd_sim* s, int32_t* perm_out_dev) {
         return SD_E_CUDA;
     std::swap(s->pos, s->pos2);
     std::swap(s->vel, s->vel2);
-    s->keys_valid = false;
-    s->counts_valid = false;
+    invalidate_keys(s);
     return SD_OK;
 }
 
@@ -388,13 +423,32 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     // gather; the permutation is applied by the deposit and gather reads, so no
     // separate reorder pass runs.
     const int32_t* perm = nullptr;
+    // After a sorted step whose gather marked the changed keys, the sort is a merge
+    // of those few into the rest (sd_resort.cu); otherwise the full radix sort.
+    const bool incr_next = sort && s->rs_base && incr_possible(s);
+    bool merged = false;  // the merge also left the new row table
     if (sort) {
-        if ((rc = ensure_sort_inputs(s))) return sim_error(s, rc);
-        rc = launch_sort_pairs(s->keys, nullptr, s->keys2, s->vals, s->keys3, s->vals2, s->N,
-                               key_bits_for(s->G, s->cfg.order), s->sort_ws, s->sort_ws_bytes, s->stream, true, true);
-        if (rc) return sim_error(s, rc);
+        if (s->incr_ready && s->keys_valid && s->rs_base) {
+            rc = launch_resort(s->rs, s->keys, s->N, s->G, key_bits_for(s->G, s->cfg.order), s->row_start, s->vals,
+                               s->sort_ws, s->sort_ws_bytes, s->stream);
+            if (rc) return sim_error(s, rc);
+            s->chg_dirty = false;  // consumed and cleared
+            merged = true;
+        } else {
+            if ((rc = ensure_sort_inputs(s))) return sim_error(s, rc);
+            rc = launch_sort_pairs(s->keys, nullptr, s->keys2, s->vals, s->keys3, s->vals2, s->N,
+                                   key_bits_for(s->G, s->cfg.order), s->sort_ws, s->sort_ws_bytes, s->stream, true,
+                                   true);
+            if (rc) return sim_error(s, rc);
+        }
         s->counts_valid = false;  // the sort consumed and cleared them
         perm = s->vals;
+    }
+    // change bits written by an earlier gather and never merged are cleared first
+    if (incr_next && s->chg_dirty) {
+        if (SD_CUDA(cudaMemsetAsync(s->rs.words, 0, sizeof(unsigned) * resort_words(s->N), s->stream)))
+            return sim_error(s, SD_E_CUDA);
+        s->chg_dirty = false;
     }
     if (timed) cudaEventRecord(s->ev[1], s->stream);
     const bool keep = keeps_rho(s);
@@ -404,7 +458,8 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     // onto the edge cells.)
     const bool fused = sort && s->cfg.order == SD_ORDER_TILED && !isolated(s);
     if (fused) {
-        if ((rc = launch_row_bounds(s->keys2, s->N, s->G * s->G, s->row_start, s->stream))) return sim_error(s, rc);
+        if (!merged && (rc = launch_row_bounds(s->keys2, s->N, s->G * s->G, s->row_start, s->stream)))
+            return sim_error(s, rc);
     } else if ((rc = launch_deposit_fixed(s->pos, s->N, s->G, s->acc, s->stream, isolated(s) ? 0 : 1))) {
         return sim_error(s, rc);
     }
@@ -453,16 +508,20 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
                                   s->cfg.order, s->N, dt_kick, dt_drift, c2, mean_in, s->partials, s->mom, s->mean,
                                   s->stream, s->mlp_on ? s->mlp_out : nullptr, s->gather_blocks,
                                   s->cfg.diagnostics ? &diag : nullptr, isolated(s) ? 2 * s->G : 0,
-                                  sort ? sort_first_counts(s->sort_ws) : nullptr,
-                                  sort_digit_bits(key_bits_for(s->G, s->cfg.order)), press ? s->hydro.acc : nullptr);
+                                  (sort && !incr_next) ? sort_first_counts(s->sort_ws) : nullptr,
+                                  sort_digit_bits(key_bits_for(s->G, s->cfg.order)), press ? s->hydro.acc : nullptr,
+                                  incr_next ? s->rs.words : nullptr);
     if (rc) return sim_error(s, rc);
     if (perm) {
         std::swap(s->pos, s->pos2);
         std::swap(s->vel, s->vel2);
     }
     s->keys_valid = true;
-    // after a sort the counts buffer was zero, and the gather counted the new keys
-    s->counts_valid = sort;
+    // after a sort the counts buffer was zero, and the gather counted the new keys --
+    // or, when the next sort can merge, marked the changed ones
+    s->counts_valid = sort && !incr_next;
+    s->incr_ready = incr_next;
+    s->chg_dirty = incr_next;
     s->mean_pending = true;
     if (timed) cudaEventRecord(s->ev[4], s->stream);
     s->ev_valid = timed;
@@ -494,13 +553,13 @@ int reconfigure(sd_sim* s, const sd_config* c) {
     const bool structural = !s->configured || c->particle_count != s->N || G != s->G ||
                             c->boundary != s->cfg.boundary || (c->keep_density && !s->rho);
     const bool soft_changed = c->softening_cells != s->cfg.softening_cells;
-    if (c->order != s->cfg.order) s->keys_valid = false;
+    if (c->order != s->cfg.order) invalidate_keys(s);
     s->cfg = *c;
     s->cfg.grid_size = G;
     if (!structural) {
         if (s->graph) cudaGraphExecDestroy(s->graph);
         s->graph = nullptr;
-        if ((rc = ensure_hydro(s))) return rc;
+        if ((rc = ensure_hydro(s)) || (rc = ensure_resort(s))) return rc;
         if (!soft_changed) return SD_OK;
         rc = poisson_plan_build(s->plan, box_of(s->G, s->cfg.boundary), s->cfg.softening_cells);
         if (!rc && isolated(s))
@@ -511,7 +570,7 @@ int reconfigure(sd_sim* s, const sd_config* c) {
     s->G = G;
     rc = allocate(s);
     if (rc) return rc;
-    if ((rc = ensure_hydro(s))) return rc;
+    if ((rc = ensure_hydro(s)) || (rc = ensure_resort(s))) return rc;
     // the reference's init / structural reconfigure ends in reset() (Sim.cu:4151)
     if ((rc = place_initial(s))) return sim_error(s, rc);
     s->sim_time = 0.0;
@@ -519,7 +578,7 @@ int reconfigure(sd_sim* s, const sd_config* c) {
     s->mean_pending = false;
     s->lf_open = false;
     s->rho_valid = false;
-    s->keys_valid = false;
+    invalidate_keys(s);
     s->cuda_failed = false;
     return SD_OK;
 }
@@ -707,7 +766,7 @@ int sd_set_particles(sd_sim* s, const float* pos, const float* vel, int n, int w
     s->mean_pending = false;
     s->lf_open = false;
     s->rho_valid = false;
-    s->keys_valid = false;
+    invalidate_keys(s);
     return SD_OK;
 }
 
@@ -851,7 +910,7 @@ int sd_step_host(sd_sim* s, const float* pos_in, const float* vel_in, int n, flo
     s->mean_pending = false;
     s->lf_open = false;
     s->rho_valid = false;
-    s->keys_valid = false;
+    invalidate_keys(s);
     s->vel_wait = s->io_ev[1];
     rc = do_step(s, dt, sort_due(s), true);
     if (s->vel_wait) {  // a step that read no velocity still owes the wait
@@ -902,7 +961,6 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
     // A two-step graph repeats the cooling schedule only when its period is 2.
     const bool graphable = (s->cfg.sort_interval == 0 || s->cfg.sort_interval == 1) &&
                            (!hydro_on(s) || cooling_period(s) == 2);
-    const int phase = hydro_on(s) ? (s->step_count & 1) : 0;
     int done = 0;
     // leapfrog opening kick and odd counts run eagerly
     while (done < nsteps && (!graphable || (s->cfg.integrator == SD_INT_KDK && !s->lf_open))) {
@@ -912,62 +970,75 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
     }
     if (done >= nsteps) return SD_OK;
     const bool sort = s->cfg.sort_interval == 1;
-    // Keys and first-pass counts are made outside the graph, so replays never
-    // depend on them being stale.
-    if (sort) {
-        int rc = ensure_sort_inputs(s);
-        if (rc) return sim_error(s, rc);
-    }
-    // A captured graph covers two steps so the pos/pos2 ping-pong returns to the
-    // same buffers; it is rebuilt when dt changes or the particles sit in the
-    // other buffer of the pair.
-    if (!s->graph || s->graph_dt != dt || s->graph_pos != s->pos || s->graph_phase != phase) {
-        if (s->graph) cudaGraphExecDestroy(s->graph);
-        s->graph = nullptr;
-        cudaGraph_t graph = nullptr;
-        if (SD_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal))) return sim_error(s, SD_E_CUDA);
-        const double t0 = s->sim_time;
-        const int c0 = s->step_count;
-        const bool lf0 = s->lf_open;
-        const float lfd = s->lf_dt_prev;
-        const bool mp0 = s->mean_pending;
-        const bool kv0 = s->keys_valid;
-        const bool cv0 = s->counts_valid;
-        const long long l0 = launches();
-        int rc = do_step(s, dt, sort, false);
-        if (!rc) rc = do_step(s, dt, sort, false);
-        cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
-        // capture only recorded the kernels; count them per replay instead
-        s->graph_launches = launches() - l0;
-        count_launch(-s->graph_launches);
-        // capture recorded work only; restore the host-side counters
-        s->sim_time = t0;
-        s->step_count = c0;
-        s->lf_open = lf0;
-        s->lf_dt_prev = lfd;
-        s->mean_pending = mp0;
-        s->keys_valid = kv0;
-        s->counts_valid = cv0;
-        if (rc) {
-            if (graph) cudaGraphDestroy(graph);
-            return rc;
-        }
-        if (SD_CUDA(e)) return sim_error(s, SD_E_CUDA);
-        e = cudaGraphInstantiate(&s->graph, graph, 0);
-        cudaGraphDestroy(graph);
-        if (SD_CUDA(e)) return sim_error(s, SD_E_CUDA);
-        s->graph_dt = dt;
-        s->graph_pos = s->pos;
-        s->graph_phase = phase;
-    }
     while (nsteps - done >= 2) {
+        // Keys and first-pass counts are made outside the graph, so replays never
+        // depend on them being stale.
+        if (sort) {
+            int rc = ensure_sort_inputs(s);
+            if (rc) return sim_error(s, rc);
+        }
+        const int phase = hydro_on(s) ? (s->step_count & 1) : 0;
+        const bool incr_now = s->incr_ready && s->keys_valid;  // the first captured step merge-sorts
+        // A captured graph covers two steps so the pos/pos2 ping-pong returns to the
+        // same buffers; it is rebuilt when dt changes, the particles sit in the other
+        // buffer of the pair, the cooling phase moved, or its first step would sort
+        // differently (a merge needs the last step's change bits).
+        if (!s->graph || s->graph_dt != dt || s->graph_pos != s->pos || s->graph_phase != phase ||
+            s->graph_incr != incr_now) {
+            if (s->graph) cudaGraphExecDestroy(s->graph);
+            s->graph = nullptr;
+            cudaGraph_t graph = nullptr;
+            if (SD_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal)))
+                return sim_error(s, SD_E_CUDA);
+            const double t0 = s->sim_time;
+            const int c0 = s->step_count;
+            const bool lf0 = s->lf_open;
+            const float lfd = s->lf_dt_prev;
+            const bool mp0 = s->mean_pending;
+            const bool kv0 = s->keys_valid;
+            const bool cv0 = s->counts_valid;
+            const bool iv0 = s->incr_ready, dv0 = s->chg_dirty;
+            const long long l0 = launches();
+            int rc = do_step(s, dt, sort, false);
+            if (!rc) rc = do_step(s, dt, sort, false);
+            cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+            // capture only recorded the kernels; count them per replay instead
+            s->graph_launches = launches() - l0;
+            count_launch(-s->graph_launches);
+            // capture recorded work only; restore the host-side counters
+            s->sim_time = t0;
+            s->step_count = c0;
+            s->lf_open = lf0;
+            s->lf_dt_prev = lfd;
+            s->mean_pending = mp0;
+            s->keys_valid = kv0;
+            s->counts_valid = cv0;
+            s->incr_ready = iv0;
+            s->chg_dirty = dv0;
+            if (rc) {
+                if (graph) cudaGraphDestroy(graph);
+                return rc;
+            }
+            if (SD_CUDA(e)) return sim_error(s, SD_E_CUDA);
+            e = cudaGraphInstantiate(&s->graph, graph, 0);
+            cudaGraphDestroy(graph);
+            if (SD_CUDA(e)) return sim_error(s, SD_E_CUDA);
+            s->graph_dt = dt;
+            s->graph_pos = s->pos;
+            s->graph_phase = phase;
+            s->graph_incr = incr_now;
+        }
         if (SD_CUDA(cudaGraphLaunch(s->graph, s->stream))) return sim_error(s, SD_E_CUDA);
         count_launch(s->graph_launches);
         s->sim_time += 2.0 * dt;
         s->step_count += 2;
         s->mean_pending = true;
         s->keys_valid = true;
-        s->counts_valid = sort;
+        {  // the graph's last step leaves what do_step leaves after a sorted step
+            const bool incr_next = sort && s->rs_base && incr_possible(s);
+            s->counts_valid = sort && !incr_next;
+            s->incr_ready = s->chg_dirty = incr_next;
+        }
         if (s->cfg.integrator == SD_INT_KDK) {
             s->lf_open = true;
             s->lf_dt_prev = dt;
@@ -995,7 +1066,7 @@ int sd_synchronize(sd_sim* s) {
                                   s->mean, s->stream, s->mlp_on ? s->mlp_out : nullptr, 0, nullptr,
                                   isolated(s) ? 2 * s->G : 0);
     if (rc) return sim_error(s, rc);
-    s->counts_valid = false;  // keys were rewritten (a lost particle changes its key)
+    s->counts_valid = s->incr_ready = false;  // keys were rewritten (a lost particle changes its key)
     s->mean_pending = true;
     s->lf_open = false;
     return SD_OK;

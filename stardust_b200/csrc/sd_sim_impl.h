@@ -33,6 +33,7 @@ struct sd_sim {
     float* green = nullptr;      // isolated boundary: real Green spectrum of the 2G box
     sd::HydroGrids hydro;        // pressure / cooling grids, allocated while either is on
     int graph_phase = 0;         // step count parity the captured graph was made at (hydro)
+    bool graph_incr = false;     // whether the captured graph's first step merge-sorts
     double* partials = nullptr;  // gather / energy / reduction partials
     size_t partials_count = 0;
     double* mom = nullptr;       // 8 doubles: momentum sums of the last step, energy results
@@ -41,6 +42,11 @@ struct sd_sim {
     bool rho_valid = false;
     bool keys_valid = false;     // keys hold the order keys of the current pos order
     bool counts_valid = false;   // the sort workspace holds the first-pass tile counts of keys
+    bool incr_ready = false;     // the last step left change bits and its row table: merge-sort next
+    bool chg_dirty = false;      // change bits written and not consumed yet (cleared before reuse)
+    bool allow_incr = true;      // merge sorting allowed (ensemble members sort in full)
+    void* rs_base = nullptr;     // merge-sort buffers (tiled order, periodic)
+    sd::ResortBufs rs;
     sd::PoissonPlan plan;
 
     // leapfrog
@@ -93,6 +99,8 @@ struct DeviceGuard {
 int sim_error(sd_sim* s, int rc);
 bool sort_due(const sd_sim* s);
 int ensure_sort_inputs(sd_sim* s);
+void invalidate_keys(sd_sim* s);
+bool incr_possible(const sd_sim* s);
 bool hydro_on(const sd_sim* s);
 int cooling_period(const sd_sim* s);
 int key_bits_for(int G, int order);

@@ -85,57 +85,71 @@ __device__ __forceinline__ unsigned block_exclusive(unsigned v, unsigned* warp_s
 
 template <int BITS>
 __global__ void __launch_bounds__(kSortThreads) k_digit_counts(const uint32_t* __restrict__ keys, int n, int shift,
-                                                               unsigned* __restrict__ counts, int tiles) {
+                                                               unsigned* __restrict__ counts, int tiles,
+                                                               const int* __restrict__ n_dev) {
     constexpr int kRadix = 1 << BITS;
     constexpr unsigned mask = kRadix - 1;
     __shared__ unsigned hist[kRadix];
-    for (int d = threadIdx.x; d < kRadix; d += kSortThreads) hist[d] = 0u;
-    __syncthreads();
-    const int base = blockIdx.x * kSortTile;
-    // Nearly sorted keys put few distinct digits in a warp: one shared add per
-    // digit and warp (of the number of lanes holding it) instead of one per key.
-    unsigned dd[kSortItems];
+    if (n_dev) n = *n_dev;  // a count made on the device; the grid covers at most the capacity
+    const int ntiles = (n + kSortTile - 1) / kSortTile;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        for (int d = threadIdx.x; d < kRadix; d += kSortThreads) hist[d] = 0u;
+        __syncthreads();
+        const int base = tile * kSortTile;
+        // Nearly sorted keys put few distinct digits in a warp: one shared add per
+        // digit and warp (of the number of lanes holding it) instead of one per key.
+        unsigned dd[kSortItems];
 #pragma unroll
-    for (int it = 0; it < kSortItems; ++it) {
-        const int idx = base + it * kSortThreads + threadIdx.x;
-        dd[it] = (idx < n) ? ((keys[idx] >> shift) & mask) : 0xffffffffu;
-    }
-    const unsigned lt = lanemask_lt();
+        for (int it = 0; it < kSortItems; ++it) {
+            const int idx = base + it * kSortThreads + threadIdx.x;
+            dd[it] = (idx < n) ? ((keys[idx] >> shift) & mask) : 0xffffffffu;
+        }
+        const unsigned lt = lanemask_lt();
 #pragma unroll
-    for (int it = 0; it < kSortItems; ++it) {
-        const unsigned d = dd[it];
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
-        if ((peers & lt) == 0u && d != 0xffffffffu) atomicAdd(&hist[d], (unsigned)__popc(peers));
+        for (int it = 0; it < kSortItems; ++it) {
+            const unsigned d = dd[it];
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            if ((peers & lt) == 0u && d != 0xffffffffu) atomicAdd(&hist[d], (unsigned)__popc(peers));
+        }
+        __syncthreads();
+        // tile-major rows: one coalesced row of kRadix counts per tile
+        for (int d = threadIdx.x; d < kRadix; d += kSortThreads) counts[(size_t)tile * kRadix + d] = hist[d];
+        __syncthreads();
     }
-    __syncthreads();
-    // tile-major rows: one coalesced row of kRadix counts per tile
-    for (int d = threadIdx.x; d < kRadix; d += kSortThreads) counts[(size_t)blockIdx.x * kRadix + d] = hist[d];
 }
 
+// Shared memory of one scatter tile.
 template <int BITS>
-__global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* __restrict__ keys_in,
-                                                                const int32_t* __restrict__ vals_in,
-                                                                uint32_t* __restrict__ keys_out,
-                                                                int32_t* __restrict__ vals_out, int n, int shift,
-                                                                unsigned* __restrict__ offsets,
-                                                                unsigned* __restrict__ next_counts,
-                                                                unsigned* __restrict__ next_sums, int next_shift) {
+struct ScatterSmem {
+    // per-warp digit counts fit 16 bits (a warp ranks at most 32 * kSortItems keys)
+    unsigned short warp_cnt[kWarps][1 << BITS];
+    unsigned local_start[1 << BITS];
+    unsigned dst_base[1 << BITS];  // global start of the digit's run minus its local start
+    unsigned scan_tmp[33];
+    uint32_t skeys[kSortTile];
+    int32_t svals[kSortTile];
+};
+
+// One tile of k_digit_scatter (n keys in all).
+template <int BITS>
+__device__ __forceinline__ void scatter_tile(ScatterSmem<BITS>& sm, int tile, const uint32_t* __restrict__ keys_in,
+                                             const int32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
+                                             int32_t* __restrict__ vals_out, int n, int shift,
+                                             unsigned* __restrict__ offsets, unsigned* __restrict__ next_counts,
+                                             unsigned* __restrict__ next_sums, int next_shift) {
     constexpr int kRadix = 1 << BITS;
     constexpr unsigned mask = kRadix - 1;
     constexpr int DPT = (kRadix + kSortThreads - 1) / kSortThreads;  // digits per thread
-    // per-warp digit counts fit 16 bits (a warp ranks at most 32 * kSortItems keys)
-    __shared__ unsigned short warp_cnt[kWarps][kRadix];
-    __shared__ unsigned local_start[kRadix];
-    __shared__ unsigned dst_base[kRadix];  // global start of the digit's run minus its local start
-    __shared__ unsigned scan_tmp[33];
-    __shared__ uint32_t skeys[kSortTile];
-    __shared__ int32_t svals[kSortTile];
-
+    auto& warp_cnt = sm.warp_cnt;
+    auto& local_start = sm.local_start;
+    auto& dst_base = sm.dst_base;
+    auto& skeys = sm.skeys;
+    auto& svals = sm.svals;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortThreads) (&warp_cnt[0][0])[i] = 0;
     __syncthreads();
 
-    const int tile0 = blockIdx.x * kSortTile;
+    const int tile0 = tile * kSortTile;
     const unsigned lt = lanemask_lt();
     uint32_t k[kSortItems];
     int32_t v[kSortItems];
@@ -191,20 +205,20 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* 
     __syncthreads();
     {
         unsigned tot;
-        unsigned ex = block_exclusive(tsum, scan_tmp, &tot);
+        unsigned ex = block_exclusive(tsum, sm.scan_tmp, &tot);
 #pragma unroll
         for (int j = 0; j < DPT; ++j) {
             const int d = threadIdx.x * DPT + j;
             if (d < kRadix) {
                 local_start[d] = ex;
-                dst_base[d] = offsets[(size_t)blockIdx.x * kRadix + d] - ex;
+                dst_base[d] = offsets[(size_t)tile * kRadix + d] - ex;
             }
             ex += dtot[j];
         }
     }
     __syncthreads();
     // this tile's row of offsets is consumed: clear it for the next sort
-    for (int d = threadIdx.x; d < kRadix; d += kSortThreads) offsets[(size_t)blockIdx.x * kRadix + d] = 0u;
+    for (int d = threadIdx.x; d < kRadix; d += kSortThreads) offsets[(size_t)tile * kRadix + d] = 0u;
 
 #pragma unroll
     for (int it = 0; it < kSortItems; ++it) {
@@ -245,6 +259,32 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* 
     }
 }
 
+// LOOP: the key count comes from the device (n_dev) and the grid loops over the
+// tiles in use; otherwise one CTA per tile (no loop state held across tiles).
+template <int BITS, bool LOOP>
+__global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* __restrict__ keys_in,
+                                                                const int32_t* __restrict__ vals_in,
+                                                                uint32_t* __restrict__ keys_out,
+                                                                int32_t* __restrict__ vals_out, int n, int shift,
+                                                                unsigned* __restrict__ offsets,
+                                                                unsigned* __restrict__ next_counts,
+                                                                unsigned* __restrict__ next_sums, int next_shift,
+                                                                const int* __restrict__ n_dev) {
+    __shared__ ScatterSmem<BITS> sm;
+    if (!LOOP) {
+        scatter_tile<BITS>(sm, blockIdx.x, keys_in, vals_in, keys_out, vals_out, n, shift, offsets, next_counts,
+                           next_sums, next_shift);
+        return;
+    }
+    n = *n_dev;  // a count made on the device; the grid covers at most the capacity
+    const int ntiles = (n + kSortTile - 1) / kSortTile;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        scatter_tile<BITS>(sm, tile, keys_in, vals_in, keys_out, vals_out, n, shift, offsets, next_counts, next_sums,
+                           next_shift);
+        __syncthreads();  // the tile's shared memory is read to the end before the next one
+    }
+}
+
 // Exclusive offsets of the tile-major digit counts counts[tile][digit]:
 //   offset(t, d) = base(d) + sum_{t' < t} counts[t'][d],  base(d) = sum_{d' < d} total(d'),
 // over chunks of kColChunk tiles and slabs of 32 digits, so every global access
@@ -255,24 +295,34 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint32_t* 
 //   k_col_apply  counts[t][d] -> base(d) + S[c][d] + prefix within the chunk,
 //                and clears S, ready for the adds of the next counts
 
+// Tiles holding n keys (n from the device when n_dev is set: the grids cover the capacity).
+__device__ __forceinline__ int tiles_of(int tiles, const int* n_dev) {
+    return n_dev ? (*n_dev + kSortTile - 1) / kSortTile : tiles;
+}
+
 __global__ void __launch_bounds__(kColThreads) k_col_sums(const unsigned* __restrict__ counts, int tiles, int radix,
-                                                          unsigned* __restrict__ S) {
-    const int c = blockIdx.x, d = blockIdx.y * kColThreads + threadIdx.x;
+                                                          unsigned* __restrict__ S, const int* __restrict__ n_dev) {
+    const int d = blockIdx.y * kColThreads + threadIdx.x;
+    tiles = tiles_of(tiles, n_dev);
     if (d >= radix) return;
-    const int t0 = c * kColChunk, t1 = min(tiles, t0 + kColChunk);
-    unsigned s = 0u;
+    for (int c = blockIdx.x; c * kColChunk < tiles; c += gridDim.x) {
+        const int t0 = c * kColChunk, t1 = min(tiles, t0 + kColChunk);
+        unsigned s = 0u;
 #pragma unroll 8
-    for (int t = t0; t < t1; ++t) s += counts[(size_t)t * radix + d];
-    S[(size_t)c * radix + d] = s;
+        for (int t = t0; t < t1; ++t) s += counts[(size_t)t * radix + d];
+        S[(size_t)c * radix + d] = s;
+    }
 }
 
 // CTA per 32-digit slab: thread (seg, lane) owns digit slab*32 + lane and a
 // contiguous run of chunks; two sweeps (sum, rewrite) around a scan of the runs.
 __global__ void __launch_bounds__(kColThreads) k_col_prefix(unsigned* __restrict__ S, int chunks, int radix,
-                                                            unsigned* __restrict__ T, unsigned* __restrict__ done) {
+                                                            unsigned* __restrict__ T, unsigned* __restrict__ done,
+                                                            const int* __restrict__ n_dev) {
     __shared__ unsigned seg_sum[kColSegs][32];
     __shared__ unsigned scan_tmp[33];
     __shared__ bool last;
+    if (n_dev) chunks = (tiles_of(0, n_dev) + kColChunk - 1) / kColChunk;
     const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
     const int d = blockIdx.x * 32 + lane;
     const int per = (chunks + kColSegs - 1) / kColSegs;
@@ -333,40 +383,45 @@ __global__ void __launch_bounds__(kColThreads) k_col_prefix(unsigned* __restrict
 // memory, scanned down each column in 8 segments of 8 tiles.
 __global__ void __launch_bounds__(kColThreads) k_col_apply(unsigned* __restrict__ counts, int tiles, int radix,
                                                            unsigned* __restrict__ S,
-                                                           const unsigned* __restrict__ T) {
+                                                           const unsigned* __restrict__ T,
+                                                           const int* __restrict__ n_dev) {
     __shared__ unsigned tile[kColChunk][33];
     __shared__ unsigned seg_sum[kColSegs][32];
     const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
-    const int c = blockIdx.x, d = blockIdx.y * 32 + lane;
-    const int t0 = c * kColChunk, rows = min(tiles - t0, kColChunk);
-    constexpr int kRowsPerSeg = kColChunk / kColSegs;
+    const int d = blockIdx.y * 32 + lane;
+    tiles = tiles_of(tiles, n_dev);
+    for (int c = blockIdx.x; c * kColChunk < tiles; c += gridDim.x) {
+        const int t0 = c * kColChunk, rows = min(tiles - t0, kColChunk);
+        constexpr int kRowsPerSeg = kColChunk / kColSegs;
 #pragma unroll
-    for (int j = 0; j < kRowsPerSeg; ++j) {
-        const int r = seg + j * kColSegs;
-        tile[r][lane] = (r < rows && d < radix) ? counts[(size_t)(t0 + r) * radix + d] : 0u;
-    }
-    __syncthreads();
-    unsigned sum = 0u;
+        for (int j = 0; j < kRowsPerSeg; ++j) {
+            const int r = seg + j * kColSegs;
+            tile[r][lane] = (r < rows && d < radix) ? counts[(size_t)(t0 + r) * radix + d] : 0u;
+        }
+        __syncthreads();
+        unsigned sum = 0u;
 #pragma unroll
-    for (int j = 0; j < kRowsPerSeg; ++j) sum += tile[seg * kRowsPerSeg + j][lane];
-    seg_sum[seg][lane] = sum;
-    __syncthreads();
-    unsigned run = (d < radix) ? T[d] + S[(size_t)c * radix + d] : 0u;
-    for (int j = 0; j < seg; ++j) run += seg_sum[j][lane];
-    __syncthreads();  // every segment has read S[c][d]
-    if (seg == 0 && d < radix) S[(size_t)c * radix + d] = 0u;
+        for (int j = 0; j < kRowsPerSeg; ++j) sum += tile[seg * kRowsPerSeg + j][lane];
+        seg_sum[seg][lane] = sum;
+        __syncthreads();
+        unsigned run = (d < radix) ? T[d] + S[(size_t)c * radix + d] : 0u;
+        for (int j = 0; j < seg; ++j) run += seg_sum[j][lane];
+        __syncthreads();  // every segment has read S[c][d] and seg_sum
+        if (seg == 0 && d < radix) S[(size_t)c * radix + d] = 0u;
 #pragma unroll
-    for (int j = 0; j < kRowsPerSeg; ++j) {
-        const int r = seg * kRowsPerSeg + j;
-        const unsigned v = tile[r][lane];
-        tile[r][lane] = run;
-        run += v;
-    }
-    __syncthreads();
+        for (int j = 0; j < kRowsPerSeg; ++j) {
+            const int r = seg * kRowsPerSeg + j;
+            const unsigned v = tile[r][lane];
+            tile[r][lane] = run;
+            run += v;
+        }
+        __syncthreads();
 #pragma unroll
-    for (int j = 0; j < kRowsPerSeg; ++j) {
-        const int r = seg + j * kColSegs;
-        if (r < rows && d < radix) counts[(size_t)(t0 + r) * radix + d] = tile[r][lane];
+        for (int j = 0; j < kRowsPerSeg; ++j) {
+            const int r = seg + j * kColSegs;
+            if (r < rows && d < radix) counts[(size_t)(t0 + r) * radix + d] = tile[r][lane];
+        }
+        __syncthreads();  // the staged chunk is written out before the next one is loaded
     }
 }
 
@@ -436,6 +491,11 @@ int launch_cell_keys(const float4* pos, int n, int G, int order, uint32_t* keys,
 
 static int col_chunks(int tiles) { return (tiles + kColChunk - 1) / kColChunk; }
 
+// Grid of a tile- or chunk-looping kernel: one CTA per unit for a count known on
+// the host; for a count on the device (at most `units`), at most `cap` CTAs.
+static int loop_grid(int units, const int* n_dev, int cap) { return n_dev ? std::min(units, cap) : units; }
+constexpr int kNumSMs = 148;
+
 // Workspace: two count buffers of tiles x radix (the pass being scattered and
 // the next pass's counts), the chunk sums S[chunks][radix], the digit totals /
 // bases T[radix] and the column scan's finish counter.
@@ -471,21 +531,23 @@ size_t sort_workspace_bytes(int n) {
            align_up(((size_t)1 << kMaxRadixBits) * sizeof(unsigned) + sizeof(unsigned), 256);
 }
 
-static int col_sums(const unsigned* counts, int tiles, int radix, unsigned* S, cudaStream_t s) {
-    k_col_sums<<<dim3(col_chunks(tiles), (radix + kColThreads - 1) / kColThreads), kColThreads, 0, s>>>(counts, tiles,
-                                                                                                     radix, S);
+static int col_sums(const unsigned* counts, int tiles, int radix, unsigned* S, cudaStream_t s, const int* n_dev) {
+    k_col_sums<<<dim3(loop_grid(col_chunks(tiles), n_dev, kNumSMs), (radix + kColThreads - 1) / kColThreads),
+                 kColThreads, 0, s>>>(
+        counts, tiles, radix, S, n_dev);
     SD_LAUNCHED(s);
     return SD_OK;
 }
 
 // counts[tiles][radix] (tile-major) with their chunk sums in w.S -> exclusive
 // global offsets, in place; leaves w.S zero.
-static int scan_offsets(unsigned* counts, int tiles, int radix, const SortWs& w, cudaStream_t s) {
+static int scan_offsets(unsigned* counts, int tiles, int radix, const SortWs& w, cudaStream_t s, const int* n_dev) {
     const int chunks = col_chunks(tiles);
     const int slabs = (radix + 31) / 32;
-    k_col_prefix<<<slabs, kColThreads, 0, s>>>(w.S, chunks, radix, w.T, w.done);
+    k_col_prefix<<<slabs, kColThreads, 0, s>>>(w.S, chunks, radix, w.T, w.done, n_dev);
     SD_LAUNCHED(s);
-    k_col_apply<<<dim3(chunks, slabs), kColThreads, 0, s>>>(counts, tiles, radix, w.S, w.T);
+    k_col_apply<<<dim3(loop_grid(chunks, n_dev, kNumSMs), slabs), kColThreads, 0, s>>>(counts, tiles, radix, w.S,
+                                                                                          w.T, n_dev);
     SD_LAUNCHED(s);
     return SD_OK;
 }
@@ -507,9 +569,9 @@ int launch_sort_first_counts(const uint32_t* keys, int n, int key_bits, void* ws
     const int tiles = (n + kSortTile - 1) / kSortTile;
     const SortWs w = sort_ws_layout(ws, n);
     switch (bits) {
-        case 8: k_digit_counts<8><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, w.cnt[0], tiles); break;
-        case 9: k_digit_counts<9><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, w.cnt[0], tiles); break;
-        default: k_digit_counts<10><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, w.cnt[0], tiles); break;
+        case 8: k_digit_counts<8><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, w.cnt[0], tiles, nullptr); break;
+        case 9: k_digit_counts<9><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, w.cnt[0], tiles, nullptr); break;
+        default: k_digit_counts<10><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, w.cnt[0], tiles, nullptr); break;
     }
     SD_LAUNCHED(s);
     return SD_OK;
@@ -517,7 +579,7 @@ int launch_sort_first_counts(const uint32_t* keys, int n, int key_bits, void* ws
 
 int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t* keys_out, int32_t* vals_out,
                       uint32_t* keys_tmp, int32_t* vals_tmp, int n, int key_bits, void* ws, size_t ws_bytes,
-                      cudaStream_t s, bool ws_zeroed, bool first_counts_ready) {
+                      cudaStream_t s, bool ws_zeroed, bool first_counts_ready, const int* n_dev) {
     if (n < 0 || key_bits < 0 || key_bits > 32) return fail(SD_E_ARG, "sort: bad n=%d or key_bits=%d", n, key_bits);
     if (n == 0) return SD_OK;
     if (!keys_in || !keys_out || !vals_out || !keys_tmp || !vals_tmp || !ws)
@@ -536,6 +598,9 @@ int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t*
     const int tiles = (n + kSortTile - 1) / kSortTile;
     const SortWs w = sort_ws_layout(ws, n);
     unsigned* const* cnt = w.cnt;
+    // a count on the device: grids of about one wave that loop over the tiles in use
+    const int count_grid = loop_grid(tiles, n_dev, kNumSMs * 8);
+    const int scatter_grid = loop_grid(tiles, n_dev, kNumSMs * 4);
     // The scatters add the next pass's counts into the second buffer, which must
     // start at zero, and the column scan counts its CTAs on w.done; a sort leaves
     // both zero, so a workspace that only ever serves this sort is cleared once.
@@ -557,31 +622,31 @@ int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t*
         const int next_shift = (p + 1) * bits;
         // key bits above key_bits are zero, so a last digit reaching past them is exact
         if (p == 0 && !first_counts_ready) {
+            const int g = count_grid;
             switch (bits) {
-                case 8: k_digit_counts<8><<<tiles, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles); break;
-                case 9: k_digit_counts<9><<<tiles, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles); break;
-                default: k_digit_counts<10><<<tiles, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles); break;
+                case 8: k_digit_counts<8><<<g, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles, n_dev); break;
+                case 9: k_digit_counts<9><<<g, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles, n_dev); break;
+                default: k_digit_counts<10><<<g, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles, n_dev); break;
             }
             SD_LAUNCHED(s);
         }
         // first-pass counts, however they were made, still need their chunk sums;
         // later passes got theirs from the scatter's adds
-        if (p == 0 && (rc = col_sums(counts, tiles, 1 << bits, w.S, s))) return rc;
-        if ((rc = scan_offsets(counts, tiles, 1 << bits, w, s))) return rc;
+        if (p == 0 && (rc = col_sums(counts, tiles, 1 << bits, w.S, s, n_dev))) return rc;
+        if ((rc = scan_offsets(counts, tiles, 1 << bits, w, s, n_dev))) return rc;
+#define SD_SCATTER(B, L)                                                                                   \
+    k_digit_scatter<B, L><<<scatter_grid, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, next, w.S, \
+                                                                next_shift, n_dev)
+#define SD_SCATTER_B(B)        \
+    if (n_dev) SD_SCATTER(B, true); \
+    else SD_SCATTER(B, false)
         switch (bits) {
-            case 8:
-                k_digit_scatter<8><<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, next,
-                                                                   w.S, next_shift);
-                break;
-            case 9:
-                k_digit_scatter<9><<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, next,
-                                                                   w.S, next_shift);
-                break;
-            default:
-                k_digit_scatter<10><<<tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, next,
-                                                                    w.S, next_shift);
-                break;
+            case 8: SD_SCATTER_B(8); break;
+            case 9: SD_SCATTER_B(9); break;
+            default: SD_SCATTER_B(10); break;
         }
+#undef SD_SCATTER_B
+#undef SD_SCATTER
         SD_LAUNCHED(s);
         kin = kout;
         vin = vout;
