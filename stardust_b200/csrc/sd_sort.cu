@@ -15,8 +15,9 @@
 //      plus the digit bases, a rescan of each chunk) turns the rows into, for
 //      every (tile, digit), the global output offset: all keys of smaller digits
 //      plus the same digit's keys in earlier tiles, which is what makes the
-//      result stable across tiles. Counts added by a scatter bring their chunk
-//      sums with them; the first pass's counts have their chunks summed;
+//      result stable across tiles. Counts from k_digit_counts or added by a
+//      scatter bring their chunk sums with them; counts added by the gather that
+//      wrote the keys have their chunks summed;
 //   3. k_digit_scatter: each tile ranks its keys stably (per warp, in input order,
 //      with __match_any_sync on the digit), stages them digit-sorted in shared
 //      memory and writes each digit run contiguously; it then clears its row of
@@ -85,7 +86,8 @@ __device__ __forceinline__ unsigned block_exclusive(unsigned v, unsigned* warp_s
 
 template <int BITS>
 __global__ void __launch_bounds__(kSortThreads) k_digit_counts(const uint32_t* __restrict__ keys, int n, int shift,
-                                                               unsigned* __restrict__ counts, int tiles,
+                                                               unsigned* __restrict__ counts,
+                                                               unsigned* __restrict__ chunk_sums,
                                                                const int* __restrict__ n_dev) {
     constexpr int kRadix = 1 << BITS;
     constexpr unsigned mask = kRadix - 1;
@@ -112,8 +114,14 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_counts(const uint32_t* _
             if ((peers & lt) == 0u && d != 0xffffffffu) atomicAdd(&hist[d], (unsigned)__popc(peers));
         }
         __syncthreads();
-        // tile-major rows: one coalesced row of kRadix counts per tile
-        for (int d = threadIdx.x; d < kRadix; d += kSortThreads) counts[(size_t)tile * kRadix + d] = hist[d];
+        // tile-major rows: one coalesced row of kRadix counts per tile; with chunk_sums
+        // (zero at the start of a sort) each tile also adds into its chunk's sums, so
+        // the column scan needs no separate summing pass
+        for (int d = threadIdx.x; d < kRadix; d += kSortThreads) {
+            const unsigned c = hist[d];
+            counts[(size_t)tile * kRadix + d] = c;
+            if (chunk_sums && c) atomicAdd(chunk_sums + (size_t)(tile >> kSortChunkShift) * kRadix + d, c);
+        }
         __syncthreads();
     }
 }
@@ -569,9 +577,9 @@ int launch_sort_first_counts(const uint32_t* keys, int n, int key_bits, void* ws
     const int tiles = (n + kSortTile - 1) / kSortTile;
     const SortWs w = sort_ws_layout(ws, n);
     switch (bits) {
-        case 8: k_digit_counts<8><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, w.cnt[0], tiles, nullptr); break;
-        case 9: k_digit_counts<9><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, w.cnt[0], tiles, nullptr); break;
-        default: k_digit_counts<10><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, w.cnt[0], tiles, nullptr); break;
+        case 8: k_digit_counts<8><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, w.cnt[0], nullptr, nullptr); break;
+        case 9: k_digit_counts<9><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, w.cnt[0], nullptr, nullptr); break;
+        default: k_digit_counts<10><<<tiles, kSortThreads, 0, s>>>(keys, n, 0, w.cnt[0], nullptr, nullptr); break;
     }
     SD_LAUNCHED(s);
     return SD_OK;
@@ -601,10 +609,12 @@ int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t*
     // a count on the device: grids of about one wave that loop over the tiles in use
     const int count_grid = loop_grid(tiles, n_dev, kNumSMs * 8);
     const int scatter_grid = loop_grid(tiles, n_dev, kNumSMs * 4);
-    // The scatters add the next pass's counts into the second buffer, which must
-    // start at zero, and the column scan counts its CTAs on w.done; a sort leaves
-    // both zero, so a workspace that only ever serves this sort is cleared once.
+    // The count kernel and the scatters add chunk sums into w.S and the scatters add
+    // the next pass's counts into the second buffer, so both must start at zero, and
+    // the column scan counts its CTAs on w.done; a sort leaves all three zero, so a
+    // workspace that only ever serves this sort is cleared once.
     if (!ws_zeroed && (SD_CUDA(cudaMemsetAsync(cnt[1], 0, sizeof(unsigned) * ((size_t)tiles << bits), s)) ||
+                       SD_CUDA(cudaMemsetAsync(w.S, 0, sizeof(unsigned) * ((size_t)col_chunks(tiles) << bits), s)) ||
                        SD_CUDA(cudaMemsetAsync(w.done, 0, sizeof(unsigned), s))))
         return SD_E_CUDA;
 
@@ -624,15 +634,15 @@ int launch_sort_pairs(const uint32_t* keys_in, const int32_t* vals_in, uint32_t*
         if (p == 0 && !first_counts_ready) {
             const int g = count_grid;
             switch (bits) {
-                case 8: k_digit_counts<8><<<g, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles, n_dev); break;
-                case 9: k_digit_counts<9><<<g, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles, n_dev); break;
-                default: k_digit_counts<10><<<g, kSortThreads, 0, s>>>(kin, n, shift, counts, tiles, n_dev); break;
+                case 8: k_digit_counts<8><<<g, kSortThreads, 0, s>>>(kin, n, shift, counts, w.S, n_dev); break;
+                case 9: k_digit_counts<9><<<g, kSortThreads, 0, s>>>(kin, n, shift, counts, w.S, n_dev); break;
+                default: k_digit_counts<10><<<g, kSortThreads, 0, s>>>(kin, n, shift, counts, w.S, n_dev); break;
             }
             SD_LAUNCHED(s);
         }
-        // first-pass counts, however they were made, still need their chunk sums;
-        // later passes got theirs from the scatter's adds
-        if (p == 0 && (rc = col_sums(counts, tiles, 1 << bits, w.S, s, n_dev))) return rc;
+        // first-pass counts made elsewhere (the gather, launch_sort_first_counts) still
+        // need their chunk sums; the count kernel above and the scatters add theirs
+        if (p == 0 && first_counts_ready && (rc = col_sums(counts, tiles, 1 << bits, w.S, s, n_dev))) return rc;
         if ((rc = scan_offsets(counts, tiles, 1 << bits, w, s, n_dev))) return rc;
 #define SD_SCATTER(B, L)                                                                                   \
     k_digit_scatter<B, L><<<scatter_grid, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, shift, counts, next, w.S, \
