@@ -341,7 +341,12 @@ def _mover_scene(n, seed, speed):
     return pos, vel
 
 
-@pytest.mark.parametrize("G,n,speed", [(16, 40_000, 3.0), (64, 300_000, 1.0), (128, 200_000, 0.2)])
+# (16, 1000): fewer positions than one chunk of change words; (64, 262144): n / 32
+# an exact number of chunks, so the padding word opens a chunk of its own;
+# (64, 2.5M, fast): nearly every key changes, and the changed set's sort loops its
+# grids over more tiles than they hold CTAs
+@pytest.mark.parametrize("G,n,speed", [(16, 40_000, 3.0), (64, 300_000, 1.0), (128, 200_000, 0.2), (16, 1_000, 3.0),
+                                       (64, 262_144, 1.0), (64, 2_500_000, 40.0)])
 def test_merge_sort_equals_full_sort(cuda, G, n, speed):
     """After a sorted step the tiled order merges the keys that changed into the
     rest instead of radix-sorting everything; the particles must come out the

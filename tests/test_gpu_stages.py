@@ -76,6 +76,24 @@ def test_sort_permutation_bit_exact(cuda, lib, oracle, n):
     assert np.array_equal(kout.cpu().numpy()[:n].view(np.uint32), np.sort(keys, kind="stable"))
 
 
+def test_sort_with_a_dirty_workspace(cuda, lib):
+    """A workspace handed to sd_sort_pairs may hold anything: the sort clears the
+    sums it accumulates into before using them."""
+    rng = np.random.default_rng(5)
+    n, bits = 300_007, 18
+    keys = rng.integers(0, 1 << bits, n, dtype=np.int64).astype(np.uint32)
+    kin = dev(cuda, keys.view(np.int32))
+    kout, ktmp = cuda.empty_like(kin), cuda.empty_like(kin)
+    vout, vtmp = cuda.empty_like(kin), cuda.empty_like(kin)
+    w = ws(cuda, lib.sd_sort_workspace_bytes(n))
+    w.fill_(0xAB)
+    for _ in range(2):  # garbage, then the state a sort leaves
+        L.check(lib.sd_sort_pairs(kin.data_ptr(), None, kout.data_ptr(), vout.data_ptr(), ktmp.data_ptr(),
+                                  vtmp.data_ptr(), n, bits, w.data_ptr(), w.numel(), None), "sort")
+        sync(cuda)
+        assert np.array_equal(vout.cpu().numpy(), np.argsort(keys, kind="stable"))
+
+
 def test_sort_full_32_bits_and_values(cuda, lib):
     rng = np.random.default_rng(7)
     n = 300_001
