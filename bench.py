@@ -53,8 +53,10 @@ def kernel_bytes(n: int, G: int) -> dict:
     spec = 8.0 * G * G * (G // 2 + 4)  # bricked half spectrum, complex64
     cells = float(G) ** 3
     return {
-        "sort": 2 * (4 + 16) * n,                 # two 10-bit passes: count keys, move key + value
-        "row_table": 4 * n + 4 * (G * G + 1),
+        # steady state merges: read the new keys, write the permutation, plus the change
+        # bits (read twice) and their per-word prefixes (written once, read once)
+        "sort": 8 * n + 4 * (n / 32) * 4,
+        "row_table": 3 * 4 * (G * G + 1),         # old table and the changed set's in, new table out
         "pass_a_deposit": 20 * n + spec,          # perm + pos once; spectrum written
         "pass_b": 2 * spec,
         "pass_c": 2 * spec,

@@ -112,7 +112,16 @@ __global__ void __launch_bounds__(kChgThreads) k_chg_compact(const unsigned* __r
                                                              int32_t* __restrict__ ci, int* __restrict__ n_changed) {
     __shared__ unsigned red[kChgThreads / 32];
     unsigned before = 0u;  // changed positions in the chunks before this one
-    for (int c = threadIdx.x; c < (int)blockIdx.x; c += kChgThreads) before += chunk_cnt[c];
+    for (int c0 = 0; c0 < (int)blockIdx.x; c0 += 8 * kChgThreads) {  // eight loads in flight per thread
+        unsigned v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int c = c0 + q * kChgThreads + threadIdx.x;
+            v[q] = (c < (int)blockIdx.x) ? chunk_cnt[c] : 0u;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) before += v[q];
+    }
     before = block_sum(before, red);
     const size_t w0 = (size_t)blockIdx.x * kChunkWords + threadIdx.x * kChgWordsPer;
     unsigned w[8];
@@ -171,13 +180,36 @@ __global__ void k_merge_changed(const uint32_t* __restrict__ ck, const int32_t* 
 }
 
 // Thread per row r in [0, rows]: c_rows[r] = first rank of C with key >= r, and
-// the new row start = unchanged positions below the old one + c_rows[r].
+// the new row start = unchanged positions below the old one + c_rows[r]. The
+// search starts where r would fall if C were spread evenly over the rows and
+// gallops outwards to a bracket, which a few steps find for an even spread.
 __global__ void k_rows(const uint32_t* __restrict__ ck, const int* __restrict__ n_changed, int rows,
                        const unsigned* __restrict__ words, const unsigned* __restrict__ word_pre,
                        int* __restrict__ c_rows, int* __restrict__ row_start) {
     const int nc = *n_changed;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r <= rows; r += gridDim.x * blockDim.x) {
-        int lo = 0, hi = nc;
+        // bracket [lo, hi] with ck[lo - 1] < r <= ck[hi] (ck[-1] = -inf, ck[nc] = +inf)
+        const int g = (int)(((long long)r * nc) / (rows > 0 ? rows : 1));
+        int lo, hi;
+        if (g < nc && ck[g] < (uint32_t)r) {  // the answer lies above g
+            int step = 1;
+            lo = g + 1;
+            hi = g + 1;
+            while (hi < nc && ck[hi] < (uint32_t)r) {
+                lo = hi + 1;
+                hi = min(nc, hi + step);
+                step <<= 1;
+            }
+        } else {  // at or below g
+            int step = 1;
+            hi = g;
+            lo = g;
+            while (lo > 0 && ck[lo - 1] >= (uint32_t)r) {
+                hi = lo - 1;
+                lo = max(0, lo - step);
+                step <<= 1;
+            }
+        }
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
             if (ck[mid] < (uint32_t)r) lo = mid + 1;
