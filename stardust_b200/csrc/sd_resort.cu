@@ -25,9 +25,9 @@
 // Kernels, in order (the size of C stays on the device throughout):
 //   k_chg_count      changed positions per chunk of 512 words
 //   k_chg_compact    per word: changed positions before it; C in position order
-//   (radix sort of C by key, grids sized for the capacity, looping over tiles)
+//   (radix sort of C by key, on grids of about one wave looping over its tiles)
 //   k_merge_changed  output slot of every C entry
-//   k_rows           row table of C (binary search per row) and the new row table
+//   k_rows           row table of C (a galloping search per row) and the new row table
 //   k_merge_unchanged output slot of every unchanged position; clears the bits
 #include <cuda_runtime.h>
 #include <stdint.h>
