@@ -21,6 +21,9 @@
 // row r are the unchanged ones below the old row_start[r] plus the changed
 // ones with key < r. The permutation is the one the radix sort gives; the
 // sorted keys themselves are not written (the row table is all the step reads).
+// Every formula holds for any set of marked positions that contains the changed
+// ones: a marked position whose key did not change simply goes through C, so
+// bits left over from a step whose merge never ran cost time, not correctness.
 //
 // Kernels, in order (the size of C stays on the device throughout):
 //   k_chg_count      changed positions per chunk of 512 words

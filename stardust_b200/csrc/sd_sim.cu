@@ -521,7 +521,9 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     // or, when the next sort can merge, marked the changed ones
     s->counts_valid = sort && !incr_next;
     s->incr_ready = incr_next;
-    s->chg_dirty = incr_next;
+    // bits stay dirty until a merge or the clear above consumes them (a step that
+    // does not sort leaves them as they are)
+    if (incr_next) s->chg_dirty = true;
     s->mean_pending = true;
     if (timed) cudaEventRecord(s->ev[4], s->stream);
     s->ev_valid = timed;
@@ -1037,7 +1039,8 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
         {  // the graph's last step leaves what do_step leaves after a sorted step
             const bool incr_next = sort && s->rs_base && incr_possible(s);
             s->counts_valid = sort && !incr_next;
-            s->incr_ready = s->chg_dirty = incr_next;
+            s->incr_ready = incr_next;
+            if (incr_next) s->chg_dirty = true;
         }
         if (s->cfg.integrator == SD_INT_KDK) {
             s->lf_open = true;

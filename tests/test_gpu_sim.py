@@ -396,3 +396,31 @@ def test_merge_sort_with_particles_lost_and_keys_unchanged(cuda):
             outs.append(s.get_particles())
     assert np.array_equal(outs[0][0].view(np.int32), outs[1][0].view(np.int32))
     assert np.array_equal(outs[0][1].view(np.int32), outs[1][1].view(np.int32))
+
+
+def test_merge_sort_across_sort_interval_changes(cuda):
+    """Sorting every step, every other step or never, and every step again (eager
+    and graph-replayed): change bits written before the unsorted steps are never
+    merged, and the merges that follow still give the full sort's particles."""
+    G, n = 64, 200_000
+    pos, vel = _mover_scene(n, 5, 1.0)
+    outs = []
+    for full in (1, 0):
+        with make_sim(cuda, n, G, gravity=200.0, softening_cells=1.0, order=L.SD_ORDER_TILED, full_sort=full) as s:
+            s.set_particles(pos, vel)
+            got = []
+            for interval, eager in ((1, True), (2, True), (1, True), (1, False), (0, False), (1, False), (2, False),
+                                    (1, True)):
+                cfg = s.config()
+                cfg.sort_interval = interval
+                s.reconfigure(cfg)
+                if eager:
+                    for _ in range(3):
+                        s.step(1e-3)
+                else:
+                    s.steps(1e-3, 4)
+                got.append(s.get_particles())
+            outs.append(got)
+    for (p0, v0), (p1, v1) in zip(outs[0], outs[1]):
+        assert np.array_equal(p0.view(np.int32), p1.view(np.int32))
+        assert np.array_equal(v0.view(np.int32), v1.view(np.int32))
