@@ -486,7 +486,9 @@ __global__ void __launch_bounds__(kFftThreads, 5) k_pass_e(const float2* __restr
     extern __shared__ float2 sm[];
     float2* tw = sm;
     float2* s = sm + G;
-    const int by = blockIdx.x, bz = blockIdx.y;
+    // CTAs run from the last row bundle to the first: pass D ends on the high-z slabs, still in L2,
+    // and the gather starts on the low-z rows of phi written last here (same results, ~8 us less)
+    const int by = gridDim.x - 1 - blockIdx.x, bz = gridDim.y - 1 - blockIdx.y;
     for (int i = threadIdx.x; i < G; i += kFftThreads) tw[i] = tw_g[i];
     float4 v[PER];
 #pragma unroll
