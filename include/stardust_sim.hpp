@@ -52,6 +52,7 @@ struct SimConfig {
     int units = SD_UNITS_REFERENCE;
     bool diagnostics = false;
     bool keepDensity = true;
+    bool fullSort = false;             // true: no merge sort of the keys that changed (same results)
 
     sd_config toC() const {
         sd_config c;
@@ -70,6 +71,7 @@ struct SimConfig {
         c.units = units;
         c.diagnostics = diagnostics ? 1 : 0;
         c.keep_density = keepDensity ? 1 : 0;
+        c.full_sort = fullSort ? 1 : 0;
         c.preset = static_cast<int>(preset);
         c.dark_matter_fraction = darkMatterFraction;
         c.big_bang_shrink = bigBangShrink;
