@@ -76,9 +76,22 @@ struct PoissonIso {
     float table_scale = 0.f;
     bool forward_only = false;
 };
+// Work plan of the fused deposit (pos != nullptr). A row bundle's CTA reads the
+// particles of the 25 base rows whose stencils reach its 16 rows; a bundle whose
+// window holds more than `split` particles is shared by several CTAs, which add
+// their exact int64 partial rows into `acc` (the fixed-point grid, zero between
+// uses) and the last of them to finish transforms the rows. `ints` is scratch of
+// deposit_work_ints(G) ints, zeroed once when allocated and left zero by every use.
+struct DepositWork {
+    long long* acc = nullptr;
+    int* ints = nullptr;
+    int split = 0;
+};
+size_t deposit_work_ints(int G);
+int deposit_split(int n, int G);  // the particles per CTA above which a window is split
 int launch_poisson_ex(const PoissonPlan& p, const long long* acc, const float* rho, const float4* pos,
                       const int* perm, const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s,
-                      cudaEvent_t* ev = nullptr, const PoissonIso* iso = nullptr);
+                      cudaEvent_t* ev = nullptr, const PoissonIso* iso = nullptr, const DepositWork* dw = nullptr);
 size_t green_table_elems(int S);
 // Green spectrum of the isolated boundary on an S^3 transform box (plan of size S);
 // kernel_grid (S^3 floats) and spec are scratch.

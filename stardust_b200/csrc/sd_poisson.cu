@@ -140,136 +140,262 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_a(const float* __restrict_
     }
 }
 
-// ---- pass A fused with the CIC deposit (particles in SD_ORDER_TILED order) --------
-// The CTA for row bundle (by, bz) owns rows y in [4by, 4by+4), z in [4bz, 4bz+4).
-// Particles are sorted by the row of their CIC base cell, rows grouped in these
-// 4x4 bundles; row_start[r] .. row_start[r+1] is the slice of key-space row r.
-// The CTA reads the 25 base rows whose stencils reach its rows (y and z in
-// [4b-1, 4b+3]), adds each in-bundle corner weight, rounded once to a multiple
-// of 2^-32, into an int64 row buffer in shared memory, then converts and
-// transforms the rows exactly as pass A does. Integer sums make the density
-// independent of the order of the adds; no density grid is written.
+// ---- balanced fused deposit ---------------------------------------------------------
+// Scratch (DepositWork::ints) of a grid with NB = G^2/16 row bundles, NC = ceil(NB/256):
+//   items[NB]    CTAs sharing each bundle (>= 1)
+//   xpre[NB]     exclusive prefix of (items - 1) inside each block of 256 bundles
+//   arrive[NB]   CTAs of a shared bundle done so far (zero between uses)
+//   cta_sum[NC], cta_pre[NC + 1]   per-block totals and their exclusive prefix
+//   plan_done    blocks of the plan kernel done (zero between uses)
 template <int G>
-__global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4* __restrict__ pos,
-                                                                    const int* __restrict__ perm,
-                                                                    const int* __restrict__ row_start,
-                                                                    float* __restrict__ rho_keep,
-                                                                    float2* __restrict__ spec,
-                                                                    const float2* __restrict__ tw_g) {
+struct DepPlan {
+    static constexpr int NB = G * G / 16;
+    static constexpr int NC = (NB + 255) / 256;
+    static constexpr int kItems = 0, kXpre = NB, kArrive = 2 * NB, kCtaSum = 3 * NB, kCtaPre = 3 * NB + NC,
+                         kDone = 3 * NB + 2 * NC + 1, kInts = kDone + 1;
+};
+
+// The 25 base rows whose CIC stencils reach the 16 rows of bundle b = bz*(G/4)+by,
+// as 7 ranges of the sorted particles: r = 0 the bundle's own rows (16 consecutive
+// keys); r = 1 the rows z_l = 3 of the bundle below in z (4 consecutive keys);
+// r = 2..5 the rows y_l = 3, z_l = r - 2 of the bundle below in y; r = 6 the row
+// y_l = z_l = 3 of the bundle below in both. Neighbours wrap (periodic box).
+template <int G>
+__device__ __forceinline__ void window_range(int b, int r, const int* __restrict__ rs, int& lo, int& hi) {
+    constexpr int TB = G / 4;
+    const int by = b & (TB - 1), bz = b / TB;
+    const int bym = (by + TB - 1) & (TB - 1), bzm = (bz + TB - 1) & (TB - 1);
+    int k0, k1;
+    if (r == 0) {
+        k0 = 16 * b;
+        k1 = k0 + 16;
+    } else if (r == 1) {
+        k0 = 16 * (bzm * TB + by) + 12;
+        k1 = k0 + 4;
+    } else if (r == 6) {
+        k0 = 16 * (bzm * TB + bym) + 15;
+        k1 = k0 + 1;
+    } else {
+        k0 = 16 * (bz * TB + bym) + 4 * (r - 2) + 3;
+        k1 = k0 + 1;
+    }
+    lo = rs[k0];
+    hi = rs[k1];
+}
+
+// Exclusive scan of one int per thread over a block of 256 threads; *total gets the sum.
+__device__ __forceinline__ int block_excl_scan256(int v, int* total) {
+    __shared__ int wsum[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        int x = lane < 8 ? wsum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += t;
+        }
+        if (lane < 8) wsum[lane] = x;
+    }
+    __syncthreads();
+    const int excl = inc - v + (warp ? wsum[warp - 1] : 0);
+    *total = wsum[7];
+    __syncthreads();  // wsum may be reused by the next call
+    return excl;
+}
+
+// How many CTAs share each bundle: ceil(window particles / split), at least 1,
+// and where each bundle's extra CTAs start. The last block to finish turns the
+// block totals into their prefix.
+template <int G>
+__global__ void __launch_bounds__(256) k_deposit_plan(const int* __restrict__ rs, int* __restrict__ w, int split) {
+    using P = DepPlan<G>;
+    const int b = blockIdx.x * 256 + threadIdx.x;
+    int extra = 0;
+    if (b < P::NB) {
+        int total = 0;
+#pragma unroll
+        for (int r = 0; r < 7; ++r) {
+            int lo, hi;
+            window_range<G>(b, r, rs, lo, hi);
+            total += hi - lo;
+        }
+        const int items = total > split ? (int)(((long long)total + split - 1) / split) : 1;
+        w[P::kItems + b] = items;
+        extra = items - 1;
+    }
+    int sum;
+    const int excl = block_excl_scan256(extra, &sum);
+    if (b < P::NB) w[P::kXpre + b] = excl;
+    if (threadIdx.x == 0) w[P::kCtaSum + blockIdx.x] = sum;
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(reinterpret_cast<unsigned*>(w + P::kDone), 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // NC <= 256 blocks (G <= 1024)
+    const int v = threadIdx.x < P::NC ? __ldcg(w + P::kCtaSum + threadIdx.x) : 0;
+    int all;
+    const int pre = block_excl_scan256(v, &all);
+    if (threadIdx.x < P::NC) w[P::kCtaPre + threadIdx.x] = pre;
+    if (threadIdx.x == 0) {
+        w[P::kCtaPre + P::NC] = all;
+        w[P::kDone] = 0;
+    }
+}
+
+// One CTA's share (slice `slice` of `items`) of bundle b: deposit its particles
+// into int64 row sums in shared memory; if the bundle is shared, add the sums into
+// the fixed-point grid and let the last CTA continue with the whole bundle; then
+// convert, transform the 16 rows along x and store the spectrum bricks.
+// A warp whose particles share few base cells (dense rows) first sums equal
+// corners across its lanes, so one lane per cell adds them: the integer sums
+// are the same in any order, and fewer adds land on the same shared word.
+template <int G>
+__device__ __forceinline__ void deposit_bundle(int b, int slice, int items, const float4* __restrict__ pos,
+                                               const int* __restrict__ perm, const int* __restrict__ row_start,
+                                               float* __restrict__ rho_keep, float2* __restrict__ spec,
+                                               const DepositWork& w, unsigned* __restrict__ arrive) {
     using T = Geo<G>;
-    constexpr int H = T::H, NBX = T::NBX, NT = kDepositThreads;
+    constexpr int H = T::H, NBX = T::NBX, NT = kDepositThreads, TB = G / 4;
+    constexpr int RS = G + 2;  // u64 words per sum row: rows 16 bytes out of step across banks
+    constexpr int kAggGroups = 16;
     extern __shared__ float2 sm[];
-    float2* tw = sm;
-    // The int64 fixed-point sums, as two 32-bit words per cell (lo[16][RS], hi[16][RS]),
-    // share their storage with the complex line buffer used after the conversion.
-    // Rows are RS = G + 4 words apart, so the row-parallel 16-byte reads of the
-    // conversion fall in different banks.
-    constexpr int RS = G + 4;
-    unsigned* acc_lo = reinterpret_cast<unsigned*>(sm + G);
-    unsigned* acc_hi = acc_lo + 16 * RS;
+    const float2* tw = sm;
+    unsigned long long* sums = reinterpret_cast<unsigned long long*>(sm + G);
     float2* s = sm + G;
-    __shared__ int range_lo[25], range_off[26];
-    const int by = blockIdx.x, bz = blockIdx.y;
+    __shared__ int r_lo[7], r_off[8];
+    __shared__ int s_last;
+    const int by = b & (TB - 1), bz = b / TB;
     const int m = G - 1;
-    // The row table is the head of this CTA's chain of dependent loads (row
-    // starts -> permutation -> positions): warp 0 issues it before the twiddle
-    // loads and the clearing of the sums, which then overlap its latency.
     const int j = threadIdx.x;
     int lo = 0, len = 0;
-    if (j < 25) {
-        // source rows (iy, iz) = (4by - 1 + j % 5, 4bz - 1 + j / 5)
-        const int iy = (4 * by - 1 + j % 5) & m, iz = (4 * bz - 1 + j / 5) & m;
-        const int key = ((iz >> 2) * (G / 4) + (iy >> 2)) * 16 + (iz & 3) * 4 + (iy & 3);
-        lo = row_start[key];
-        len = row_start[key + 1] - lo;
+    if (j < 7) {
+        int hi;
+        window_range<G>(b, j, row_start, lo, hi);
+        len = hi - lo;
     }
-    for (int i = threadIdx.x; i < G; i += NT) tw[i] = tw_g[i];
-    for (int i = threadIdx.x; i < 8 * RS; i += NT) reinterpret_cast<uint4*>(acc_lo)[i] = make_uint4(0u, 0u, 0u, 0u);
+    __syncthreads();  // the shared buffers of the previous bundle are free
+    for (int i = threadIdx.x; i < 8 * RS; i += NT) reinterpret_cast<uint4*>(sums)[i] = make_uint4(0u, 0u, 0u, 0u);
     if (threadIdx.x < 32) {
-        int inc = len;  // inclusive scan of the lengths across the warp
+        int inc = len;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
+        for (int o = 1; o < 8; o <<= 1) {
             const int t = __shfl_up_sync(0xffffffffu, inc, o);
             if (j >= o) inc += t;
         }
-        if (j < 25) {
-            range_lo[j] = lo;
-            range_off[j + 1] = inc;
+        if (j < 7) {
+            r_lo[j] = lo;
+            r_off[j + 1] = inc;
         }
-        if (j == 0) range_off[0] = 0;
+        if (j == 0) r_off[0] = 0;
     }
     __syncthreads();
-    const int total = range_off[25];
-    const bool split16 = total < 65536;
-    // Up to kBatch particles per thread and round: their slots are located first
-    // (binary search of the row offsets), then all permutation loads and then all
-    // position loads are issued before any result is used.
+    const int total = r_off[7];
+    const int f_lo = (int)((long long)total * slice / items);
+    const int f_hi = (int)((long long)total * (slice + 1) / items);
+    const int lane = threadIdx.x & 31;
     constexpr int kBatch = 4;
-    for (int f0 = threadIdx.x; f0 < total; f0 += kBatch * NT) {
+    // warp-uniform loop: lane f = base + q * NT + lane
+    for (int base = f_lo + (threadIdx.x & ~31); base < f_hi; base += kBatch * NT) {
         int src[kBatch];
 #pragma unroll
-        for (int b = 0; b < kBatch; ++b) {
-            const int f = f0 + b * NT;
-            src[b] = -1;
-            if (f < total) {
-                int r = 0;  // largest r < 25 with range_off[r] <= f
-#pragma unroll
-                for (int step = 16; step > 0; step >>= 1)
-                    if (r + step < 25 && range_off[r + step] <= f) r += step;
-                src[b] = range_lo[r] + (f - range_off[r]);
+        for (int q = 0; q < kBatch; ++q) {
+            const int f = base + q * NT + lane;
+            src[q] = -1;
+            if (f < f_hi) {
+                int r = (r_off[4] <= f) ? 4 : 0;  // largest r < 7 with r_off[r] <= f
+                if (r + 2 < 7 && r_off[r + 2] <= f) r += 2;
+                if (r + 1 < 7 && r_off[r + 1] <= f) r += 1;
+                src[q] = r_lo[r] + (f - r_off[r]);
             }
         }
         if (perm) {
 #pragma unroll
-            for (int b = 0; b < kBatch; ++b)
-                if (src[b] >= 0) src[b] = perm[src[b]];
+            for (int q = 0; q < kBatch; ++q)
+                if (src[q] >= 0) src[q] = perm[src[q]];
         }
         float4 pb[kBatch];
 #pragma unroll
-        for (int b = 0; b < kBatch; ++b)
-            if (src[b] >= 0) pb[b] = pos[src[b]];
+        for (int q = 0; q < kBatch; ++q) pb[q] = (src[q] >= 0) ? pos[src[q]] : make_float4(-1.f, -1.f, -1.f, 0.f);
 #pragma unroll
-        for (int b = 0; b < kBatch; ++b) {
-            if (f0 + b * NT >= total) break;
-            const float4 p = pb[b];
-            if (p.x < 0.f) continue;  // empty slots sort into row 0
+        for (int q = 0; q < kBatch; ++q) {
+            if (base + q * NT >= f_hi) break;  // warp-uniform
+            const float4 p = pb[q];
+            const bool valid = p.x >= 0.f;  // empty slots sort into row 0
             int ix, iy, iz;
             float fx, fy, fz;
             cic_axis(p.x, G, ix, fx);
             cic_axis(p.y, G, iy, fy);
             cic_axis(p.z, G, iz, fz);
             const int x0 = ix & m, x1 = (ix + 1) & m;
+            const unsigned cell =
+                valid ? (unsigned)((((iz & m) * G) + (iy & m)) * G + x0) : (0x80000000u | (unsigned)lane);
+            const unsigned grp = __match_any_sync(0xffffffffu, cell);
+            const bool leader = (grp & lanemask_lt()) == 0;
+            const bool merge = __popc(__ballot_sync(0xffffffffu, leader)) <= kAggGroups;  // warp-uniform
+            if (!merge && !valid) continue;
 #pragma unroll
             for (int oyz = 0; oyz < 4; ++oyz) {
-                const int oy = oyz & 1, oz = oyz >> 1;
-                const int yl = ((iy + oy) & m) - 4 * by;
-                const int zl = ((iz + oz) & m) - 4 * bz;
-                if ((unsigned)yl >= 4u || (unsigned)zl >= 4u) continue;
+                const int yl = ((iy + (oyz & 1)) & m) - 4 * by;
+                const int zl = ((iz + (oyz >> 1)) & m) - 4 * bz;
+                const bool in = valid && (unsigned)yl < 4u && (unsigned)zl < 4u;
+                if (!merge && !in) continue;
                 const int rowc = (zl * 4 + yl) * RS;
 #pragma unroll
                 for (int ox = 0; ox < 2; ++ox) {
-                    const unsigned long long q =
-                        (unsigned long long)fixed_weight(cic_weight(ox | (oy << 1) | (oz << 2), fx, fy, fz));
-                    const int c = rowc + (ox ? x1 : x0);
-                    if (split16) {
-                        // q in [0, 2^32] as (q >> 16) * 2^16 + (q & 0xffff): with fewer than
-                        // 2^16 particles in the tile neither 32-bit sum can overflow, so two
-                        // plain adds (no returned value) keep the 64-bit total exact.
-                        atomicAdd(acc_hi + c, (unsigned)(q >> 16));
-                        atomicAdd(acc_lo + c, (unsigned)(q & 0xffffu));
-                    } else {
-                        // add the low word and carry into the high word; atomicAdd returns the
-                        // previous low word, so every wrap is seen by exactly one add
-                        const unsigned lo = (unsigned)q;
-                        const unsigned old = atomicAdd(acc_lo + c, lo);
-                        const unsigned up = (unsigned)(q >> 32) + ((old + lo < old) ? 1u : 0u);
-                        if (up) atomicAdd(acc_hi + c, up);
+                    unsigned long long qv =
+                        in ? (unsigned long long)fixed_weight(cic_weight(ox | (oyz << 1), fx, fy, fz)) : 0ull;
+                    if (merge) {
+                        // lanes with the same base cell share every corner cell: sum the
+                        // weight over the group in two 16-bit halves (no overflow for 32
+                        // lanes); the lowest lane adds the exact total
+                        const unsigned hi = __reduce_add_sync(grp, (unsigned)(qv >> 16));
+                        const unsigned lo16 = __reduce_add_sync(grp, (unsigned)(qv & 0xffffu));
+                        qv = ((unsigned long long)hi << 16) + (unsigned long long)lo16;
+                        if (!leader || !in) continue;
                     }
+                    atomicAdd(sums + rowc + (ox ? x1 : x0), qv);
                 }
             }
         }
     }
     __syncthreads();
+    if (items > 1) {
+        // a shared bundle: every CTA adds its rows into the fixed-point grid; the last
+        // to arrive reads the complete sums back (and leaves the grid zero)
+        unsigned long long* g = reinterpret_cast<unsigned long long*>(w.acc);
+#pragma unroll 1
+        for (int u = threadIdx.x; u < 16 * G; u += NT) {
+            const int l = u / G, x = u & m;
+            const unsigned long long v = sums[l * RS + x];
+            if (v) atomicAdd(g + ((size_t)(4 * bz + (l >> 2)) * G + 4 * by + (l & 3)) * G + x, v);
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) s_last = atomicAdd(arrive + b, 1u) == (unsigned)(items - 1);
+        __syncthreads();
+        if (!s_last) return;
+        __threadfence();
+#pragma unroll 1
+        for (int u = threadIdx.x; u < 16 * G; u += NT) {
+            const int l = u / G, x = u & m;
+            const size_t gi = ((size_t)(4 * bz + (l >> 2)) * G + 4 * by + (l & 3)) * G + x;
+            sums[l * RS + x] = __ldcg(g + gi);
+            g[gi] = 0ull;
+        }
+        if (threadIdx.x == 0) arrive[b] = 0u;
+        __syncthreads();
+    }
     // int64 rows -> complex positions z[m] = x[2m] + i x[2m+1] on line l = z_l*4 + y_l,
     // staged through registers because the line buffer overlays the sums.
     constexpr int CITEMS = 16 * (H / 2);
@@ -280,13 +406,10 @@ __global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4
         const int u = threadIdx.x + p * NT;
         if (CITEMS % NT == 0 || u < CITEMS) {
             const int l = u & 15, mp = u >> 4;
-            const uint4 lo = *reinterpret_cast<const uint4*>(acc_lo + l * RS + 4 * mp);
-            const uint4 hi = *reinterpret_cast<const uint4*>(acc_hi + l * RS + 4 * mp);
-            const int sh = split16 ? 16 : 32;
-            cv[p] = make_float4(fixed_to_float((long long)(((unsigned long long)hi.x << sh) + lo.x)),
-                                fixed_to_float((long long)(((unsigned long long)hi.y << sh) + lo.y)),
-                                fixed_to_float((long long)(((unsigned long long)hi.z << sh) + lo.z)),
-                                fixed_to_float((long long)(((unsigned long long)hi.w << sh) + lo.w)));
+            const ulonglong2 a = *reinterpret_cast<const ulonglong2*>(sums + l * RS + 4 * mp);
+            const ulonglong2 c = *reinterpret_cast<const ulonglong2*>(sums + l * RS + 4 * mp + 2);
+            cv[p] = make_float4(fixed_to_float((long long)a.x), fixed_to_float((long long)a.y),
+                                fixed_to_float((long long)c.x), fixed_to_float((long long)c.y));
         }
     }
     __syncthreads();
@@ -320,8 +443,8 @@ __global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4
         const float2 zk = s[k * 16 + l], zc = s[(H - k) * 16 + l];
         const float er = 0.5f * (zk.x + zc.x), ei = 0.5f * (zk.y - zc.y);
         const float orr = 0.5f * (zk.y + zc.y), oi = -0.5f * (zk.x - zc.x);
-        const float2 w = tw[k];
-        s[k * 16 + l] = make_float2(er + (w.x * orr - w.y * oi), ei + (w.x * oi + w.y * orr));
+        const float2 wk = tw[k];
+        s[k * 16 + l] = make_float2(er + (wk.x * orr - wk.y * oi), ei + (wk.x * oi + wk.y * orr));
         if (2 * k != H) {
             const float2 w2 = tw[H - k];
             s[(H - k) * 16 + l] = make_float2(er + (w2.x * orr + w2.y * oi), -ei + (w2.y * orr - w2.x * oi));
@@ -331,8 +454,47 @@ __global__ void __launch_bounds__(kDepositThreads) k_pass_a_deposit(const float4
     for (int u = threadIdx.x; u < NBX * 32; u += NT) {
         const int bx = u >> 5, c = u & 31;
         const int l = (c >> 3) * 4 + ((c >> 1) & 3), kx = bx * 4 + (c & 1) * 2;
-        const float2 a = s[kx * 16 + l], b = s[(kx + 1) * 16 + l];
-        *reinterpret_cast<float4*>(spec + T::brick(bx, by, bz) + 2 * c) = make_float4(a.x, a.y, b.x, b.y);
+        const float2 a = s[kx * 16 + l], c2 = s[(kx + 1) * 16 + l];
+        *reinterpret_cast<float4*>(spec + T::brick(bx, by, bz) + 2 * c) = make_float4(a.x, a.y, c2.x, c2.y);
+    }
+}
+
+// Grid: X CTAs that take the extra shares of heavy bundles (first, so they start
+// early), then one CTA per bundle for its first share. 40 registers at G = 512
+// keep three 70 KB CTAs per SM; smaller grids need more for their FFT stages.
+template <int G>
+__global__ void __launch_bounds__(kDepositThreads, G >= 512 ? 3 : 2)
+    k_pass_a_deposit_bal(const float4* __restrict__ pos, const int* __restrict__ perm,
+                         const int* __restrict__ row_start, float* __restrict__ rho_keep, float2* __restrict__ spec,
+                         const float2* __restrict__ tw_g, DepositWork w) {
+    using P = DepPlan<G>;
+    extern __shared__ float2 sm[];
+    for (int i = threadIdx.x; i < G; i += kDepositThreads) sm[i] = tw_g[i];  // ordered by the first barrier
+    const int* items = w.ints + P::kItems;
+    const int* xpre = w.ints + P::kXpre;
+    const int* cta_pre = w.ints + P::kCtaPre;
+    unsigned* arrive = reinterpret_cast<unsigned*>(w.ints + P::kArrive);
+    const int X = (int)gridDim.x - P::NB;
+    const bool first = (int)blockIdx.x >= X;  // a bundle's first share, then done
+    const int extras = first ? 0 : cta_pre[P::NC];
+    for (int e = first ? 0 : (int)blockIdx.x; first || e < extras; e += X) {
+        int b, slice;
+        if (first) {
+            b = (int)blockIdx.x - X;
+            slice = 0;
+        } else {
+            // the bundle of extra share e: the last b whose extras start at or before e
+            int lo = 0, hi = P::NB - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (cta_pre[mid >> 8] + xpre[mid] <= e) lo = mid;
+                else hi = mid - 1;
+            }
+            b = lo;
+            slice = 1 + e - (cta_pre[lo >> 8] + xpre[lo]);
+        }
+        deposit_bundle<G>(b, slice, items[b], pos, perm, row_start, rho_keep, spec, w, arrive);
+        if (first) break;
     }
 }
 
@@ -551,9 +713,16 @@ struct Launcher {
     static size_t smem_bd() { return sizeof(float2) * ((size_t)G + 16 * (size_t)G); }
     static size_t smem_c() { return sizeof(float2) * ((size_t)G + (T::H + 2) / 2 + 1 + 16 * (size_t)G); }
     // the line buffer (16 * PX float2) overlays the 32-bit sum words (2 * 16 * (G + 4))
-    static size_t smem_dep() {
-        const size_t lines = sizeof(float2) * 16 * (size_t)T::PX, sums = 2 * sizeof(unsigned) * 16 * (size_t)(G + 4);
+    // the balanced deposit keeps one u64 word per cell, rows G + 2 words apart, under
+    // the line buffer
+    static size_t smem_bal() {
+        const size_t lines = sizeof(float2) * 16 * (size_t)T::PX, sums = sizeof(unsigned long long) * 16 * (size_t)(G + 2);
         return sizeof(float2) * (size_t)G + (lines > sums ? lines : sums);
+    }
+    // CTAs that take the extra shares of heavy bundles
+    static int extra_ctas() {
+        const int nb = DepPlan<G>::NB / 4;
+        return nb < 8 ? 8 : (nb > 296 ? 296 : nb);
     }
 
     static int configure() {
@@ -568,7 +737,8 @@ struct Launcher {
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_c<G, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_c<G, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_e<G>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
-        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a_deposit<G>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a_deposit_bal<G>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                           carve));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a<G, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ae()));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a<G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ae()));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_y<G, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -579,19 +749,23 @@ struct Launcher {
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_c<G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c()));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_c<G, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c()));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_e<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ae()));
-        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a_deposit<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem_dep()));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a_deposit_bal<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem_bal()));
         return rc == SD_OK ? SD_OK : SD_E_CUDA;
     }
 
     static int run(const PoissonPlan& p, const long long* acc, const float* rho, const float4* pos, const int* perm,
                    const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s, cudaEvent_t* ev,
-                   const PoissonIso* iso) {
+                   const PoissonIso* iso, const DepositWork* dw) {
         const dim3 grid_rows(T::NBY, T::NBZ), grid_y(T::NBX, T::NBZ), grid_z(T::NBX, T::NBY);
         const int src_g = (iso && iso->src_g > 0) ? iso->src_g : G;
-        if (pos)
-            k_pass_a_deposit<G><<<grid_rows, kDepositThreads, smem_dep(), s>>>(pos, perm, row_start, keep, spec, p.tw);
-        else if (acc)
+        if (pos) {
+            if (!dw || !dw->acc || !dw->ints || dw->split <= 0) return fail(SD_E_ARG, "fused deposit: no work plan");
+            k_deposit_plan<G><<<DepPlan<G>::NC, 256, 0, s>>>(row_start, dw->ints, dw->split);
+            SD_LAUNCHED(s);
+            k_pass_a_deposit_bal<G><<<extra_ctas() + DepPlan<G>::NB, kDepositThreads, smem_bal(), s>>>(
+                pos, perm, row_start, keep, spec, p.tw, *dw);
+        } else if (acc)
             k_pass_a<G, 1><<<grid_rows, kFftThreads, smem_ae(), s>>>(nullptr, const_cast<long long*>(acc), keep, spec,
                                                                      p.tw, src_g);
         else
@@ -636,6 +810,26 @@ int poisson_configure(int G) {
 
 }  // namespace
 
+size_t deposit_work_ints(int G) {
+    switch (G) {
+        case 16: return DepPlan<16>::kInts;
+        case 32: return DepPlan<32>::kInts;
+        case 64: return DepPlan<64>::kInts;
+        case 128: return DepPlan<128>::kInts;
+        case 256: return DepPlan<256>::kInts;
+        case 512: return DepPlan<512>::kInts;
+        default: return 0;
+    }
+}
+
+int deposit_split(int n, int G) {
+    // about five times a window's mean particle count (a window spans 25 rows for a
+    // bundle's 16), and at least 2048
+    const long long nb = (long long)G * G / 16;
+    const long long t = 5ll * (long long)n / (nb > 0 ? nb : 1);
+    return (int)(t < 2048 ? 2048 : (t > (1 << 30) ? (1 << 30) : t));
+}
+
 size_t poisson_spectrum_elems(int G) { return (size_t)G * G * (size_t)(G / 2 + 4); }
 
 int poisson_plan_build(PoissonPlan& p, int G, float soft) {
@@ -678,14 +872,14 @@ int launch_poisson(const PoissonPlan& p, const long long* acc, const float* rho,
 
 int launch_poisson_ex(const PoissonPlan& p, const long long* acc, const float* rho, const float4* pos,
                       const int* perm, const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s,
-                      cudaEvent_t* ev, const PoissonIso* iso) {
+                      cudaEvent_t* ev, const PoissonIso* iso, const DepositWork* dw) {
     switch (p.G) {
-        case 16: return Launcher<16>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso);
-        case 32: return Launcher<32>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso);
-        case 64: return Launcher<64>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso);
-        case 128: return Launcher<128>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso);
-        case 256: return Launcher<256>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso);
-        case 512: return Launcher<512>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso);
+        case 16: return Launcher<16>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso, dw);
+        case 32: return Launcher<32>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso, dw);
+        case 64: return Launcher<64>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso, dw);
+        case 128: return Launcher<128>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso, dw);
+        case 256: return Launcher<256>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso, dw);
+        case 512: return Launcher<512>::run(p, acc, rho, pos, perm, row_start, keep, spec, phi, s, ev, iso, dw);
         default: return fail(SD_E_UNSUPPORTED, "poisson: grid size %d not supported", p.G);
     }
 }

@@ -145,7 +145,8 @@ void free_buffers(sd_sim* s) {
     if (s->sort_ws) cudaFree(s->sort_ws);
     s->sort_ws = nullptr;
     s->sort_ws_bytes = 0;
-    free_dev(s->acc); free_dev(s->row_start); free_dev(s->spec); free_dev(s->phi); free_dev(s->rho);
+    free_dev(s->acc); free_dev(s->row_start); free_dev(s->dep_ints); free_dev(s->spec); free_dev(s->phi);
+    free_dev(s->rho);
     free_dev(s->green);
     hydro_free(s->hydro);
     if (s->rs_base) cudaFree(s->rs_base);
@@ -179,6 +180,7 @@ size_t estimate_bytes(int n, int G, int boundary) {
     b += (sizeof(uint32_t) * 3 + sizeof(int32_t) * 2) * N;
     b += sort_workspace_bytes((int)N);
     b += sizeof(long long) * cells;                    // fixed-point deposit
+    b += sizeof(int) * deposit_work_ints(G);           // the fused deposit's work plan
     b += sizeof(float2) * poisson_spectrum_elems(S);
     b += sizeof(float) * (box + cells);                // phi, kept density
     if (S != G) b += sizeof(float) * green_table_elems(S);
@@ -211,6 +213,7 @@ int allocate(sd_sim* s) {
     if (!rc && SD_CUDA(cudaMemset(s->sort_ws, 0, s->sort_ws_bytes))) rc = SD_E_CUDA;
     rc = rc ? rc : alloc_dev(s->acc, cells);
     rc = rc ? rc : alloc_dev(s->row_start, (size_t)s->G * s->G + 1);
+    rc = rc ? rc : alloc_dev(s->dep_ints, deposit_work_ints(s->G));
     rc = rc ? rc : alloc_dev(s->spec, poisson_spectrum_elems(S));
     rc = rc ? rc : alloc_dev(s->phi, box);
     if (!rc && isolated(s)) rc = alloc_dev(s->green, green_table_elems(S));
@@ -235,6 +238,7 @@ int allocate(sd_sim* s) {
     }
     // zeroed state: empty slots, clear fixed-point grid, no pending mean
     if (SD_CUDA(cudaMemsetAsync(s->acc, 0, sizeof(long long) * cells, s->stream)) ||
+        SD_CUDA(cudaMemsetAsync(s->dep_ints, 0, sizeof(int) * deposit_work_ints(s->G), s->stream)) ||
         SD_CUDA(cudaMemsetAsync(s->mean, 0, sizeof(float) * 4, s->stream)) ||
         SD_CUDA(cudaMemsetAsync(s->mom, 0, sizeof(double) * 8, s->stream)) ||
         SD_CUDA(cudaMemsetAsync(s->diag_count, 0, sizeof(unsigned long long), s->stream)) ||
@@ -465,9 +469,13 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     }
     if (timed) cudaEventRecord(s->ev[2], s->stream);
     PoissonIso io;
+    DepositWork dw;
+    dw.acc = s->acc;
+    dw.ints = s->dep_ints;
+    dw.split = deposit_split(s->N, s->G);
     if ((rc = launch_poisson_ex(s->plan, fused ? nullptr : s->acc, nullptr, fused ? s->pos : nullptr, perm,
                                 s->row_start, keep ? s->rho : nullptr, s->spec, s->phi, s->stream,
-                                timed ? s->pev : nullptr, iso_opts(s, io))))
+                                timed ? s->pev : nullptr, iso_opts(s, io), &dw)))
         return sim_error(s, rc);
     if (keep) s->rho_valid = true;
     if (timed) cudaEventRecord(s->ev[3], s->stream);

@@ -27,6 +27,7 @@ struct sd_sim {
     size_t sort_ws_bytes = 0;
     long long* acc = nullptr;
     int* row_start = nullptr;    // key-space row starts of the sorted particles (tiled order)
+    int* dep_ints = nullptr;     // work plan of the fused deposit (deposit_work_ints(G), zero between uses)
     float2* spec = nullptr;     // bricked spectrum, transformed in place
     float* phi = nullptr;
     float* rho = nullptr;        // kept density (keep_density)

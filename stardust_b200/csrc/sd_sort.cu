@@ -451,41 +451,33 @@ __global__ void k_copy_keys(const uint32_t* __restrict__ kin, const int32_t* __r
     vout[i] = vin ? vin[i] : i;
 }
 
-// Sorted row keys (tiled order: key = row) -> row_start[r] = first i with key >= r.
-// Thread i writes row_start[r] = i for every r in (keys[i-1], keys[i]]; the last
-// thread closes the tail up to `rows` with n.
-// Each thread covers 8 consecutive indices (two 16-byte key loads plus the key
-// before them), so the kernel streams the keys instead of waiting on them.
-constexpr int kBoundsPer = 8;
+// Sorted row keys (tiled order: key = row) -> row_start[r] = first i with key >= r,
+// for r in [0, rows]; keys are below `rows`, so row_start[rows] = n.
+// One thread per row runs a lower-bound search over the keys. The work is the
+// same for every row, however the particles cluster: a scan that fills the rows
+// between consecutive keys leaves one thread to write every row of a long empty
+// run, and a clustered scene is mostly empty rows. Neighbouring rows take the
+// same first steps of the search, so those loads are shared in L1/L2.
 __global__ void k_row_bounds(const uint32_t* __restrict__ keys, int n, int rows, int* __restrict__ row_start) {
-    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * kBoundsPer;
-    if (i0 > n) return;
-    uint32_t k[kBoundsPer];
-    if (i0 + kBoundsPer <= n) {
-        const uint4 a = *reinterpret_cast<const uint4*>(keys + i0);
-        const uint4 b = *reinterpret_cast<const uint4*>(keys + i0 + 4);
-        k[0] = a.x; k[1] = a.y; k[2] = a.z; k[3] = a.w;
-        k[4] = b.x; k[5] = b.y; k[6] = b.z; k[7] = b.w;
-    } else {
-#pragma unroll
-        for (int j = 0; j < kBoundsPer; ++j) k[j] = (i0 + j < n) ? keys[i0 + j] : 0u;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r > rows) return;
+    int lo = 0, len = n;
+    while (len > 0) {
+        const int half = len >> 1;
+        if (__ldg(keys + lo + half) < (uint32_t)r) {
+            lo += half + 1;
+            len -= half + 1;
+        } else {
+            len = half;
+        }
     }
-    int lo = (i0 == 0) ? 0 : (int)min(keys[i0 - 1] + 1u, (uint32_t)rows);
-#pragma unroll
-    for (int j = 0; j < kBoundsPer; ++j) {
-        const int i = i0 + j;
-        if (i > n) break;
-        const int hi = (i == n) ? rows + 1 : (int)min(k[j] + 1u, (uint32_t)rows);
-        for (int r = lo; r < hi; ++r) row_start[r] = i;
-        if (hi > lo) lo = hi;
-    }
+    row_start[r] = lo;
 }
 
 }  // namespace
 
 int launch_row_bounds(const uint32_t* keys, int n, int rows, int* row_start, cudaStream_t s) {
-    const int threads = (n + 1 + kBoundsPer - 1) / kBoundsPer;
-    k_row_bounds<<<(threads + 255) / 256, 256, 0, s>>>(keys, n, rows, row_start);
+    k_row_bounds<<<(rows + 1 + 255) / 256, 256, 0, s>>>(keys, n, rows, row_start);
     SD_LAUNCHED(s);
     return SD_OK;
 }
