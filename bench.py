@@ -245,6 +245,18 @@ def run_ours(args, rank, world):
     if dist:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
     e2e_ms = float(t.item())
+    # the force error of the step's field: the accelerations of the current
+    # positions against FP64 particle-mesh on the same grid, at 65,536 sampled
+    # particles (the FP64 direct/Ewald judge is reported by the learned comparison)
+    from stardust_b200.ewald import force_error, pm_accel_f64
+
+    p_now, _ = sim.get_particles()
+    a_now = sim.accel()
+    live = np.nonzero(p_now[:, 0] >= 0.0)[0]
+    sample = np.random.default_rng(0).choice(live, min(65536, len(live)), replace=False)
+    pot_scale = 4.0 * np.pi * float(G) ** 3 / n  # Newton units, G = 1, each particle 1/N
+    ferr = force_error(a_now[sample, :3], pm_accel_f64(p_now, sample, G, pot_scale, 1.0))
+    del p_now, a_now
     sim.close()
 
     peak, peak_kind = hbm_peak()
@@ -286,10 +298,53 @@ def run_ours(args, rank, world):
                 "h2d_bytes_per_step": 2 * 16 * n, "d2h_bytes_per_step": 2 * 16 * n,
                 "path": "sd_step_host: pinned host pos/vel in, one step, host pos/vel out"},
         "gpu_launches": int(launches),
+        "force_error": {"vs": "FP64 particle-mesh on the same grid", "particles": int(len(sample)),
+                        "rms_rel": ferr["rms_rel"], "max_rel": ferr["max_rel"],
+                        "metric": "RMS|a - a_ref| / RMS|a_ref|"},
         "clocks": clock_info,
         "diagnostics": diag,
     }
     return out
+
+
+def time_workload(name: str, order: int = 2, steps: int = 20, warmup: int = 4, full_sort: int = 0) -> dict:
+    """One workload on this rank's GPU: graph-replayed ms/step (CUDA events on the
+    handle's stream), per-kernel ms of eager steps, and the step's byte model
+    (184 N + 40 G^3) as a fraction of the HBM peak."""
+    import torch
+
+    from stardust_b200 import _lib as L
+    from stardust_b200.sim import Sim, SimConfig
+
+    pos, vel, G, dt = make_workload(name)
+    n = len(pos)
+    cfg = SimConfig(particle_count=n, grid_size=G, gravity=1.0, units=L.SD_UNITS_NEWTON, softening_cells=1.0,
+                    sort_interval=1, order=order, keep_density=0, full_sort=full_sort)
+    stream = torch.cuda.Stream()
+    with Sim(torch.cuda.current_device()) as sim:
+        sim.init(cfg)
+        sim.set_stream(stream)
+        sim.set_particles(pos, vel)
+        sim.steps(dt, warmup)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.steps(dt, steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        kms = []
+        for _ in range(3):
+            sim.step(dt)
+            kms.append(sim.timings()["kernel_ms"])
+    peak, _ = hbm_peak()
+    B = model_bytes(n, G)
+    return {"particles": n, "grid": G, "dt": dt, "order": ["rowmajor", "morton", "tiled"][order],
+            "ms_per_step": ms, "value": n / (ms * 1e-3), "unit": "particle-steps/s",
+            "kernel_ms": dict(zip(KERNELS, np.median(np.array(kms), axis=0).tolist())),
+            "step_roofline": {"model_bytes": B, "achieved_gbs": B / (ms * 1e-3) / 1e9,
+                              "frac": B / (ms * 1e-3) / 1e9 / peak}}
 
 
 def run_ensemble(rank, world, steps: int = 100, warmup: int = 3, dt: float = 1e-3) -> dict:
@@ -337,7 +392,19 @@ def run_ensemble(rank, world, steps: int = 100, warmup: int = 3, dt: float = 1e-
     kernels = ens.graph_kernels()
     ens.close()
     tiled = sum(1 for tt in tuning if tt["order"] == "tiled")
+    # the byte model summed over this rank's scenes, against the HBM peak; and the
+    # spread of the scenes' solo step times (the autotuner's measurements), whose sum
+    # over the ensemble's step time is how much the branches overlap
+    B = float(sum(model_bytes(members[i]["n"], members[i]["grid"]) for i in mine))
+    peak, peak_kind = hbm_peak()
+    solo = np.array([tt["step_ms"] for tt in tuning], np.float64)
+    roof = {"model_bytes": B, "model": "sum of 184 N + 40 G^3", "achieved_gbs": B / (ms * 1e-3) / 1e9,
+            "frac": B / (ms * 1e-3) / 1e9 / peak, "peak": peak, "peak_source": peak_kind}
+    branches = {"solo_ms_quantiles": {q: float(np.quantile(solo, float(q))) for q in ("0", "0.5", "0.9", "1")},
+                "solo_ms_sum": float(solo.sum()), "overlap": float(solo.sum() / ms),
+                "largest_scene_share": float(solo.max() / ms)}
     return {"value": n_total / (ms * 1e-3), "unit": "particle-steps/s", "ms_per_step": ms, "steps": steps,
+            "step_roofline": roof, "branches": branches,
             "scenes": len(members), "particles": int(n_total),
             "grids": {str(g): sum(1 for m in members if m["grid"] == g) for g in (32, 64, 128)},
             "graph_launches_per_step": 1, "kernels_per_graph_rank0": kernels,
@@ -459,6 +526,8 @@ def main(argv=None) -> int:
     ap.add_argument("--order", type=int, default=2, help="0 row-major (reference), 1 Morton, 2 tiled (fused deposit)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-scene batched ensemble")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other workloads (disk_64, two_galaxy_256) and the row-major / Morton orders")
     ap.add_argument("--no-diagnostics", action="store_true", help="time the step without the per-step FP64 records")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-correction comparison (2M particles, 128^3 + MLP vs 128..512^3)")
@@ -479,6 +548,12 @@ def main(argv=None) -> int:
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     out = run_ours(args, rank, world)
+    if world == 1 and not args.no_configs:
+        # the other single-scene configurations (the headline's workload is cosmic_web_512)
+        out["configs"] = {w: time_workload(w) for w in ("disk_64", "two_galaxy_256") if w != args.workload}
+        # the reference's own particle order (row-major cell keys, the atomic deposit) and
+        # the 30-bit Morton order on the headline workload
+        out["orders"] = {o: time_workload(args.workload, order=k, steps=10) for k, o in ((0, "rowmajor"), (1, "morton"))}
     if not args.no_ensemble:
         out["ensemble"] = run_ensemble(rank, world)
     if world == 1 and not args.no_learned:

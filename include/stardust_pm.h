@@ -155,6 +155,32 @@ int sd_config_default(sd_config* cfg);
 int sd_max_grid_size(int boundary);
 /* Sim::estimateBytes (Sim.cu:3935-3998), for this implementation's buffers. */
 size_t sd_estimate_bytes(int particle_count, int grid_size, int boundary);
+/* Sim::maxParticlesFor (Sim.cu:4057-4066): the most particles a grid leaves room
+ * for in free_bytes of device memory. The grid's buffers come first; 80 % of the
+ * rest holds particles, at this implementation's bytes per particle. 0 when the
+ * grid alone does not fit. At most 400,000,000 (the largest particle_count). */
+int sd_max_particles_for(int grid_size, int boundary, size_t free_bytes);
+/* Sim::estimateStepMs (Sim.cu:4022-4055): a step's time from this build's byte
+ * model (184 B per particle + 40 B per transform-box cell) at 55 % of the device's
+ * memory bandwidth, plus launch overhead. 0 without a device. Particles crowded
+ * into a few rows cost more than the model says. */
+double sd_estimate_step_ms(int particle_count, int grid_size, int boundary);
+/* Sim::deviceFreeBytes (Sim.cu:3921-3925): cudaMemGetInfo's free bytes of the
+ * current device, or the override below. 0 without a device. */
+size_t sd_device_free_bytes(void);
+/* Testing aid (no reference counterpart): when bytes > 0, sd_device_free_bytes and
+ * the VRAM clamp of sd_init / sd_reconfigure see this many free bytes instead of
+ * the device's; 0 restores the real query. Process-wide. */
+void sd_set_device_free_bytes_override(size_t bytes);
+/* Sim::deviceBandwidthGBs (Sim.cu:4003-4012): memory clock x bus width x 2, GB/s. */
+double sd_device_bandwidth_gbs(void);
+/* Sim::deviceMultiProcessors (Sim.cu:3926-3930). */
+int sd_device_multiprocessors(void);
+/* Sim::deviceName / deviceDriver (Sim.cu:3907-3920): the current device's name
+ * ("unknown" without one) and the CUDA version its driver supports ("CUDA 12.9";
+ * empty without a driver), NUL-terminated into out[capacity]. */
+int sd_device_name(char* out, int capacity);
+int sd_device_driver(char* out, int capacity);
 
 /* ---- lifetime (Sim::Sim / ~Sim, Sim.cu:3900-3901) --------------------------- */
 int sd_create(sd_sim** out, int device);
@@ -163,6 +189,16 @@ int sd_destroy(sd_sim* sim);
 int sd_set_stream(sd_sim* sim, void* cuda_stream);
 
 /* ---- configuration (Sim::init / reconfigure / reset, Sim.cu:4068-4238) ------ */
+/* Sim::init / Sim::reconfigure (Sim.cu:4068-4152). A request is structural when
+ * its particle_count, grid_size (after clamping to a power of two) or boundary
+ * differs from the last structural request; repeating a request changes nothing.
+ * A structural request with the same grid and boundary and no more particles than
+ * the kernels run over only narrows that range: no reallocation, particles and
+ * simulation time stay (the reference's shrink-only path, Sim.cu:4108-4116).
+ * Other structural requests clamp particle_count to what the device's free memory
+ * holds (sd_max_particles_for; Sim.cu:4123-4134), reallocate and lay down the
+ * preset; SD_E_NOMEM, with nothing changed, when the grid alone does not fit.
+ * sd_init always reallocates. Other fields apply in place. */
 int sd_init(sd_sim* sim, const sd_config* cfg);
 int sd_reconfigure(sd_sim* sim, const sd_config* cfg);
 /* Sim::reset (Sim.cu:4160-4238): zero time and step count and lay down the
@@ -225,12 +261,18 @@ int sd_load_state(sd_sim* sim, const char* path);
 int sd_timings_get(const sd_sim* sim, sd_timings* out);             /* Sim::timings */
 double sd_sim_time(const sd_sim* sim);                              /* Sim::simTime */
 int sd_grid_size(const sd_sim* sim);                                /* Sim::gridSize */
-int sd_particle_count(const sd_sim* sim);                           /* Sim::particleCount */
+int sd_particle_count(const sd_sim* sim);                           /* Sim::particleCount: slots the kernels run over (allocN) */
+int sd_particle_capacity(const sd_sim* sim);                        /* slots allocated (capacityN, Sim.cu:3032-3045) */
 int sd_active_count(const sd_sim* sim);                             /* Sim::activeCount */
 int sd_step_count(const sd_sim* sim);
 double sd_measure_total_grid_mass(sd_sim* sim);                     /* Sim.cu:4890-4906 */
 double sd_measure_max_density(sd_sim* sim);                         /* Sim.cu:4908-4924 */
 double sd_measure_kinetic_energy(sd_sim* sim);                      /* Sim.cu:5141-5149 */
+/* Sim::measureOccupiedCells (Sim.cu:4926-4935): density cells above 1e-6 (needs keep_density) */
+int sd_measure_occupied_cells(sd_sim* sim);
+/* Sim::measureCentroid (Sim.cu:4937-4950): mean x and y of the live particles, in
+ * FP64 with a fixed summation order; 0.5, 0.5 when none is live. */
+int sd_measure_centroid(sd_sim* sim, double* cx, double* cy);
 int sd_diagnostics_get(sd_sim* sim, sd_diagnostics* out);
 /* Per-step FP64 records of the steps taken with diagnostics = 1 (accumulated
  * inside the gather, no extra pass; kept in a device ring of the last 4096

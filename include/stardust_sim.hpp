@@ -109,6 +109,25 @@ class Sim {
     static size_t estimateBytes(int particleCount, int gridSize, Boundary b) {
         return sd_estimate_bytes(particleCount, gridSize, static_cast<int>(b));
     }
+    static int maxParticlesFor(int gridSize, Boundary b, size_t freeBytes) {
+        return sd_max_particles_for(gridSize, static_cast<int>(b), freeBytes);
+    }
+    static double estimateStepMs(int particleCount, int gridSize, Boundary b) {
+        return sd_estimate_step_ms(particleCount, gridSize, static_cast<int>(b));
+    }
+    static size_t deviceFreeBytes() { return sd_device_free_bytes(); }
+    static double deviceBandwidthGBs() { return sd_device_bandwidth_gbs(); }
+    static int deviceMultiProcessors() { return sd_device_multiprocessors(); }
+    static std::string deviceName() {
+        char b[256];
+        sd_device_name(b, (int)sizeof(b));
+        return b;
+    }
+    static std::string deviceDriver() {
+        char b[64];
+        sd_device_driver(b, (int)sizeof(b));
+        return b;
+    }
     static bool failed() { return sd_failed() != 0; }
     static std::string failMessage() { return sd_last_error(); }
 
@@ -158,6 +177,8 @@ class Sim {
     double measureTotalGridMass() { return sd_measure_total_grid_mass(h_); }
     double measureMaxDensity() { return sd_measure_max_density(h_); }
     double measureKineticEnergy() { return sd_measure_kinetic_energy(h_); }
+    int measureOccupiedCells() { return sd_measure_occupied_cells(h_); }
+    void measureCentroid(double& cx, double& cy) { sd_measure_centroid(h_, &cx, &cy); }
 
     bool saveState(const std::string& path) { return sd_save_state(h_, path.c_str()) == SD_OK; }
     bool loadState(const std::string& path) {

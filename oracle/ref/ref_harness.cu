@@ -190,4 +190,18 @@ int ref_timings(void* h, float* out6) {
 
 double ref_sim_time(void* h) { return static_cast<Sim*>(h)->simTime(); }
 
+// Sim::setViewRot + Sim::fieldDevicePtr (Sim.cu:5220-5296): the G^2 screen grid of
+// field 0 (the density projected along z, or through the rotation: kProjectXY) or
+// field 1 (the velocity dispersion of the particles: kScatterDispersion,
+// kDivideInto) for the current state. rot9 (row-major 3x3) may be null: identity.
+int ref_field(void* h, int field, const float* rot9, float* out, int G) {
+    Sim* s = static_cast<Sim*>(h);
+    const float eye[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
+    s->setViewRot(rot9 ? rot9 : eye);
+    const float* p = s->fieldDevicePtr(field == 0 ? Sim::Field::Density : Sim::Field::Dispersion);
+    if (cudaDeviceSynchronize() != cudaSuccess || Sim::failed()) return -2;
+    if (cudaMemcpy(out, p, 4 * (size_t)G * G, cudaMemcpyDeviceToHost) != cudaSuccess) return -2;
+    return 0;
+}
+
 }  // extern "C"

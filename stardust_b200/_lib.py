@@ -103,6 +103,14 @@ SIGNATURES = [
     ("sd_config_default", _I, [ctypes.POINTER(SdConfig)]),
     ("sd_max_grid_size", _I, [_I]),
     ("sd_estimate_bytes", _S, [_I, _I, _I]),
+    ("sd_max_particles_for", _I, [_I, _I, _S]),
+    ("sd_estimate_step_ms", _D, [_I, _I, _I]),
+    ("sd_device_free_bytes", _S, []),
+    ("sd_set_device_free_bytes_override", None, [_S]),
+    ("sd_device_bandwidth_gbs", _D, []),
+    ("sd_device_multiprocessors", _I, []),
+    ("sd_device_name", _I, [ctypes.c_char_p, _I]),
+    ("sd_device_driver", _I, [ctypes.c_char_p, _I]),
     ("sd_create", _I, [ctypes.POINTER(_P), _I]),
     ("sd_destroy", _I, [_P]),
     ("sd_set_stream", _I, [_P, _P]),
@@ -130,11 +138,14 @@ SIGNATURES = [
     ("sd_sim_time", _D, [_P]),
     ("sd_grid_size", _I, [_P]),
     ("sd_particle_count", _I, [_P]),
+    ("sd_particle_capacity", _I, [_P]),
     ("sd_active_count", _I, [_P]),
     ("sd_step_count", _I, [_P]),
     ("sd_measure_total_grid_mass", _D, [_P]),
     ("sd_measure_max_density", _D, [_P]),
     ("sd_measure_kinetic_energy", _D, [_P]),
+    ("sd_measure_occupied_cells", _I, [_P]),
+    ("sd_measure_centroid", _I, [_P, _P, _P]),
     ("sd_diagnostics_get", _I, [_P, ctypes.POINTER(SdDiagnostics)]),
     ("sd_kernel_launches", _LL, [_P]),
     ("sd_cell_keys", _I, [_P, _I, _I, _I, _P, _P]),

@@ -140,7 +140,11 @@ int launch_max_speed(const float4* pos, const float4* vel, int n, const float* m
                      cudaStream_t s);
 int launch_energy(const float* phi, int G, const float4* pos, const float4* vel, int n, const float* mean_vel,
                   double* partials, double* out8, cudaStream_t s, int iso_S = 0);
+// op 0: sum, 1: max, 2: cells above 1e-6 (kCountOccupied, Sim.cu:2727-2730); fixed summation order
 int launch_reduce_grid(const float* rho, size_t cells, int op, double* partials, double* out, cudaStream_t s);
+// out[0..2] = sum x, sum y and count of the live particles (kCentroidAccum, Sim.cu:2733-2741),
+// in a fixed summation order
+int launch_centroid(const float4* pos, int n, double* partials, double* out3, cudaStream_t s);
 // The step's sort as a merge of the unchanged and the changed keys (sd_resort.cu).
 struct ResortBufs {
     unsigned* words = nullptr;      // change bits, one per position (zero between uses)

@@ -561,7 +561,7 @@ __global__ void __launch_bounds__(256) k_reduce_grid(const float* __restrict__ a
                                                      double* __restrict__ partials) {
     double acc = (op == 1) ? -INFINITY : 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const double v = a[i];
+        const double v = (op == 2) ? (a[i] > 1e-6f ? 1.0 : 0.0) : (double)a[i];
         acc = (op == 1) ? fmax(acc, v) : acc + v;
     }
     __shared__ double red[256];
@@ -580,6 +580,37 @@ __global__ void k_reduce_final(const double* __restrict__ partials, int blocks, 
     double acc = (op == 1) ? -INFINITY : 0.0;
     for (int b = 0; b < blocks; ++b) acc = (op == 1) ? fmax(acc, partials[b]) : acc + partials[b];
     *out = acc;
+}
+
+// Per-block sums of x, y and the count of live particles (pos.x >= 0), then one
+// thread adds the block sums in block order: the result does not depend on timing.
+__global__ void __launch_bounds__(256) k_centroid(const float4* __restrict__ pos, int n, double* __restrict__ partials) {
+    double sx = 0.0, sy = 0.0, c = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 p = pos[i];
+        if (p.x < 0.f) continue;
+        sx += (double)p.x;
+        sy += (double)p.y;
+        c += 1.0;
+    }
+    __shared__ double red[3][256];
+    red[0][threadIdx.x] = sx;
+    red[1][threadIdx.x] = sy;
+    red[2][threadIdx.x] = c;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            for (int k = 0; k < 3; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x < 3) partials[3 * blockIdx.x + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void k_centroid_final(const double* __restrict__ partials, int blocks, double* __restrict__ out) {
+    if (threadIdx.x >= 3) return;
+    double acc = 0.0;
+    for (int b = 0; b < blocks; ++b) acc += partials[3 * b + threadIdx.x];
+    out[threadIdx.x] = acc;
 }
 
 __global__ void k_hide_range(float4* __restrict__ pos, float4* __restrict__ vel, int from, int to) {
@@ -740,6 +771,15 @@ int launch_reduce_grid(const float* a, size_t cells, int op, double* partials, d
     k_reduce_grid<<<blocks, 256, 0, s>>>(a, cells, op, partials);
     SD_LAUNCHED(s);
     k_reduce_final<<<1, 32, 0, s>>>(partials, blocks, op, out);
+    SD_LAUNCHED(s);
+    return SD_OK;
+}
+
+int launch_centroid(const float4* pos, int n, double* partials, double* out3, cudaStream_t s) {
+    const int blocks = 296;
+    k_centroid<<<blocks, 256, 0, s>>>(pos, n, partials);
+    SD_LAUNCHED(s);
+    k_centroid_final<<<1, 32, 0, s>>>(partials, blocks, out3);
     SD_LAUNCHED(s);
     return SD_OK;
 }

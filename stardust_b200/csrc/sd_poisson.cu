@@ -16,6 +16,7 @@
 //   E  x-rows complex -> real, write phi
 // Every global access moves whole 512-byte bricks or whole rows, B/C/D stage
 // their bricks with cp.async, and each pass reads and writes every element once.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -267,11 +268,16 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
                                                const DepositWork& w, unsigned* __restrict__ arrive) {
     using T = Geo<G>;
     constexpr int H = T::H, NBX = T::NBX, NT = kDepositThreads, TB = G / 4;
-    constexpr int RS = G + 2;  // u64 words per sum row: rows 16 bytes out of step across banks
+    // The int64 fixed-point sums, as two 32-bit words per cell (lo[16][RS], hi[16][RS]),
+    // share their storage with the complex line buffer used after the conversion.
+    // Rows are RS = G + 4 words apart, so the row-parallel 16-byte reads of the
+    // conversion fall in different banks.
+    constexpr int RS = G + 4;
     constexpr int kAggGroups = 16;
     extern __shared__ float2 sm[];
     const float2* tw = sm;
-    unsigned long long* sums = reinterpret_cast<unsigned long long*>(sm + G);
+    unsigned* acc_lo = reinterpret_cast<unsigned*>(sm + G);
+    unsigned* acc_hi = acc_lo + 16 * RS;
     float2* s = sm + G;
     __shared__ int r_lo[7], r_off[8];
     __shared__ int s_last;
@@ -285,7 +291,7 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
         len = hi - lo;
     }
     __syncthreads();  // the shared buffers of the previous bundle are free
-    for (int i = threadIdx.x; i < 8 * RS; i += NT) reinterpret_cast<uint4*>(sums)[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (int i = threadIdx.x; i < 8 * RS; i += NT) reinterpret_cast<uint4*>(acc_lo)[i] = make_uint4(0u, 0u, 0u, 0u);
     if (threadIdx.x < 32) {
         int inc = len;
 #pragma unroll
@@ -303,6 +309,11 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
     const int total = r_off[7];
     const int f_lo = (int)((long long)total * slice / items);
     const int f_hi = (int)((long long)total * (slice + 1) / items);
+    // A weight q <= 2^32 is added as (q >> 16) into the high word and (q & 0xffff)
+    // into the low word: with fewer than 2^16 particles in this share neither 32-bit
+    // sum can overflow, so plain adds keep the 64-bit total exact. Larger shares
+    // add the low 32 bits and carry into the high word instead.
+    const bool split16 = f_hi - f_lo < 65536;
     const int lane = threadIdx.x & 31;
     constexpr int kBatch = 4;
     // warp-uniform loop: lane f = base + q * NT + lane
@@ -364,12 +375,24 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
                         qv = ((unsigned long long)hi << 16) + (unsigned long long)lo16;
                         if (!leader || !in) continue;
                     }
-                    atomicAdd(sums + rowc + (ox ? x1 : x0), qv);
+                    const int c = rowc + (ox ? x1 : x0);
+                    if (split16) {
+                        atomicAdd(acc_hi + c, (unsigned)(qv >> 16));
+                        atomicAdd(acc_lo + c, (unsigned)(qv & 0xffffu));
+                    } else {
+                        // atomicAdd returns the previous low word, so every wrap is seen by
+                        // exactly one add
+                        const unsigned lw = (unsigned)qv;
+                        const unsigned old = atomicAdd(acc_lo + c, lw);
+                        const unsigned up = (unsigned)(qv >> 32) + ((old + lw < old) ? 1u : 0u);
+                        if (up) atomicAdd(acc_hi + c, up);
+                    }
                 }
             }
         }
     }
     __syncthreads();
+    int sh = split16 ? 16 : 32;  // value of a cell: (hi << sh) + lo
     if (items > 1) {
         // a shared bundle: every CTA adds its rows into the fixed-point grid; the last
         // to arrive reads the complete sums back (and leaves the grid zero)
@@ -377,7 +400,8 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
 #pragma unroll 1
         for (int u = threadIdx.x; u < 16 * G; u += NT) {
             const int l = u / G, x = u & m;
-            const unsigned long long v = sums[l * RS + x];
+            const unsigned long long v =
+                ((unsigned long long)acc_hi[l * RS + x] << sh) + (unsigned long long)acc_lo[l * RS + x];
             if (v) atomicAdd(g + ((size_t)(4 * bz + (l >> 2)) * G + 4 * by + (l & 3)) * G + x, v);
         }
         __threadfence();
@@ -390,9 +414,12 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
         for (int u = threadIdx.x; u < 16 * G; u += NT) {
             const int l = u / G, x = u & m;
             const size_t gi = ((size_t)(4 * bz + (l >> 2)) * G + 4 * by + (l & 3)) * G + x;
-            sums[l * RS + x] = __ldcg(g + gi);
+            const unsigned long long v = __ldcg(g + gi);
+            acc_lo[l * RS + x] = (unsigned)v;
+            acc_hi[l * RS + x] = (unsigned)(v >> 32);
             g[gi] = 0ull;
         }
+        sh = 32;
         if (threadIdx.x == 0) arrive[b] = 0u;
         __syncthreads();
     }
@@ -406,10 +433,12 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
         const int u = threadIdx.x + p * NT;
         if (CITEMS % NT == 0 || u < CITEMS) {
             const int l = u & 15, mp = u >> 4;
-            const ulonglong2 a = *reinterpret_cast<const ulonglong2*>(sums + l * RS + 4 * mp);
-            const ulonglong2 c = *reinterpret_cast<const ulonglong2*>(sums + l * RS + 4 * mp + 2);
-            cv[p] = make_float4(fixed_to_float((long long)a.x), fixed_to_float((long long)a.y),
-                                fixed_to_float((long long)c.x), fixed_to_float((long long)c.y));
+            const uint4 lw = *reinterpret_cast<const uint4*>(acc_lo + l * RS + 4 * mp);
+            const uint4 hw = *reinterpret_cast<const uint4*>(acc_hi + l * RS + 4 * mp);
+            cv[p] = make_float4(fixed_to_float((long long)(((unsigned long long)hw.x << sh) + lw.x)),
+                                fixed_to_float((long long)(((unsigned long long)hw.y << sh) + lw.y)),
+                                fixed_to_float((long long)(((unsigned long long)hw.z << sh) + lw.z)),
+                                fixed_to_float((long long)(((unsigned long long)hw.w << sh) + lw.w)));
         }
     }
     __syncthreads();
@@ -713,10 +742,9 @@ struct Launcher {
     static size_t smem_bd() { return sizeof(float2) * ((size_t)G + 16 * (size_t)G); }
     static size_t smem_c() { return sizeof(float2) * ((size_t)G + (T::H + 2) / 2 + 1 + 16 * (size_t)G); }
     // the line buffer (16 * PX float2) overlays the 32-bit sum words (2 * 16 * (G + 4))
-    // the balanced deposit keeps one u64 word per cell, rows G + 2 words apart, under
-    // the line buffer
+    // the line buffer (16 * PX float2) overlays the 32-bit sum words (2 * 16 * (G + 4))
     static size_t smem_bal() {
-        const size_t lines = sizeof(float2) * 16 * (size_t)T::PX, sums = sizeof(unsigned long long) * 16 * (size_t)(G + 2);
+        const size_t lines = sizeof(float2) * 16 * (size_t)T::PX, sums = 2 * sizeof(unsigned) * 16 * (size_t)(G + 4);
         return sizeof(float2) * (size_t)G + (lines > sums ? lines : sums);
     }
     // CTAs that take the extra shares of heavy bundles
@@ -796,6 +824,21 @@ struct Launcher {
     }
 };
 
+// The Green's function's exponent table exp(-(2 pi soft / G)^2 k^2 / 2), k = 0..G/2,
+// evaluated in FP64 and rounded once (both Poisson entry points build it here).
+__global__ void k_fill_gexp(float* __restrict__ gexp, int G, float soft) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > G / 2) return;
+    const double s = 6.283185307179586476925286766559 * (double)(soft > 0.f ? soft : 0.f) / (double)G;
+    gexp[k] = (float)exp(-0.5 * s * s * (double)k * (double)k);
+}
+
+int fill_gexp(float* gexp, int G, float soft, cudaStream_t st) {
+    k_fill_gexp<<<(G / 2 + 1 + 127) / 128, 128, 0, st>>>(gexp, G, soft);
+    SD_LAUNCHED(st);
+    return SD_OK;
+}
+
 int poisson_configure(int G) {
     switch (G) {
         case 16: return Launcher<16>::configure();
@@ -843,14 +886,13 @@ int poisson_plan_build(PoissonPlan& p, int G, float soft) {
         const double a = -two_pi * (double)m / (double)G;
         tw[m] = make_float2((float)cos(a), (float)sin(a));
     }
-    std::vector<float> ge((size_t)G / 2 + 1);
-    const double s = two_pi * (double)(soft > 0.f ? soft : 0.f) / (double)G;
-    for (int k = 0; k <= G / 2; ++k) ge[k] = (float)exp(-0.5 * s * s * (double)k * (double)k);
     if (SD_CUDA(cudaMalloc(&p.tw, sizeof(float2) * tw.size())) != SD_OK) return SD_E_NOMEM;
-    if (SD_CUDA(cudaMalloc(&p.gexp, sizeof(float) * ge.size())) != SD_OK) return SD_E_NOMEM;
-    if (SD_CUDA(cudaMemcpy(p.tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice)) != SD_OK ||
-        SD_CUDA(cudaMemcpy(p.gexp, ge.data(), sizeof(float) * ge.size(), cudaMemcpyHostToDevice)) != SD_OK)
+    if (SD_CUDA(cudaMalloc(&p.gexp, sizeof(float) * ((size_t)G / 2 + 1))) != SD_OK) return SD_E_NOMEM;
+    if (SD_CUDA(cudaMemcpy(p.tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice)) != SD_OK)
         return SD_E_CUDA;
+    // the same kernel as the allocation-free solve's, so both tables hold the same bits
+    if (int rc = fill_gexp(p.gexp, G, soft, nullptr)) return rc;
+    if (SD_CUDA(cudaStreamSynchronize(nullptr))) return SD_E_CUDA;
     p.scale = (float)(1.0 / (4.0 * 3.14159265358979323846 * 3.14159265358979323846 * (double)G * G * G));
     p.G = G;
     p.soft = soft;
@@ -943,21 +985,40 @@ static __device__ __align__(256) float g_noalloc_gexp[kNoAllocMaxGrid / 2 + 1];
 
 struct NoAllocDevice {
     bool ready = false;
+    unsigned long long ctx_id = 0;  // the context the addresses and tables belong to
     float2* spec = nullptr;
     float2* tw = nullptr;
     float* gexp = nullptr;
 };
+
+// The unique ID of the current context (cuCtxGetId through the runtime's driver
+// entry points; 0 if unavailable). A device reset ends the context: its file-scope
+// arrays come back zeroed under a new ID, so the cached set-up is redone.
+unsigned long long current_ctx_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        cudaGetLastError();
+    });
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 NoAllocDevice g_noalloc[kNoAllocMaxDevices];
 std::mutex g_noalloc_mu;
-
-// exp(-(2 pi soft / G)^2 k^2 / 2) in FP64, k = 0..G/2 (the table poisson_plan_build
-// makes on the host).
-__global__ void k_fill_gexp(float* __restrict__ gexp, int G, float soft) {
-    const int k = threadIdx.x;
-    if (k > G / 2) return;
-    const double s = 6.283185307179586476925286766559 * (double)(soft > 0.f ? soft : 0.f) / (double)G;
-    gexp[k] = (float)exp(-0.5 * s * s * (double)k * (double)k);
-}
 
 int noalloc_slot(int G) { return G == 16 ? 0 : (G == 32 ? 1 : (G == 64 ? 2 : 3)); }
 
@@ -967,9 +1028,13 @@ int noalloc_slot(int G) { return G == 16 ? 0 : (G == 32 ? 1 : (G == 64 ? 2 : 3))
 int noalloc_setup(int dev) {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     NoAllocDevice& d = g_noalloc[dev];
-    if (d.ready) return SD_OK;
     void* p = nullptr;
+    // resolving a symbol also makes the device's context current, which the ID needs
     if (SD_CUDA(cudaGetSymbolAddress(&p, g_noalloc_spec))) return SD_E_CUDA;
+    const unsigned long long ctx = current_ctx_id();
+    if (d.ready && ctx == d.ctx_id) return SD_OK;
+    d.ready = false;
+    d.ctx_id = ctx;
     d.spec = static_cast<float2*>(p);
     if (SD_CUDA(cudaGetSymbolAddress(&p, g_noalloc_tw))) return SD_E_CUDA;
     d.tw = static_cast<float2*>(p);
@@ -1010,8 +1075,7 @@ extern "C" int sd_poisson_noalloc(const float* rho, int grid_size, float softeni
     const NoAllocDevice& d = g_noalloc[dev];
     cudaStream_t st = (cudaStream_t)stream;
     // the exponent table depends on the softening: rebuilt by every call
-    k_fill_gexp<<<1, kNoAllocMaxGrid, 0, st>>>(d.gexp, G, softening_cells);
-    SD_LAUNCHED(st);
+    if (int rc = fill_gexp(d.gexp, G, softening_cells, st)) return rc;
     PoissonPlan plan;
     plan.G = G;
     plan.soft = softening_cells;

@@ -556,19 +556,90 @@ int copy_out(void* dst, const void* src, size_t bytes, int where, cudaStream_t s
     return rc;
 }
 
+// Free device memory for the VRAM clamp (Sim::deviceFreeBytes, Sim.cu:3921-3925), or
+// the value a test set with sd_set_device_free_bytes_override.
+std::atomic<size_t> g_free_override{0};
+
+size_t device_free_bytes() {
+    const size_t o = g_free_override.load();
+    if (o) return o;
+    size_t f = 0, t = 0;
+    if (cudaMemGetInfo(&f, &t) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return f;
+}
+
+constexpr int kMaxParticles = 400000000;  // validate_config's limit
+
+// Device bytes that grow with the particle count, from the allocation model.
+size_t per_particle_bytes(int G, int boundary) {
+    const int step = 1 << 20;
+    const size_t a = estimate_bytes(1, G, boundary), b = estimate_bytes(step + 1, G, boundary);
+    return (b - a + step - 1) / step;
+}
+
+// Sim::maxParticlesFor (Sim.cu:4057-4066): the grid takes its share first, then 80 %
+// of the rest holds particles (the other 20 % stays for the driver and other users).
+int max_particles_for(int G, int boundary, size_t free_bytes) {
+    const size_t grid_part = estimate_bytes(1, G, boundary);
+    if (free_bytes <= grid_part) return 0;
+    const size_t usable = (size_t)((double)(free_bytes - grid_part) * 0.8);
+    const size_t n = usable / per_particle_bytes(G, boundary);
+    return n > (size_t)kMaxParticles ? kMaxParticles : (int)n;
+}
+
+// Sim::reconfigure (Sim.cu:4074-4152). A request is structural when its count, grid
+// or boundary differs from the last structural request (not from the clamped
+// count, so repeating a clamped request changes nothing). A structural request
+// that keeps the grid and boundary and asks for no more slots than the kernels
+// run over only narrows that range: buffers, particles and time stay (the
+// shrink-only path, Sim.cu:4108-4116). Any other structural request clamps the
+// count to the device's free memory (Sim.cu:4123-4134; a grid that leaves no room
+// fails with SD_E_NOMEM and changes nothing), reallocates and lays down the preset.
 int reconfigure(sd_sim* s, const sd_config* c) {
     int rc = validate_config(c);
     if (rc) return rc;
     const int G = ceil_pow2_clamp(c->grid_size, sd_max_grid_size(c->boundary));
-    const bool structural = !s->configured || c->particle_count != s->N || G != s->G ||
-                            c->boundary != s->cfg.boundary || (c->keep_density && !s->rho);
+    const bool requested = !s->configured || c->particle_count != s->req_n || G != s->req_g ||
+                           c->boundary != s->req_boundary;
+    const bool shrink =
+        requested && s->configured && G == s->G && c->boundary == s->req_boundary && c->particle_count <= s->N;
+    int n = c->particle_count;
+    if (requested && !shrink) {
+        size_t avail = device_free_bytes();
+        if (avail > 0) {
+            // what this handle holds now is freed before the new allocation
+            if (s->pos && s->capacity > 0 && s->req_boundary >= 0)
+                avail += estimate_bytes(s->capacity, s->G, s->req_boundary);
+            const int cap = max_particles_for(G, c->boundary, avail);
+            if (cap <= 0)
+                return fail(SD_E_NOMEM, "reconfigure: a %d^3 grid (%s boundary) does not fit this device (%zu bytes free)",
+                            G, c->boundary == SD_BOUNDARY_ISOLATED ? "isolated" : "periodic", avail);
+            if (n > cap) n = cap;
+        }
+    }
     const bool soft_changed = c->softening_cells != s->cfg.softening_cells;
     if (c->order != s->cfg.order) invalidate_keys(s);
     s->cfg = *c;
     s->cfg.grid_size = G;
-    if (!structural) {
+    if (!requested || shrink) {
+        if (shrink) {
+            s->req_n = c->particle_count;
+            s->N = c->particle_count;
+            if (s->active > s->N) s->active = s->N;
+            s->rho_valid = false;
+            invalidate_keys(s);  // the sort covers a shorter range
+            // change bits of slots past the new range must not reach a merge
+            if (s->rs_base &&
+                SD_CUDA(cudaMemsetAsync(s->rs.words, 0, sizeof(unsigned) * resort_words(s->capacity), s->stream)))
+                return sim_error(s, SD_E_CUDA);
+            s->chg_dirty = false;
+        }
         if (s->graph) cudaGraphExecDestroy(s->graph);
         s->graph = nullptr;
+        if (c->keep_density && !s->rho && (rc = alloc_dev(s->rho, (size_t)s->G * s->G * s->G))) return rc;
         if ((rc = ensure_hydro(s)) || (rc = ensure_resort(s))) return rc;
         if (!soft_changed) return SD_OK;
         rc = poisson_plan_build(s->plan, box_of(s->G, s->cfg.boundary), s->cfg.softening_cells);
@@ -576,10 +647,17 @@ int reconfigure(sd_sim* s, const sd_config* c) {
             rc = build_green_table(s->plan, s->cfg.softening_cells, s->phi, s->spec, s->green, s->stream);
         return rc;
     }
-    s->N = c->particle_count;
+    s->req_n = c->particle_count;
+    s->req_g = G;
+    s->req_boundary = c->boundary;
+    s->N = s->capacity = n;
     s->G = G;
     rc = allocate(s);
-    if (rc) return rc;
+    if (rc) {
+        s->req_n = s->req_g = s->req_boundary = -1;
+        s->capacity = 0;
+        return rc;
+    }
     if ((rc = ensure_hydro(s)) || (rc = ensure_resort(s))) return rc;
     // the reference's init / structural reconfigure ends in reset() (Sim.cu:4151)
     if ((rc = place_initial(s))) return sim_error(s, rc);
@@ -671,6 +749,80 @@ int sd_max_grid_size(int boundary) { return boundary == SD_BOUNDARY_ISOLATED ? 2
 size_t sd_estimate_bytes(int particle_count, int grid_size, int boundary) {
     const int G = ceil_pow2_clamp(grid_size, sd_max_grid_size(boundary));
     return estimate_bytes(particle_count, G, boundary);
+}
+
+int sd_max_particles_for(int grid_size, int boundary, size_t free_bytes) {
+    if (boundary != SD_BOUNDARY_PERIODIC && boundary != SD_BOUNDARY_ISOLATED) return 0;
+    const int G = ceil_pow2_clamp(grid_size, sd_max_grid_size(boundary));
+    return max_particles_for(G, boundary, free_bytes);
+}
+
+size_t sd_device_free_bytes(void) { return device_free_bytes(); }
+
+void sd_set_device_free_bytes_override(size_t bytes) { g_free_override.store(bytes); }
+
+double sd_device_bandwidth_gbs(void) {
+    // Sim::deviceBandwidthGBs (Sim.cu:4003-4012): memory clock x bus width x 2 (DDR)
+    int khz = 0, bits = 0, dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&khz, cudaDevAttrMemoryClockRate, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&bits, cudaDevAttrGlobalMemoryBusWidth, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0.0;
+    }
+    if (khz <= 0 || bits <= 0) return 0.0;
+    return (double)khz * 1000.0 * ((double)bits / 8.0) * 2.0 / 1.0e9;
+}
+
+double sd_estimate_step_ms(int particle_count, int grid_size, int boundary) {
+    // Sim::estimateStepMs (Sim.cu:4022-4055) with this build's costs: the byte model
+    // of a step, 184 B per particle + 40 B per cell of the transform box, at 55 % of
+    // the memory bandwidth (a 16M / 512^3 step runs at about 0.66 of the measured
+    // copy bandwidth), plus 0.02 ms of launch overhead. A scene whose particles
+    // crowd a few rows costs more than the model says.
+    const double bw = sd_device_bandwidth_gbs();
+    if (bw <= 0.0) return 0.0;
+    if (boundary != SD_BOUNDARY_PERIODIC && boundary != SD_BOUNDARY_ISOLATED) return 0.0;
+    const double G = (double)ceil_pow2_clamp(grid_size, sd_max_grid_size(boundary));
+    const double S = (boundary == SD_BOUNDARY_ISOLATED) ? 2.0 * G : G;
+    const double n = (double)(particle_count > 0 ? particle_count : 0);
+    const double bytes = 184.0 * n + 40.0 * S * S * S;
+    return bytes / (0.55 * bw * 1.0e9) * 1.0e3 + 0.02;
+}
+
+int sd_device_multiprocessors(void) {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return sms;
+}
+
+int sd_device_name(char* out, int capacity) {
+    if (!out || capacity <= 0) return fail(SD_E_ARG, "device_name: no buffer");
+    int dev = 0;
+    cudaDeviceProp p{};
+    const char* name = "unknown";
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaGetDeviceProperties(&p, dev) == cudaSuccess)
+        name = p.name;
+    else
+        cudaGetLastError();
+    snprintf(out, (size_t)capacity, "%s", name);
+    return SD_OK;
+}
+
+int sd_device_driver(char* out, int capacity) {
+    // the CUDA version the driver supports (Sim::deviceDriver, Sim.cu:3912-3920)
+    if (!out || capacity <= 0) return fail(SD_E_ARG, "device_driver: no buffer");
+    int v = 0;
+    out[0] = 0;
+    if (cudaDriverGetVersion(&v) != cudaSuccess || v <= 0) {
+        cudaGetLastError();
+        return SD_OK;
+    }
+    snprintf(out, (size_t)capacity, "CUDA %d.%d", v / 1000, (v % 1000) / 10);
+    return SD_OK;
 }
 
 int sd_create(sd_sim** out, int device) {
@@ -1162,7 +1314,10 @@ int sd_load_state(sd_sim* s, const char* path) {
     }
     const int n = h.count < s->N ? h.count : s->N;
     std::vector<float4> hp((size_t)n), hv((size_t)n);
+    // positions of every record come first, then velocities: skip the positions
+    // past a clamped count
     const bool ok = fread(hp.data(), sizeof(float4), (size_t)n, f) == (size_t)n &&
+                    (n == h.count || fseek(f, (long)(sizeof(float4) * (size_t)(h.count - n)), SEEK_CUR) == 0) &&
                     fread(hv.data(), sizeof(float4), (size_t)n, f) == (size_t)n;
     fclose(f);
     if (!ok) return fail(SD_E_FORMAT, "load_state: truncated particle data");
@@ -1202,6 +1357,7 @@ int sd_timings_get(const sd_sim* s, sd_timings* out) {
 double sd_sim_time(const sd_sim* s) { return s ? s->sim_time : 0.0; }
 int sd_grid_size(const sd_sim* s) { return s ? s->G : 0; }
 int sd_particle_count(const sd_sim* s) { return s ? s->N : 0; }
+int sd_particle_capacity(const sd_sim* s) { return s ? s->capacity : 0; }
 int sd_active_count(const sd_sim* s) { return s ? s->active : 0; }
 int sd_step_count(const sd_sim* s) { return s ? s->step_count : 0; }
 
@@ -1217,6 +1373,23 @@ static double reduce_rho(sd_sim* s, int op) {
 
 double sd_measure_total_grid_mass(sd_sim* s) { return reduce_rho(s, 0); }
 double sd_measure_max_density(sd_sim* s) { return reduce_rho(s, 1); }
+int sd_measure_occupied_cells(sd_sim* s) { return (int)reduce_rho(s, 2); }
+
+int sd_measure_centroid(sd_sim* s, double* cx, double* cy) {
+    if (cx) *cx = 0.5;
+    if (cy) *cy = 0.5;
+    if (!s || !s->configured || !cx || !cy) return fail(SD_E_ARG, "measure_centroid: not initialised or null output");
+    DeviceGuard g(s->device);
+    double out[3] = {0.0, 0.0, 0.0};
+    int rc = launch_centroid(s->pos, s->N, s->partials, s->mom + 5, s->stream);
+    if (!rc) rc = copy_out(out, s->mom + 5, sizeof(double) * 3, SD_HOST, s->stream);
+    if (rc) return sim_error(s, rc);
+    if (out[2] > 0.0) {
+        *cx = out[0] / out[2];
+        *cy = out[1] / out[2];
+    }
+    return SD_OK;
+}
 
 double sd_measure_kinetic_energy(sd_sim* s) {
     if (!s || !s->configured) return 0.0;

@@ -14,8 +14,12 @@ struct sd_sim {
     bool configured = false;
     bool cuda_failed = false;
     sd_config cfg{};
-    int N = 0;          // slots (allocN)
+    int N = 0;          // slots the kernels run over (the reference's allocN)
     int G = 0;
+    int capacity = 0;   // slots allocated (capacityN); N <= capacity, a shrink narrows N only
+    // the last structural request (requestedN / requestedG / requestedBoundary): a
+    // repeated request changes nothing even when N was clamped below it
+    int req_n = -1, req_g = -1, req_boundary = -1;
     int active = 0;     // slots loaded by the last set_particles / load_state
     double sim_time = 0.0;
     int step_count = 0;

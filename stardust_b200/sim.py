@@ -135,6 +135,40 @@ class Sim:
     def estimate_bytes(particle_count: int, grid_size: int, boundary: int = L.SD_BOUNDARY_PERIODIC) -> int:
         return int(L.lib().sd_estimate_bytes(particle_count, grid_size, boundary))
 
+    @staticmethod
+    def max_particles_for(grid_size: int, boundary: int, free_bytes: int) -> int:
+        """Sim::maxParticlesFor (Sim.cu:4057-4066)."""
+        return int(L.lib().sd_max_particles_for(grid_size, boundary, free_bytes))
+
+    @staticmethod
+    def estimate_step_ms(particle_count: int, grid_size: int, boundary: int = L.SD_BOUNDARY_PERIODIC) -> float:
+        """Sim::estimateStepMs (Sim.cu:4022-4055); 0 without a device."""
+        return float(L.lib().sd_estimate_step_ms(particle_count, grid_size, boundary))
+
+    @staticmethod
+    def device_free_bytes() -> int:
+        return int(L.lib().sd_device_free_bytes())
+
+    @staticmethod
+    def device_bandwidth_gbs() -> float:
+        return float(L.lib().sd_device_bandwidth_gbs())
+
+    @staticmethod
+    def device_multiprocessors() -> int:
+        return int(L.lib().sd_device_multiprocessors())
+
+    @staticmethod
+    def device_name() -> str:
+        buf = ctypes.create_string_buffer(256)
+        L.check(L.lib().sd_device_name(buf, 256), "sd_device_name")
+        return buf.value.decode()
+
+    @staticmethod
+    def device_driver() -> str:
+        buf = ctypes.create_string_buffer(64)
+        L.check(L.lib().sd_device_driver(buf, 64), "sd_device_driver")
+        return buf.value.decode()
+
     # ---- configuration -----------------------------------------------------------
     def init(self, cfg: SimConfig) -> None:
         c = cfg.to_c()
@@ -267,6 +301,9 @@ class Sim:
     def particle_count(self) -> int:
         return int(L.lib().sd_particle_count(self._h))
 
+    def particle_capacity(self) -> int:
+        return int(L.lib().sd_particle_capacity(self._h))
+
     def active_count(self) -> int:
         return int(L.lib().sd_active_count(self._h))
 
@@ -281,6 +318,14 @@ class Sim:
 
     def measure_kinetic_energy(self) -> float:
         return float(L.lib().sd_measure_kinetic_energy(self._h))
+
+    def measure_occupied_cells(self) -> int:
+        return int(L.lib().sd_measure_occupied_cells(self._h))
+
+    def measure_centroid(self) -> tuple[float, float]:
+        cx, cy = ctypes.c_double(0.5), ctypes.c_double(0.5)
+        L.check(L.lib().sd_measure_centroid(self._h, ctypes.byref(cx), ctypes.byref(cy)), "sd_measure_centroid")
+        return cx.value, cy.value
 
     def diagnostics(self) -> dict:
         d = L.SdDiagnostics()

@@ -65,9 +65,10 @@ static void disk(int n, uint64_t seed, std::vector<float>& pos, std::vector<floa
     }
 }
 
-static std::string fmt(const char* f, double a, double b, double c) {
-    char buf[200];
-    std::snprintf(buf, sizeof(buf), f, a, b, c);
+template <class... A>
+static std::string fmt(const char* f, A... a) {
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), f, (double)a...);
     return buf;
 }
 
@@ -217,6 +218,137 @@ static void test_sticky_failure() {
     sd_clear_error();
 }
 
+// tests/sim_tests.cpp:236-265 (testVramClamp): an impossible request is cut to
+// the most the device holds, and the cut scene still runs. The free memory is
+// set through the library's test override so the cut is small; the real query
+// is checked to answer.
+static void test_vram_clamp() {
+    std::printf("[8] VRAM clamp of an impossible request\n");
+    const int gCap = Sim::maxGridSize(Boundary::Isolated);
+    const size_t real_free = Sim::deviceFreeBytes();
+    check(real_free > 0, "deviceFreeBytes answers", fmt("free=%g MB", real_free / 1048576.0));
+    const size_t freeB = Sim::estimateBytes(1, gCap, Boundary::Isolated) + ((size_t)64 << 20);
+    const int maxN = Sim::maxParticlesFor(gCap, Boundary::Isolated, freeB);
+    sd_set_device_free_bytes_override(freeB);
+    Sim sim;
+    SimConfig cfg;
+    cfg.particleCount = 350000000;
+    cfg.gridSize = gCap;
+    cfg.boundary = Boundary::Isolated;
+    sim.init(cfg);
+    const int got = sim.particleCount();
+    check(got > 1000 && got <= maxN && Sim::estimateBytes(got, gCap, Boundary::Isolated) <= freeB,
+          "an excessive request is cut to the most the memory holds", fmt("requested 3.5e8 got=%g max=%g", got, maxN));
+    const double t0 = sim.simTime();
+    sim.step();
+    const double mass = sim.measureTotalGridMass();
+    check(std::fabs(mass - got) / got < 1e-2, "the cut scene runs", fmt("grid mass %g for %g particles", mass, got));
+    // repeating the clamped request is not a new request: nothing is reallocated
+    sim.reconfigure(cfg);
+    check(sim.particleCount() == got && sim.simTime() > t0, "repeating the clamped request keeps the scene",
+          fmt("N=%g t=%g", sim.particleCount(), sim.simTime()));
+    // a grid that leaves no room for particles fails and changes nothing
+    sd_clear_error();
+    sd_set_device_free_bytes_override(Sim::estimateBytes(1, gCap, Boundary::Isolated) / 2);
+    SimConfig other = cfg;
+    other.particleCount = 1000;
+    sim.reconfigure(other);
+    const bool refused = Sim::failed();
+    check(refused && sim.particleCount() == got, "a grid that does not fit is refused", Sim::failMessage());
+    sd_clear_error();
+    sd_set_device_free_bytes_override(0);
+}
+
+// tests/sim_tests.cpp:512-543 (testNoReallocOnSameRequest): the same request
+// repeated leaves the scene alone; a changed request reallocates and resets.
+static void test_no_realloc_on_same_request() {
+    std::printf("[9] the same request repeated does not reallocate\n");
+    Sim sim;
+    SimConfig cfg;
+    cfg.particleCount = 500000;
+    cfg.gridSize = 256;
+    sim.init(cfg);
+    for (int i = 0; i < 50; ++i) sim.step();
+    const double tBefore = sim.simTime();
+    const int nBefore = sim.activeCount();
+    for (int i = 0; i < 200; ++i) sim.reconfigure(cfg);
+    const double tAfterSame = sim.simTime();
+    SimConfig bigger = cfg;
+    bigger.particleCount = 700000;
+    sim.reconfigure(bigger);
+    const double tAfterChange = sim.simTime();
+    const int nAfterChange = sim.activeCount();
+    check(tBefore > 0.0 && tAfterSame == tBefore && tAfterChange == 0.0 && nAfterChange == 700000,
+          "the same request is kept, a changed one reallocates and resets",
+          fmt("t %g -> %g -> %g, active %g -> %g", tBefore, tAfterSame, tAfterChange, nBefore, nAfterChange));
+}
+
+// Sim.cu:4108-4116: fewer particles on the same grid narrow the kernel range;
+// buffers, the particles below the new count and the time stay.
+static void test_shrink_keeps_the_scene() {
+    std::printf("[10] a shrink keeps the particles\n");
+    const int n0 = 200000, n1 = 150000;
+    Sim sim;
+    SimConfig cfg;
+    cfg.particleCount = n0;
+    cfg.gridSize = 64;
+    cfg.order = SD_ORDER_TILED;
+    sim.init(cfg);
+    std::vector<float> p, v;
+    disk(n0, 5, p, v);
+    sim.setParticles(p.data(), v.data(), n0);
+    for (int i = 0; i < 5; ++i) sim.step(1e-3f);
+    std::vector<float> pb(4 * (size_t)n0), vb(4 * (size_t)n0);
+    sim.getParticles(pb.data(), vb.data(), n0);
+    const double t0 = sim.simTime();
+    cfg.particleCount = n1;
+    sim.reconfigure(cfg);
+    std::vector<float> pa(4 * (size_t)n1), va(4 * (size_t)n1);
+    sim.getParticles(pa.data(), va.data(), n1);
+    const bool same = std::equal(pa.begin(), pa.end(), pb.begin()) && std::equal(va.begin(), va.end(), vb.begin());
+    check(sim.particleCount() == n1 && sd_particle_capacity(sim.handle()) == n0 && sim.simTime() == t0 && same,
+          "the kernel range narrows, particles and time stay bit for bit",
+          fmt("N=%g capacity=%g t=%g", sim.particleCount(), sd_particle_capacity(sim.handle()), sim.simTime()));
+    sim.step(1e-3f);
+    const double mass = sim.measureTotalGridMass();
+    check(std::fabs(mass - n1) / n1 < 1e-3, "the narrowed scene deposits only its particles",
+          fmt("grid mass %g", mass));
+    // growing again is a new structural request: reallocate and lay down the preset
+    cfg.particleCount = n0;
+    sim.reconfigure(cfg);
+    check(sim.simTime() == 0.0 && sim.particleCount() == n0, "growing back reallocates and resets",
+          fmt("t=%g N=%g", sim.simTime(), sim.particleCount()));
+}
+
+// Sim::estimateStepMs / maxParticlesFor / measureOccupiedCells / measureCentroid.
+static void test_estimates_and_measures() {
+    std::printf("[11] estimators and measurements\n");
+    const double a = Sim::estimateStepMs(1 << 20, 128, Boundary::Periodic);
+    const double b = Sim::estimateStepMs(1 << 22, 128, Boundary::Periodic);
+    const double c = Sim::estimateStepMs(1 << 20, 256, Boundary::Periodic);
+    const double d = Sim::estimateStepMs(1 << 20, 128, Boundary::Isolated);
+    check(a > 0.0 && b > a && c > a && d > a, "estimateStepMs grows with N, G and the isolated box",
+          fmt("%g %g %g %g ms", a, b, c, d));
+    check(Sim::deviceBandwidthGBs() > 100.0 && Sim::deviceMultiProcessors() > 0 && !Sim::deviceName().empty(),
+          "device bandwidth, SM count and name answer",
+          fmt("%g GB/s, %g SMs", Sim::deviceBandwidthGBs(), Sim::deviceMultiProcessors()) + " " + Sim::deviceName());
+    Sim sim;
+    SimConfig cfg;
+    cfg.particleCount = 1;
+    cfg.gridSize = 32;
+    cfg.gravity = 0.f;
+    sim.init(cfg);
+    const float p1[4] = {0.3f, 0.7f, 0.55f, 0.f}, v1[4] = {0.f, 0.f, 0.f, 0.f};
+    sim.setParticles(p1, v1, 1);
+    sim.step(1e-4f);
+    check(sim.measureOccupiedCells() == 8, "one particle occupies its 8 CIC cells",
+          fmt("%g cells", sim.measureOccupiedCells()));
+    double cx = 0, cy = 0;
+    sim.measureCentroid(cx, cy);
+    check(std::fabs(cx - 0.3) < 1e-6 && std::fabs(cy - 0.7) < 1e-6, "the centroid of one particle is its x, y",
+          fmt("(%g, %g)", cx, cy));
+}
+
 int main(int argc, char** argv) {
     const std::string dir = argc > 1 ? argv[1] : ".";
     if (!Sim::deviceAvailable()) {
@@ -230,6 +362,10 @@ int main(int argc, char** argv) {
     test_state_round_trip(dir);
     test_init_lays_down_the_preset();
     test_sticky_failure();
+    test_vram_clamp();
+    test_no_realloc_on_same_request();
+    test_shrink_keeps_the_scene();
+    test_estimates_and_measures();
     std::printf("%d failure(s)\n", g_failures);
     return g_failures == 0 ? 0 : 1;
 }

@@ -1,7 +1,12 @@
 """Generate golden fixtures by running the unmodified reference on a GPU.
 
 Usage (on a machine with a CUDA GPU and the prebuilt oracle/_ref/libsimref.so):
-    python tests/golden/make_reference_fixtures.py OUTDIR
+    python tests/golden/make_reference_fixtures.py OUTDIR [CASE ...]
+
+With CASE names, only those cases are written (e.g. ``disk_g64 fields_g32``).
+``reference_disk_g64.npz`` holds no inputs: the test rebuilds them from the seeded
+scene and checks them against the stored digest. ``reference_fields_g32.npz`` holds
+the screen grids of Sim::fieldDevicePtr (density projection, velocity dispersion).
 
 For each step case it writes ``reference_<name>.npz`` holding the seeded input
 particles, the reference's density after Sim::loadState (deposit of the loaded
@@ -121,9 +126,82 @@ def preset_cases():
     yield "empty_dark", 3000, 16, 1, 0.3, 0.0, 0.5, 0.0, 0.1
 
 
-def main(outdir: str) -> int:
+def compact_step_cases():
+    """Steps stored without their inputs, which the test regenerates from the same
+    seeded scene: name, (scene kind, n, seed), grid, gravity, softening, dt, sampled
+    output slots."""
+    yield "disk_g64", ("disk", 262_144, 0), 64, float(4 * np.pi * 64 ** 3), 1.0, 1e-3, 16384
+
+
+def scene_inputs(kind, n, seed):
+    p, v = scenes.disk_galaxy(n, seed) if kind == "disk" else scenes.two_galaxies(n, seed)
+    p = np.ascontiguousarray(p, np.float32)
+    v = np.ascontiguousarray(v, np.float32)
+    v[:, 3] = np.arange(n, dtype=np.float32)  # ids through the reference's sort
+    return p, v
+
+
+def input_digest(pos, vel) -> str:
+    import hashlib
+
+    return hashlib.sha256(pos.tobytes() + vel.tobytes()).hexdigest()
+
+
+def field_cases():
+    """Screen grids of Sim::fieldDevicePtr: name, (scene kind, n, seed), grid, view rotation."""
+    c, s_ = np.cos(0.6), np.sin(0.6)
+    rx = np.array([[1, 0, 0], [0, c, -s_], [0, s_, c]])
+    ry = np.array([[np.cos(0.35), 0, np.sin(0.35)], [0, 1, 0], [-np.sin(0.35), 0, np.cos(0.35)]])
+    rot = (ry @ rx).astype(np.float32).reshape(9)
+    yield "fields_g32", ("disk", 8192, 13), 32, rot
+
+
+def main(outdir: str, only=()) -> int:
     os.makedirs(outdir, exist_ok=True)
     L = load_ref()
+    L.ref_field.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+
+    def want(name):
+        return not only or name in only
+
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, (kind, n, seed), G, grav, soft, dt, sample in compact_step_cases():
+            if not want(name):
+                continue
+            pos, vel = scene_inputs(kind, n, seed)
+            rho, p1, v1, dt_used = run_case(L, pos, vel, G, grav, soft, dt, tmp)
+            slots = np.sort(np.random.default_rng(5).choice(n, sample, replace=False)).astype(np.int32)
+            np.savez_compressed(os.path.join(outdir, f"reference_{name}.npz"), scene=np.array([kind]), n=n, seed=seed,
+                                digest=np.array([input_digest(pos, vel)]), rho_loaded=rho,
+                                ids_out=v1[:, 3].astype(np.int32), slots=slots, pos_out=p1[slots], vel_out=v1[slots],
+                                grid=G, gravity=grav, soft=soft, dt=np.float32(dt_used))
+            print(name, "dt_used", dt_used, "mass", float(rho.sum()))
+        for name, (kind, n, seed), G, rot in field_cases():
+            if not want(name):
+                continue
+            pos, vel = scene_inputs(kind, n, seed)
+            h = L.ref_create()
+            try:
+                path = os.path.join(tmp, "f.stardust").encode()
+                if L.ref_load(h, pos.ctypes.data, vel.ctypes.data, n, G, 1.0, 1.0, 1.0, 1, path) != 0:
+                    raise RuntimeError(f"ref_load failed: {L.ref_fail_message()}")
+                rho = np.empty(G ** 3, np.float32)
+                L.ref_density(h, rho.ctypes.data, G)
+                grids = {}
+                for field, fname in ((0, "density"), (1, "dispersion")):
+                    for r, rname in ((None, "top"), (rot, "rot")):
+                        out = np.empty(G * G, np.float32)
+                        rp = None if r is None else np.ascontiguousarray(r, np.float32)
+                        if L.ref_field(h, field, None if rp is None else rp.ctypes.data, out.ctypes.data, G) != 0:
+                            raise RuntimeError(f"ref_field failed: {L.ref_fail_message()}")
+                        grids[f"{fname}_{rname}"] = out.reshape(G, G)
+            finally:
+                L.ref_destroy(h)
+            np.savez_compressed(os.path.join(outdir, f"reference_{name}.npz"), pos=pos, vel=vel, grid=G, rot=rot,
+                                rho_loaded=rho.reshape(G, G, G), **grids)
+            print(name, {k: float(v.sum()) for k, v in grids.items()})
+    if only:
+        return 0
     for name, pos, vel, G, grav, soft, dt, steps, pk, rate in hydro_cases():
         pos = np.ascontiguousarray(pos, np.float32)
         vel = np.ascontiguousarray(vel, np.float32)
@@ -184,4 +262,6 @@ def main(outdir: str) -> int:
 
 
 if __name__ == "__main__":
-    sys.exit(main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden")))
+    if len(sys.argv) < 2:
+        sys.exit(__doc__)
+    sys.exit(main(sys.argv[1], tuple(sys.argv[2:])))

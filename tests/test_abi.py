@@ -90,3 +90,32 @@ def test_create_without_device_reports_cuda_error(lib):
     assert lib.sd_create(ctypes.byref(h), 0) == L.SD_E_CUDA
     assert lib.sd_device_available() == 0
     lib.sd_clear_error()
+
+
+def test_max_particles_for_fits_the_memory(lib):
+    """Sim::maxParticlesFor (Sim.cu:4057-4066): the grid's share first, 80 % of the
+    rest for particles; the allocation model of that many particles fits."""
+    for G, b in ((64, L.SD_BOUNDARY_PERIODIC), (512, L.SD_BOUNDARY_PERIODIC), (256, L.SD_BOUNDARY_ISOLATED)):
+        grid = lib.sd_estimate_bytes(1, G, b)
+        assert lib.sd_max_particles_for(G, b, grid) == 0          # nothing left for particles
+        assert lib.sd_max_particles_for(G, b, grid // 2) == 0
+        free = grid + (1 << 30)
+        n = lib.sd_max_particles_for(G, b, free)
+        assert 1000 < n
+        assert lib.sd_estimate_bytes(n, G, b) <= free
+        # 80 % of the room: the model of 1.3 n particles no longer fits in it
+        assert lib.sd_estimate_bytes(int(n * 1.3), G, b) > free
+    assert lib.sd_max_particles_for(512, L.SD_BOUNDARY_PERIODIC, 1 << 62) == 400_000_000
+    assert lib.sd_max_particles_for(64, 7, 1 << 40) == 0
+
+
+def test_device_queries_without_a_device(lib):
+    """Without a GPU the device queries answer 0 or empty, as the reference's do."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    assert lib.sd_estimate_step_ms(1 << 20, 128, L.SD_BOUNDARY_PERIODIC) == 0.0
+    assert lib.sd_device_bandwidth_gbs() == 0.0
+    buf = ctypes.create_string_buffer(64)
+    assert lib.sd_device_name(buf, 64) == 0 and buf.value == b"unknown"

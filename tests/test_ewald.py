@@ -57,3 +57,22 @@ def test_gpu_ewald_two_particles_is_newtonian_at_short_range(cuda, lib):
     m, r = 0.5, 0.02
     assert a[0, 0] > 0 and a[1, 0] < 0
     assert a[0, 0] == pytest.approx(m / r ** 2, rel=2e-3)
+
+
+def test_fp64_pm_judge_matches_the_oracle(oracle):
+    """The FP64 particle-mesh judge the benchmark reports the force error against
+    (stardust_b200.ewald.pm_accel_f64) is the oracle's FP64 PM on the same grid."""
+    from stardust_b200.ewald import pm_accel_f64
+
+    rng = np.random.default_rng(3)
+    n, G = 30000, 32
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = (rng.random((8, 3))[rng.integers(0, 8, n)] + rng.normal(scale=0.05, size=(n, 3))) % 1.0
+    pos[:, :3][pos[:, :3] >= 1.0] = 0.0
+    pos[::17] = (-1.0, -1.0, -1.0, 0.0)  # empty slots deposit nothing
+    live = np.nonzero(pos[:, 0] >= 0)[0]
+    sample = live[::37]
+    for soft in (0.0, 1.5):
+        a = pm_accel_f64(pos, sample, G, 0.37, soft)
+        b = oracle.pm_accel_f64(pos[pos[:, 0] >= 0], G, 0.37, soft)[np.searchsorted(live, sample)]
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()

@@ -93,10 +93,76 @@ def test_pm_accel_f64_two_particles_antisymmetric(oracle):
 
 
 def _golden_files(isolated=False):
-    """One-step plain-PM fixtures (not the preset and hydro fixtures)."""
+    """One-step plain-PM fixtures holding their inputs (not the preset, hydro,
+    field or compact fixtures)."""
     files = sorted(glob.glob(os.path.join(GOLDEN, "reference_*.npz")))
-    files = [f for f in files if not os.path.basename(f).startswith(("reference_preset_", "reference_hydro_"))]
+    files = [f for f in files if not os.path.basename(f).startswith(
+        ("reference_preset_", "reference_hydro_", "reference_fields_")) and "pos_in" in np.load(f).files]
     return [f for f in files if ("isolated" in os.path.basename(f)) == isolated]
+
+
+def _compact_files():
+    """One-step fixtures stored without their inputs (rebuilt from the seeded scene)."""
+    return [f for f in sorted(glob.glob(os.path.join(GOLDEN, "reference_*.npz"))) if "digest" in np.load(f).files]
+
+
+@pytest.mark.skipif(not _compact_files(), reason="no compact reference fixture committed")
+@pytest.mark.parametrize("path", _compact_files(), ids=lambda p: os.path.basename(p)[10:-4])
+def test_oracle_against_reference_at_benchmark_scale(oracle, path):
+    """One step of the unmodified reference at the first benchmark configuration's
+    scale (262,144 disk-galaxy particles on 64^3): the seeded inputs are rebuilt
+    and checked against the fixture's digest, then the oracle's step must give the
+    reference's sort permutation exactly, its loaded density within float-atomic
+    rounding, and on a sample of output slots its velocity change and positions."""
+    import hashlib
+
+    from stardust_b200 import scenes
+
+    f = np.load(path)
+    kind, n, seed = str(f["scene"][0]), int(f["n"]), int(f["seed"])
+    pos, vel = scenes.disk_galaxy(n, seed) if kind == "disk" else scenes.two_galaxies(n, seed)
+    pos = np.ascontiguousarray(pos, np.float32)
+    vel = np.ascontiguousarray(vel, np.float32)
+    vel[:, 3] = np.arange(n, dtype=np.float32)
+    assert hashlib.sha256(pos.tobytes() + vel.tobytes()).hexdigest() == str(f["digest"][0]), "scene inputs drifted"
+    G = int(f["grid"])
+    rho = oracle.density_fixed(pos, G)
+    assert np.abs(rho - f["rho_loaded"]).max() <= 2e-5 * max(1.0, float(f["rho_loaded"].max()))
+    p1, v1, _, _ = oracle.step(pos, vel, G, gravity=float(f["gravity"]), soft_cells=float(f["soft"]),
+                               dt_kick=float(f["dt"]), dt_drift=float(f["dt"]))
+    assert np.array_equal(v1[:, 3].astype(np.int64), f["ids_out"].astype(np.int64))
+    slots = f["slots"]
+    ids = f["ids_out"][slots].astype(np.int64)
+    dv_ref = f["vel_out"][:, :3] - vel[ids, :3]
+    dv = v1[slots, :3] - vel[ids, :3]
+    scale = np.sqrt(np.mean(np.sum(dv_ref.astype(np.float64) ** 2, axis=1)))
+    err = np.sqrt(np.mean(np.sum((dv - dv_ref).astype(np.float64) ** 2, axis=1))) / scale
+    assert err < 2e-4, err
+    dp = (p1[slots, :3] - f["pos_out"][:, :3] + 0.5) % 1.0 - 0.5
+    assert np.abs(dp).max() < 1e-5
+
+
+FIELDS = os.path.join(GOLDEN, "reference_fields_g32.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(FIELDS), reason="no field fixture committed")
+@pytest.mark.parametrize("view", ["top", "rot"])
+def test_render_fields_oracle_against_reference(oracle, view):
+    """The screen grids the headless grid view shades, against the unmodified
+    reference's Sim::fieldDevicePtr (kProjectXY; kScatterDispersion and
+    kDivideInto) on the same loaded scene, straight down and through a view
+    rotation: the density projection of the reference's own loaded density, and
+    the velocity dispersion of the particles. The reference sums with float
+    atomics in no fixed order, hence the tolerances."""
+    f = np.load(FIELDS)
+    G = int(f["grid"])
+    v = {"rot_on": 0} if view == "top" else {"rot_on": 1, "rot": f["rot"], "center": (0.5, 0.5, 0.5)}
+    dens = oracle.project_field(f["rho_loaded"], v)
+    ref = f[f"density_{view}"].astype(np.float64)
+    assert np.abs(dens - ref).max() <= 1e-5 * ref.max()
+    disp = oracle.dispersion_field(f["pos"], f["vel"], G, v)
+    ref = f[f"dispersion_{view}"].astype(np.float64)
+    assert np.abs(disp - ref).max() <= 1e-4 * ref.max()
 
 
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "reference_preset_*.npz"))),

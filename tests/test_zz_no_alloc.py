@@ -27,17 +27,20 @@ def _solve_regular(cuda, lib, rho_d, G, soft):
     return phi.cpu().numpy()
 
 
-def _solve_noalloc(cuda, lib, rho_d, G, soft):
+def _solve_noalloc(cuda, lib, rho_d, G, soft, stream=None):
     phi = cuda.empty(G ** 3, dtype=cuda.float32, device="cuda")
-    L.check(lib.sd_poisson_noalloc(rho_d.data_ptr(), G, ctypes.c_float(soft), phi.data_ptr(), None),
+    handle = None if stream is None else ctypes.c_void_p(stream.cuda_stream)
+    L.check(lib.sd_poisson_noalloc(rho_d.data_ptr(), G, ctypes.c_float(soft), phi.data_ptr(), handle),
             "sd_poisson_noalloc")
     cuda.cuda.synchronize()
     return phi.cpu().numpy()
 
 
+@pytest.mark.parametrize("on_stream", [False, True], ids=["default-stream", "caller-stream"])
 @pytest.mark.parametrize("G", [16, 64, 128])
-def test_noalloc_matches_regular_entry_point_twice(cuda, lib, G):
+def test_noalloc_matches_regular_entry_point_twice(cuda, lib, oracle, G, on_stream):
     rng = np.random.default_rng(G)
+    stream = cuda.cuda.Stream() if on_stream else None
     # two different inputs in a row: the shared workspace keeps the previous
     # call's contents, which must not leak into the next result
     for call, soft in enumerate((1.0, 2.5)):
@@ -45,9 +48,13 @@ def test_noalloc_matches_regular_entry_point_twice(cuda, lib, G):
         rho[rng.integers(0, G, 8), rng.integers(0, G, 8), rng.integers(0, G, 8)] += 50.0
         rho_d = cuda.from_numpy(rho).cuda()
         ref = _solve_regular(cuda, lib, rho_d, G, soft)
-        got = _solve_noalloc(cuda, lib, rho_d, G, soft)
-        span = float(ref.max() - ref.min())
-        assert np.abs(got - ref).max() <= RTOL * span, (G, call)
+        got = _solve_noalloc(cuda, lib, rho_d, G, soft, stream)
+        # the same kernels and the same tables as sd_poisson: the same bits
+        assert np.array_equal(got.view(np.int32), ref.view(np.int32)), (G, call)
+        # and the FP64 solve, within the Poisson tolerance of the stage tests
+        exact = oracle.poisson_periodic_f64(rho.astype(np.float64), soft).reshape(-1)
+        span = float(exact.max() - exact.min())
+        assert np.abs(got - exact).max() <= RTOL * span, (G, call)
 
 
 def test_noalloc_rejects_grids_beyond_its_workspace(cuda, lib):
