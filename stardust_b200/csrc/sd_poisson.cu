@@ -258,9 +258,9 @@ __global__ void __launch_bounds__(256) k_deposit_plan(const int* __restrict__ rs
 // into int64 row sums in shared memory; if the bundle is shared, add the sums into
 // the fixed-point grid and let the last CTA continue with the whole bundle; then
 // convert, transform the 16 rows along x and store the spectrum bricks.
-// A warp whose particles share few base cells (dense rows) first sums equal
-// corners across its lanes, so one lane per cell adds them: the integer sums
-// are the same in any order, and fewer adds land on the same shared word.
+// (Summing equal corners across a warp's lanes first, with __match_any_sync and
+// __reduce_add_sync, made dense scenes slower, not faster: 0.27 against 0.18 ms
+// at 4M particles / 256^3.)
 template <int G>
 __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, const float4* __restrict__ pos,
                                                const int* __restrict__ perm, const int* __restrict__ row_start,
@@ -273,7 +273,6 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
     // Rows are RS = G + 4 words apart, so the row-parallel 16-byte reads of the
     // conversion fall in different banks.
     constexpr int RS = G + 4;
-    constexpr int kAggGroups = 16;
     extern __shared__ float2 sm[];
     const float2* tw = sm;
     unsigned* acc_lo = reinterpret_cast<unsigned*>(sm + G);
@@ -316,7 +315,7 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
     const bool split16 = f_hi - f_lo < 65536;
     const int lane = threadIdx.x & 31;
     constexpr int kBatch = 4;
-    // warp-uniform loop: lane f = base + q * NT + lane
+    // lane f = base + q * NT + lane
     for (int base = f_lo + (threadIdx.x & ~31); base < f_hi; base += kBatch * NT) {
         int src[kBatch];
 #pragma unroll
@@ -340,7 +339,7 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
         for (int q = 0; q < kBatch; ++q) pb[q] = (src[q] >= 0) ? pos[src[q]] : make_float4(-1.f, -1.f, -1.f, 0.f);
 #pragma unroll
         for (int q = 0; q < kBatch; ++q) {
-            if (base + q * NT >= f_hi) break;  // warp-uniform
+            if (base + q * NT >= f_hi) break;
             const float4 p = pb[q];
             const bool valid = p.x >= 0.f;  // empty slots sort into row 0
             int ix, iy, iz;
@@ -348,33 +347,18 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
             cic_axis(p.x, G, ix, fx);
             cic_axis(p.y, G, iy, fy);
             cic_axis(p.z, G, iz, fz);
+            if (!valid) continue;
             const int x0 = ix & m, x1 = (ix + 1) & m;
-            const unsigned cell =
-                valid ? (unsigned)((((iz & m) * G) + (iy & m)) * G + x0) : (0x80000000u | (unsigned)lane);
-            const unsigned grp = __match_any_sync(0xffffffffu, cell);
-            const bool leader = (grp & lanemask_lt()) == 0;
-            const bool merge = __popc(__ballot_sync(0xffffffffu, leader)) <= kAggGroups;  // warp-uniform
-            if (!merge && !valid) continue;
 #pragma unroll
             for (int oyz = 0; oyz < 4; ++oyz) {
                 const int yl = ((iy + (oyz & 1)) & m) - 4 * by;
                 const int zl = ((iz + (oyz >> 1)) & m) - 4 * bz;
-                const bool in = valid && (unsigned)yl < 4u && (unsigned)zl < 4u;
-                if (!merge && !in) continue;
+                if ((unsigned)yl >= 4u || (unsigned)zl >= 4u) continue;
                 const int rowc = (zl * 4 + yl) * RS;
 #pragma unroll
                 for (int ox = 0; ox < 2; ++ox) {
-                    unsigned long long qv =
-                        in ? (unsigned long long)fixed_weight(cic_weight(ox | (oyz << 1), fx, fy, fz)) : 0ull;
-                    if (merge) {
-                        // lanes with the same base cell share every corner cell: sum the
-                        // weight over the group in two 16-bit halves (no overflow for 32
-                        // lanes); the lowest lane adds the exact total
-                        const unsigned hi = __reduce_add_sync(grp, (unsigned)(qv >> 16));
-                        const unsigned lo16 = __reduce_add_sync(grp, (unsigned)(qv & 0xffffu));
-                        qv = ((unsigned long long)hi << 16) + (unsigned long long)lo16;
-                        if (!leader || !in) continue;
-                    }
+                    const unsigned long long qv =
+                        (unsigned long long)fixed_weight(cic_weight(ox | (oyz << 1), fx, fy, fz));
                     const int c = rowc + (ox ? x1 : x0);
                     if (split16) {
                         atomicAdd(acc_hi + c, (unsigned)(qv >> 16));

@@ -247,14 +247,16 @@ static void test_vram_clamp() {
     sim.reconfigure(cfg);
     check(sim.particleCount() == got && sim.simTime() > t0, "repeating the clamped request keeps the scene",
           fmt("N=%g t=%g", sim.particleCount(), sim.simTime()));
-    // a grid that leaves no room for particles fails and changes nothing
+    // a new grid that leaves no room for particles fails and changes nothing
     sd_clear_error();
-    sd_set_device_free_bytes_override(Sim::estimateBytes(1, gCap, Boundary::Isolated) / 2);
+    sd_set_device_free_bytes_override(Sim::estimateBytes(1, gCap / 2, Boundary::Isolated) / 2);
     SimConfig other = cfg;
     other.particleCount = 1000;
+    other.gridSize = gCap / 2;
     sim.reconfigure(other);
     const bool refused = Sim::failed();
-    check(refused && sim.particleCount() == got, "a grid that does not fit is refused", Sim::failMessage());
+    check(refused && sim.particleCount() == got && sim.gridSize() == gCap, "a grid that does not fit is refused",
+          Sim::failMessage());
     sd_clear_error();
     sd_set_device_free_bytes_override(0);
 }
