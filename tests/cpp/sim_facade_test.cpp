@@ -247,15 +247,22 @@ static void test_vram_clamp() {
     sim.reconfigure(cfg);
     check(sim.particleCount() == got && sim.simTime() > t0, "repeating the clamped request keeps the scene",
           fmt("N=%g t=%g", sim.particleCount(), sim.simTime()));
-    // a new grid that leaves no room for particles fails and changes nothing
+    sd_set_device_free_bytes_override(0);
+    // a grid that leaves no room for particles fails and changes nothing: a small
+    // scene asks for the largest periodic grid while 1 byte is free (plus the
+    // memory the small scene holds, which a reallocation would free first)
+    Sim small;
+    SimConfig sc;
+    sc.particleCount = 1000;
+    sc.gridSize = 32;
+    small.init(sc);
     sd_clear_error();
-    sd_set_device_free_bytes_override(Sim::estimateBytes(1, gCap / 2, Boundary::Isolated) / 2);
-    SimConfig other = cfg;
-    other.particleCount = 1000;
-    other.gridSize = gCap / 2;
-    sim.reconfigure(other);
+    sd_set_device_free_bytes_override(1);
+    SimConfig big = sc;
+    big.gridSize = Sim::maxGridSize(Boundary::Periodic);
+    small.reconfigure(big);
     const bool refused = Sim::failed();
-    check(refused && sim.particleCount() == got && sim.gridSize() == gCap, "a grid that does not fit is refused",
+    check(refused && small.particleCount() == 1000 && small.gridSize() == 32, "a grid that does not fit is refused",
           Sim::failMessage());
     sd_clear_error();
     sd_set_device_free_bytes_override(0);
