@@ -244,6 +244,18 @@ int sd_step_auto(sd_sim* sim);
  * when the outputs are written. Use pinned host memory for full copy speed. */
 int sd_step_host(sd_sim* sim, const float* pos_in, const float* vel_in, int n, float dt, float* pos_out,
                  float* vel_out);
+/* The same offload step, pipelined (no reference counterpart): the call queues
+ * the upload, the step and the download and returns. Consecutive calls overlap
+ * one step's download, the next step's computation and the upload after it (both
+ * copy directions at once), through a third particle set the handle allocates on
+ * the first call (32 bytes per slot). The outputs of the queued calls are complete
+ * when sd_step_host_wait returns; until then the caller leaves pos_in and vel_in
+ * unchanged and does not read pos_out or vel_out. Every other call on the handle
+ * first waits for the queued ones. Each call's result is the same as
+ * sd_step_host's on the same inputs. Use pinned host memory. */
+int sd_step_host_async(sd_sim* sim, const float* pos_in, const float* vel_in, int n, float dt, float* pos_out,
+                       float* vel_out);
+int sd_step_host_wait(sd_sim* sim);
 /* nsteps fixed-dt steps; replays a captured CUDA graph after the first call. */
 int sd_steps(sd_sim* sim, float dt, int nsteps);
 /* Leapfrog: apply the closing half kick so velocities are synchronous with

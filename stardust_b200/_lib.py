@@ -129,6 +129,8 @@ SIGNATURES = [
     ("sd_step", _I, [_P, _F]),
     ("sd_step_auto", _I, [_P]),
     ("sd_step_host", _I, [_P, _P, _P, _I, _F, _P, _P]),
+    ("sd_step_host_async", _I, [_P, _P, _P, _I, _F, _P, _P]),
+    ("sd_step_host_wait", _I, [_P]),
     ("sd_steps", _I, [_P, _F, _I]),
     ("sd_synchronize", _I, [_P]),
     ("sd_sort_only", _I, [_P, _P, _I]),

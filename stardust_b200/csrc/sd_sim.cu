@@ -140,6 +140,8 @@ void free_dev(T*& p) {
 
 void free_buffers(sd_sim* s) {
     free_dev(s->pos); free_dev(s->vel); free_dev(s->pos2); free_dev(s->vel2);
+    free_dev(s->stage_pos); free_dev(s->stage_vel);
+    s->stage_free = nullptr;
     free_dev(s->keys); free_dev(s->keys2); free_dev(s->keys3);
     free_dev(s->vals); free_dev(s->vals2);
     if (s->sort_ws) cudaFree(s->sort_ws);
@@ -688,6 +690,20 @@ struct StateHeader {
 static_assert(sizeof(StateHeader) == 76, "STARDUST header layout");
 constexpr size_t kBlackHoleRecord = 48;  // sizeof(BlackHoleState) (Sim.h:813-825)
 
+// Wait for queued offload steps (sd_step_host_async) before any other use of the
+// handle: their uploads, steps and downloads run on three streams, and the other
+// entry points assume the handle's buffers are at rest between calls.
+int settle(sd_sim* s) {
+    if (!s->async_pending) return SD_OK;
+    s->async_pending = false;
+    int rc = SD_OK;
+    if (s->up_stream && SD_CUDA(cudaStreamSynchronize(s->up_stream))) rc = SD_E_CUDA;
+    if (s->io_stream && SD_CUDA(cudaStreamSynchronize(s->io_stream))) rc = SD_E_CUDA;
+    if (SD_CUDA(cudaStreamSynchronize(s->stream))) rc = SD_E_CUDA;
+    s->stage_free = nullptr;
+    return rc ? sim_error(s, rc) : SD_OK;
+}
+
 }  // namespace sdsim
 
 using namespace sdsim;
@@ -854,9 +870,16 @@ int sd_create(sd_sim** out, int device) {
 int sd_destroy(sd_sim* s) {
     if (!s) return SD_OK;
     DeviceGuard g(s->device);
+    settle(s);
     if (s->stream) cudaStreamSynchronize(s->stream);
     free_buffers(s);
     free_dev(s->mlp_params);
+    for (auto& e : s->up_ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : s->down_ev)
+        if (e) cudaEventDestroy(e);
+    if (s->out_ev) cudaEventDestroy(s->out_ev);
+    if (s->up_stream) cudaStreamDestroy(s->up_stream);
     for (auto& e : s->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : s->pev)
@@ -875,6 +898,7 @@ int sd_destroy(sd_sim* s) {
 int sd_set_stream(sd_sim* s, void* stream) {
     if (!s) return fail(SD_E_ARG, "set_stream: null handle");
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     cudaStreamSynchronize(s->stream);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     s->stream = (cudaStream_t)stream;
@@ -887,6 +911,7 @@ int sd_set_stream(sd_sim* s, void* stream) {
 int sd_init(sd_sim* s, const sd_config* c) {
     if (!s) return fail(SD_E_ARG, "init: null handle");
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     s->configured = false;
     return reconfigure(s, c);
 }
@@ -894,12 +919,14 @@ int sd_init(sd_sim* s, const sd_config* c) {
 int sd_reconfigure(sd_sim* s, const sd_config* c) {
     if (!s) return fail(SD_E_ARG, "reconfigure: null handle");
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     return reconfigure(s, c);
 }
 
 int sd_reset(sd_sim* s) {
     if (!s || !s->configured) return fail(SD_E_STATE, "reset: not initialised");
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     s->sim_time = 0.0;
     s->step_count = 0;
     s->lf_open = false;
@@ -918,6 +945,7 @@ int sd_set_particles(sd_sim* s, const float* pos, const float* vel, int n, int w
     if (!s || !s->configured) return fail(SD_E_STATE, "set_particles: not initialised");
     if (!pos || !vel || n < 0 || n > s->N) return fail(SD_E_ARG, "set_particles: bad arguments (n=%d)", n);
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     int rc = copy_in(s->pos, pos, sizeof(float4) * (size_t)n, where, s->stream);
     if (!rc) rc = copy_in(s->vel, vel, sizeof(float4) * (size_t)n, where, s->stream);
     if (!rc) rc = launch_hide_range(s->pos, s->vel, n, s->N, s->stream);
@@ -936,6 +964,7 @@ int sd_get_particles(sd_sim* s, float* pos, float* vel, int n, int where) {
     if (!s || !s->configured) return fail(SD_E_STATE, "get_particles: not initialised");
     if (n < 0 || n > s->N) return fail(SD_E_ARG, "get_particles: bad n=%d", n);
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     int rc = materialize(s);
     if (!rc && pos) rc = copy_out(pos, s->pos, sizeof(float4) * (size_t)n, where, s->stream);
     if (!rc && vel) rc = copy_out(vel, s->vel, sizeof(float4) * (size_t)n, where, s->stream);
@@ -945,6 +974,7 @@ int sd_get_particles(sd_sim* s, float* pos, float* vel, int n, int where) {
 const float* sd_particle_pos_device_ptr(sd_sim* s) {
     if (!s || !s->configured) return nullptr;
     DeviceGuard g(s->device);
+    settle(s);
     materialize(s);
     return reinterpret_cast<const float*>(s->pos);
 }
@@ -952,6 +982,7 @@ const float* sd_particle_pos_device_ptr(sd_sim* s) {
 const float* sd_particle_vel_device_ptr(sd_sim* s) {
     if (!s || !s->configured) return nullptr;
     DeviceGuard g(s->device);
+    settle(s);
     materialize(s);
     return reinterpret_cast<const float*>(s->vel);
 }
@@ -964,6 +995,7 @@ const float* sd_density_device_ptr(sd_sim* s) {
 int sd_get_density(sd_sim* s, float* out, int where) {
     if (!s || !s->configured || !out) return fail(SD_E_STATE, "get_density: not initialised");
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     if (!s->rho) return fail(SD_E_STATE, "get_density: keep_density is off");
     if (!s->rho_valid) {  // no step yet: density of the current positions
         int rc = do_field(s, true);
@@ -975,6 +1007,7 @@ int sd_get_density(sd_sim* s, float* out, int where) {
 int sd_get_potential(sd_sim* s, float* out, int where) {
     if (!s || !s->configured || !out) return fail(SD_E_STATE, "get_potential: not initialised");
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     if (!isolated(s)) return copy_out(out, s->phi, sizeof(float) * (size_t)s->G * s->G * s->G, where, s->stream);
     // isolated: the G^3 corner of the 2G box, one 2D copy per z plane
     const int G = s->G, S = 2 * G;
@@ -990,6 +1023,7 @@ int sd_get_accel(sd_sim* s, float* out, int n, int where) {
     if (!s || !s->configured || !out) return fail(SD_E_STATE, "get_accel: not initialised");
     if (n < 0 || n > s->N) return fail(SD_E_ARG, "get_accel: bad n=%d", n);
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     int rc = do_field(s, keeps_rho(s));
     if (rc) return sim_error(s, rc);
     if (s->mlp_on && (rc = mlp_correction(s, nullptr))) return sim_error(s, rc);
@@ -1007,6 +1041,7 @@ int sd_set_mlp(sd_sim* s, const float* params_device, float out_scale) {
     if (!s || !s->configured) return fail(SD_E_STATE, "set_mlp: not initialised");
     if (params_device && isolated(s)) return fail(SD_E_UNSUPPORTED, "set_mlp: the correction is trained for periodic boxes");
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     if (s->graph) cudaGraphExecDestroy(s->graph);  // replays must see the new setting
     s->graph = nullptr;
     if (!params_device) {
@@ -1030,6 +1065,7 @@ int sd_set_mlp(sd_sim* s, const float* params_device, float out_scale) {
 int sd_step(sd_sim* s, float dt) {
     if (!s) return fail(SD_E_ARG, "step: null handle");
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     const bool sort = sort_due(s);
     int rc = do_step(s, dt, sort, true);
     if (rc) return rc;
@@ -1044,6 +1080,7 @@ int sd_step_host(sd_sim* s, const float* pos_in, const float* vel_in, int n, flo
     if (!pos_in || !vel_in || !pos_out || !vel_out || n < 0 || n > s->N)
         return fail(SD_E_ARG, "step_host: bad arguments (n=%d)", n);
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     if (!s->io_stream) {
         if (SD_CUDA(cudaStreamCreateWithFlags(&s->io_stream, cudaStreamNonBlocking))) return SD_E_CUDA;
         for (auto& e : s->io_ev)
@@ -1095,9 +1132,100 @@ int sd_step_host(sd_sim* s, const float* pos_in, const float* vel_in, int n, flo
     return SD_OK;
 }
 
+int sd_step_host_async(sd_sim* s, const float* pos_in, const float* vel_in, int n, float dt, float* pos_out,
+                       float* vel_out) {
+    if (!s || !s->configured) return fail(SD_E_STATE, "step_host_async: not initialised");
+    if (!pos_in || !vel_in || !pos_out || !vel_out || n < 0 || n > s->N)
+        return fail(SD_E_ARG, "step_host_async: bad arguments (n=%d)", n);
+    DeviceGuard g(s->device);
+    if (!s->up_stream) {
+        if (SD_CUDA(cudaStreamCreateWithFlags(&s->up_stream, cudaStreamNonBlocking))) return SD_E_CUDA;
+        for (auto& e : s->up_ev)
+            if (SD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming))) return SD_E_CUDA;
+        for (auto& e : s->down_ev)
+            if (SD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming))) return SD_E_CUDA;
+        if (SD_CUDA(cudaEventCreateWithFlags(&s->out_ev, cudaEventDisableTiming))) return SD_E_CUDA;
+    }
+    if (!s->io_stream && SD_CUDA(cudaStreamCreateWithFlags(&s->io_stream, cudaStreamNonBlocking))) return SD_E_CUDA;
+    // the staging set: allocated by the first call, kept with the other particle buffers
+    if (!s->stage_pos) {
+        int rc = settle(s);
+        if (!rc) rc = alloc_dev(s->stage_pos, (size_t)s->N);
+        if (!rc) rc = alloc_dev(s->stage_vel, (size_t)s->N);
+        if (rc) return rc;
+        s->stage_free = nullptr;
+    }
+    const size_t bytes = sizeof(float4) * (size_t)n;
+    cudaStream_t st = s->stream, io = s->io_stream, up = s->up_stream;
+    // on failure the queued work is drained before returning, so no copy still
+    // reads or writes the caller's buffers
+    auto drain = [&](int code) {
+        s->async_pending = true;
+        settle(s);
+        return sim_error(s, code);
+    };
+    // 1. upload into the staging set once its last download (two calls ago) is done
+    int rc = SD_OK;
+    if (s->stage_free) rc = SD_CUDA(cudaStreamWaitEvent(up, s->stage_free, 0));
+    if (!rc) rc = SD_CUDA(cudaMemcpyAsync(s->stage_pos, pos_in, bytes, cudaMemcpyHostToDevice, up));
+    if (!rc) rc = SD_CUDA(cudaEventRecord(s->up_ev[0], up));
+    if (!rc) rc = SD_CUDA(cudaMemcpyAsync(s->stage_vel, vel_in, bytes, cudaMemcpyHostToDevice, up));
+    if (!rc) rc = SD_CUDA(cudaEventRecord(s->up_ev[1], up));
+    if (rc) return drain(rc);
+    // 2. rotate the three particle sets: the staged inputs become the step's input;
+    // the last result, still downloading, becomes the next staging set (free once
+    // its download event fires); the last input stays the step's output buffer
+    float4* const last_pos = s->pos;
+    float4* const last_vel = s->vel;
+    s->pos = s->stage_pos;
+    s->vel = s->stage_vel;
+    s->stage_pos = last_pos;
+    s->stage_vel = last_vel;
+    s->stage_free = (s->async_calls > 0 && s->async_pending) ? s->down_ev[(s->async_calls - 1) & 1] : nullptr;
+    s->async_pending = true;
+    // 3. the step, on the handle's stream, after the positions arrive; the first
+    // kernel that reads velocities waits for them
+    rc = SD_CUDA(cudaStreamWaitEvent(st, s->up_ev[0], 0));
+    if (!rc) rc = launch_hide_range(s->pos, s->vel, n, s->N, st);  // slots >= n: disjoint from the copy
+    if (!rc && SD_CUDA(cudaMemsetAsync(s->mean, 0, sizeof(float) * 4, st))) rc = SD_E_CUDA;
+    if (rc) return drain(rc);
+    s->active = n;
+    s->mean_pending = false;
+    s->lf_open = false;
+    s->rho_valid = false;
+    invalidate_keys(s);
+    s->vel_wait = s->up_ev[1];
+    rc = do_step(s, dt, sort_due(s), false);
+    if (s->vel_wait) {  // a step that read no velocity still owes the wait
+        if (!rc) rc = SD_CUDA(cudaStreamWaitEvent(st, s->vel_wait, 0));
+        s->vel_wait = nullptr;
+    }
+    if (!rc) rc = materialize(s);
+    if (rc) return drain(rc);
+    s->tm.dt_used = dt;
+    s->tm.steps = 1;
+    // 4. download the result on the offload stream
+    const int k = (int)(s->async_calls & 1);
+    rc = SD_CUDA(cudaEventRecord(s->out_ev, st));
+    if (!rc) rc = SD_CUDA(cudaStreamWaitEvent(io, s->out_ev, 0));
+    if (!rc) rc = SD_CUDA(cudaMemcpyAsync(pos_out, s->pos, bytes, cudaMemcpyDeviceToHost, io));
+    if (!rc) rc = SD_CUDA(cudaMemcpyAsync(vel_out, s->vel, bytes, cudaMemcpyDeviceToHost, io));
+    if (!rc) rc = SD_CUDA(cudaEventRecord(s->down_ev[k], io));
+    if (rc) return drain(rc);
+    ++s->async_calls;
+    return SD_OK;
+}
+
+int sd_step_host_wait(sd_sim* s) {
+    if (!s) return fail(SD_E_ARG, "step_host_wait: null handle");
+    DeviceGuard g(s->device);
+    return settle(s);
+}
+
 int sd_step_auto(sd_sim* s) {
     if (!s || !s->configured) return fail(SD_E_STATE, "step_auto: not initialised");
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     // CFL (Sim.cu:4255-4269): vmax of the current (momentum-zeroed) velocities.
     int rc = launch_max_speed(s->pos, s->vel, s->N, s->mean_pending ? s->mean : nullptr, s->mean + 3, s->stream);
     if (rc) return sim_error(s, rc);
@@ -1120,6 +1248,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
     if (!s || !s->configured) return fail(SD_E_STATE, "steps: not initialised");
     if (nsteps < 0) return fail(SD_E_ARG, "steps: negative count");
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     // A two-step graph repeats the cooling schedule only when its period is 2.
     const bool graphable = (s->cfg.sort_interval == 0 || s->cfg.sort_interval == 1) &&
                            (!hydro_on(s) || cooling_period(s) == 2);
@@ -1220,6 +1349,7 @@ int sd_synchronize(sd_sim* s) {
     if (!s || !s->configured) return fail(SD_E_STATE, "synchronize: not initialised");
     if (s->cfg.integrator != SD_INT_KDK || !s->lf_open) return SD_OK;
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     int rc = do_field(s, keeps_rho(s));
     if (rc) return sim_error(s, rc);
     if (s->mlp_on && (rc = mlp_correction(s, nullptr))) return sim_error(s, rc);
@@ -1238,6 +1368,7 @@ int sd_synchronize(sd_sim* s) {
 int sd_sort_only(sd_sim* s, int32_t* perm, int where) {
     if (!s || !s->configured) return fail(SD_E_STATE, "sort_only: not initialised");
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     int32_t* dev_perm = nullptr;
     if (perm && where == SD_DEVICE) dev_perm = perm;
     int rc = do_sort(s, dev_perm);
@@ -1254,6 +1385,7 @@ int sd_sort_only(sd_sim* s, int32_t* perm, int where) {
 int sd_save_state(sd_sim* s, const char* path) {
     if (!s || !s->configured || !path) return fail(SD_E_STATE, "save_state: not initialised");
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     const int n = (s->active > 0) ? s->active : s->N;
     std::vector<float4> hp((size_t)n), hv((size_t)n);
     int rc = sd_get_particles(s, reinterpret_cast<float*>(hp.data()), reinterpret_cast<float*>(hv.data()), n, SD_HOST);
@@ -1280,6 +1412,7 @@ int sd_save_state(sd_sim* s, const char* path) {
 int sd_load_state(sd_sim* s, const char* path) {
     if (!s || !path) return fail(SD_E_ARG, "load_state: null");
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     FILE* f = fopen(path, "rb");
     if (!f) return fail(SD_E_IO, "load_state: cannot open %s", path);
     StateHeader h;
@@ -1364,6 +1497,7 @@ int sd_step_count(const sd_sim* s) { return s ? s->step_count : 0; }
 static double reduce_rho(sd_sim* s, int op) {
     if (!s || !s->configured || !s->rho) return 0.0;
     DeviceGuard g(s->device);
+    settle(s);
     if (!s->rho_valid && do_field(s, true)) return 0.0;
     double out = 0.0;
     if (launch_reduce_grid(s->rho, (size_t)s->G * s->G * s->G, op, s->partials, s->mom + 7, s->stream)) return 0.0;
@@ -1380,6 +1514,7 @@ int sd_measure_centroid(sd_sim* s, double* cx, double* cy) {
     if (cy) *cy = 0.5;
     if (!s || !s->configured || !cx || !cy) return fail(SD_E_ARG, "measure_centroid: not initialised or null output");
     DeviceGuard g(s->device);
+    settle(s);
     double out[3] = {0.0, 0.0, 0.0};
     int rc = launch_centroid(s->pos, s->N, s->partials, s->mom + 5, s->stream);
     if (!rc) rc = copy_out(out, s->mom + 5, sizeof(double) * 3, SD_HOST, s->stream);
@@ -1394,6 +1529,7 @@ int sd_measure_centroid(sd_sim* s, double* cx, double* cy) {
 double sd_measure_kinetic_energy(sd_sim* s) {
     if (!s || !s->configured) return 0.0;
     DeviceGuard g(s->device);
+    settle(s);
     double out[8];
     if (launch_energy(nullptr, s->G, s->pos, s->vel, s->N, s->mean_pending ? s->mean : nullptr, s->partials, s->mom,
                       s->stream))
@@ -1405,6 +1541,7 @@ double sd_measure_kinetic_energy(sd_sim* s) {
 int sd_diagnostics_get(sd_sim* s, sd_diagnostics* out) {
     if (!s || !out || !s->configured) return fail(SD_E_ARG, "diagnostics: null");
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     double d[8];
     // momentum sums of the last gather (before zeroing) and energies after zeroing
     int rc = launch_energy(s->phi, s->G, s->pos, s->vel, s->N, s->mean_pending ? s->mean : nullptr, s->partials,
@@ -1430,6 +1567,7 @@ int sd_diagnostics_get(sd_sim* s, sd_diagnostics* out) {
 int sd_diagnostics_history(sd_sim* s, double* out, int max_records, int* count_out) {
     if (!s || !s->configured || !out || max_records < 0) return fail(SD_E_ARG, "diagnostics_history: bad arguments");
     DeviceGuard g(s->device);
+    if (int rc_settle = settle(s)) return rc_settle;
     unsigned long long total = 0;
     if (copy_out(&total, s->diag_count, sizeof(total), SD_HOST, s->stream)) return sim_error(s, SD_E_CUDA);
     const unsigned long long avail = total < (unsigned long long)kDiagCap ? total : (unsigned long long)kDiagCap;

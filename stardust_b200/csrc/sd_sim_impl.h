@@ -66,6 +66,17 @@ struct sd_sim {
     cudaStream_t io_stream = nullptr;
     cudaEvent_t io_ev[2] = {nullptr, nullptr};
     cudaEvent_t vel_wait = nullptr;
+    // pipelined offload (sd_step_host_async): a third particle set that stages the
+    // next step's inputs, the stream that uploads into it, and the events ordering
+    // uploads, steps and downloads across calls
+    cudaStream_t up_stream = nullptr;
+    float4 *stage_pos = nullptr, *stage_vel = nullptr;
+    cudaEvent_t up_ev[2] = {nullptr, nullptr};    // this call's positions / velocities are on the device
+    cudaEvent_t out_ev = nullptr;                 // this call's result is ready to download
+    cudaEvent_t down_ev[2] = {nullptr, nullptr};  // downloads done, alternating between calls
+    cudaEvent_t stage_free = nullptr;             // the staging set's last download (null: free)
+    long long async_calls = 0;
+    bool async_pending = false;                   // offload work queued and not waited for
     bool ev_valid = false;
     sd_timings tm{};
     sd_diagnostics diag{};

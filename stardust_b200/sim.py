@@ -259,6 +259,16 @@ class Sim:
                 "sd_step_host")
         return out
 
+    def step_host_async(self, pos, vel, dt: float, out) -> None:
+        """Queue one offload step (sd_step_host_async): ``pos``/``vel`` pinned CPU
+        tensors, ``out`` = (pos, vel) pinned CPU tensors written by the time
+        ``step_host_wait`` returns. Consecutive calls overlap their copies."""
+        L.check(L.lib().sd_step_host_async(self._h, pos.data_ptr(), vel.data_ptr(), int(pos.shape[0]), float(dt),
+                                           out[0].data_ptr(), out[1].data_ptr()), "sd_step_host_async")
+
+    def step_host_wait(self) -> None:
+        L.check(L.lib().sd_step_host_wait(self._h), "sd_step_host_wait")
+
     def step(self, dt: float | None = None) -> None:
         """``step()`` is the reference's CFL-clamped step; ``step(dt)`` advances by dt."""
         if dt is None:

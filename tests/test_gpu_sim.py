@@ -331,6 +331,33 @@ def test_step_host_equals_set_step_get(cuda, order, diag):
         assert np.array_equal(b.view(np.int32), d.view(np.int32))
 
 
+@pytest.mark.parametrize("order", [L.SD_ORDER_ROWMAJOR, L.SD_ORDER_TILED])
+def test_pipelined_offload_equals_offload_step(cuda, order):
+    """sd_step_host_async queues upload, step and download and returns; five calls
+    in a row (inputs staged in a third particle set while the previous result
+    downloads) give each step's result bit for bit as sd_step_host does, also with
+    n below capacity, and the handle is usable normally afterwards."""
+    G, N, n = 32, 70_000, 65_000
+    ins = [random_particles(n, 60 + k, clustered=True) for k in range(5)]
+    with make_sim(cuda, N, G, gravity=300.0, softening_cells=1.0, order=order) as s:
+        ref = [s.step_host(p, v, 1e-3) for p, v in ins]
+    pinned = [(cuda.from_numpy(p).pin_memory(), cuda.from_numpy(v).pin_memory()) for p, v in ins]
+    outs = [(cuda.empty((n, 4), dtype=cuda.float32).pin_memory(), cuda.empty((n, 4), dtype=cuda.float32).pin_memory())
+            for _ in ins]
+    with make_sim(cuda, N, G, gravity=300.0, softening_cells=1.0, order=order) as s:
+        for (p, v), o in zip(pinned, outs):
+            s.step_host_async(p, v, 1e-3, o)
+        s.step_host_wait()
+        for (p, v), (a, b) in zip(ref, outs):
+            assert np.array_equal(p.view(np.int32), a.numpy().view(np.int32))
+            assert np.array_equal(v.view(np.int32), b.numpy().view(np.int32))
+        # the handle holds the last result and steps on from it as usual
+        p_last, v_last = s.get_particles(n)
+        assert np.array_equal(p_last.view(np.int32), outs[-1][0].numpy().view(np.int32))
+        s.step(1e-3)
+        assert s.get_particles(n)[0].shape == (n, 4)
+
+
 def _mover_scene(n, seed, speed):
     """Particles moving fast enough that many cross rows (y and z, across the
     4x4-row bundles) every step, with empty slots."""
