@@ -277,6 +277,13 @@ int sd_particle_count(const sd_sim* sim);                           /* Sim::part
 int sd_particle_capacity(const sd_sim* sim);                        /* slots allocated (capacityN, Sim.cu:3032-3045) */
 int sd_active_count(const sd_sim* sim);                             /* Sim::activeCount */
 int sd_step_count(const sd_sim* sim);
+/* The merge sort (tiled order, periodic; no reference counterpart) measures the
+ * share of particles whose row key changed since the last sorted step. Above 10 %
+ * the steps run the full radix sort instead (the same permutation), with one
+ * probing merge every 64 steps. sd_changed_fraction: the last measured share
+ * (-1 before the first merge); sd_merge_sorting: 1 while merges are chosen. */
+double sd_changed_fraction(const sd_sim* sim);
+int sd_merge_sorting(const sd_sim* sim);
 double sd_measure_total_grid_mass(sd_sim* sim);                     /* Sim.cu:4890-4906 */
 double sd_measure_max_density(sd_sim* sim);                         /* Sim.cu:4908-4924 */
 double sd_measure_kinetic_energy(sd_sim* sim);                      /* Sim.cu:5141-5149 */

@@ -143,6 +143,8 @@ SIGNATURES = [
     ("sd_particle_capacity", _I, [_P]),
     ("sd_active_count", _I, [_P]),
     ("sd_step_count", _I, [_P]),
+    ("sd_changed_fraction", _D, [_P]),
+    ("sd_merge_sorting", _I, [_P]),
     ("sd_measure_total_grid_mass", _D, [_P]),
     ("sd_measure_max_density", _D, [_P]),
     ("sd_measure_kinetic_energy", _D, [_P]),

@@ -265,7 +265,7 @@ template <int G>
 __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, const float4* __restrict__ pos,
                                                const int* __restrict__ perm, const int* __restrict__ row_start,
                                                float* __restrict__ rho_keep, float2* __restrict__ spec,
-                                               const DepositWork& w, unsigned* __restrict__ arrive) {
+                                               const DepositWork& w, unsigned* __restrict__ arrive, bool reuse) {
     using T = Geo<G>;
     constexpr int H = T::H, NBX = T::NBX, NT = kDepositThreads, TB = G / 4;
     // The int64 fixed-point sums, as two 32-bit words per cell (lo[16][RS], hi[16][RS]),
@@ -289,7 +289,7 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
         window_range<G>(b, j, row_start, lo, hi);
         len = hi - lo;
     }
-    __syncthreads();  // the shared buffers of the previous bundle are free
+    if (reuse) __syncthreads();  // the shared buffers of this CTA's previous bundle are free
     for (int i = threadIdx.x; i < 8 * RS; i += NT) reinterpret_cast<uint4*>(acc_lo)[i] = make_uint4(0u, 0u, 0u, 0u);
     if (threadIdx.x < 32) {
         int inc = len;
@@ -506,7 +506,8 @@ __global__ void __launch_bounds__(kDepositThreads, G >= 512 ? 3 : 2)
             b = lo;
             slice = 1 + e - (cta_pre[lo >> 8] + xpre[lo]);
         }
-        deposit_bundle<G>(b, slice, items[b], pos, perm, row_start, rho_keep, spec, w, arrive);
+        deposit_bundle<G>(b, slice, items[b], pos, perm, row_start, rho_keep, spec, w, arrive,
+                          !first && e != (int)blockIdx.x);
         if (first) break;
     }
 }

@@ -298,6 +298,34 @@ bool incr_possible(const sd_sim* s) {
     return s->allow_incr && !s->cfg.full_sort && s->cfg.order == SD_ORDER_TILED && !isolated(s);
 }
 
+// Above this share of changed keys the full radix sort is cheaper than the merge
+// (4M particles on 256^3 with a third of the keys changing: merge 0.146 ms, full
+// sort with its row table 0.093 ms; 16M on 512^3 with 0.8 % changing: merge
+// 0.12 ms, full sort 0.23 ms).
+constexpr double kMergeMaxFraction = 0.10;
+constexpr int kMergeProbe = 64;
+
+// The next sorted step leaves change bits for a merge (otherwise first-pass counts).
+bool merge_next(const sd_sim* s) { return s->rs_base && incr_possible(s) && !s->merge_off; }
+
+// Read the share of keys the last merge found changed (written to pinned memory
+// by the device, possibly a step or more behind) and choose merge or full sort.
+void update_merge_policy(sd_sim* s) {
+    if (!s->rs_base || !s->chg_host) return;
+    const int c = *reinterpret_cast<volatile int*>(s->chg_host);
+    if (c >= 0 && s->N > 0) s->chg_frac = (double)c / (double)s->N;
+    if (!s->merge_off) {
+        if (c >= 0 && s->chg_frac > kMergeMaxFraction) {
+            s->merge_off = true;
+            s->merge_probe_at = s->step_count + kMergeProbe;
+        }
+    } else if (s->step_count >= s->merge_probe_at) {
+        // probe: merge again, and decide on the share that merge measures
+        s->merge_off = false;
+        *reinterpret_cast<volatile int*>(s->chg_host) = -1;
+    }
+}
+
 // Merge-sort buffers exist while the configuration can merge-sort (zeroed when made).
 int ensure_resort(sd_sim* s) {
     if (!incr_possible(s)) {
@@ -307,6 +335,16 @@ int ensure_resort(sd_sim* s) {
         return SD_OK;
     }
     if (s->rs_base) return SD_OK;
+    if (!s->chg_host) {
+        if (cudaHostAlloc((void**)&s->chg_host, sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            s->chg_host = nullptr;
+            return fail(SD_E_NOMEM, "cudaHostAlloc of the changed-key count failed");
+        }
+        *s->chg_host = -1;
+    }
+    s->chg_frac = -1.0;
+    s->merge_off = false;
     const size_t b = resort_bytes(s->N, s->G);
     if (cudaMalloc(&s->rs_base, b) != cudaSuccess) {
         cudaGetLastError();
@@ -431,13 +469,17 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     const int32_t* perm = nullptr;
     // After a sorted step whose gather marked the changed keys, the sort is a merge
     // of those few into the rest (sd_resort.cu); otherwise the full radix sort.
-    const bool incr_next = sort && s->rs_base && incr_possible(s);
+    const bool incr_next = sort && merge_next(s);
     bool merged = false;  // the merge also left the new row table
     if (sort) {
         if (s->incr_ready && s->keys_valid && s->rs_base) {
             rc = launch_resort(s->rs, s->keys, s->N, s->G, key_bits_for(s->G, s->cfg.order), s->row_start, s->vals,
                                s->sort_ws, s->sort_ws_bytes, s->stream);
             if (rc) return sim_error(s, rc);
+            // the share of changed keys, for the choice between merge and full sort
+            if (s->chg_host && SD_CUDA(cudaMemcpyAsync(s->chg_host, s->rs.n_changed, sizeof(int),
+                                                       cudaMemcpyDeviceToHost, s->stream)))
+                return sim_error(s, SD_E_CUDA);
             s->chg_dirty = false;  // consumed and cleared
             merged = true;
         } else {
@@ -880,6 +922,7 @@ int sd_destroy(sd_sim* s) {
         if (e) cudaEventDestroy(e);
     if (s->out_ev) cudaEventDestroy(s->out_ev);
     if (s->up_stream) cudaStreamDestroy(s->up_stream);
+    if (s->chg_host) cudaFreeHost(s->chg_host);
     for (auto& e : s->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : s->pev)
@@ -1066,6 +1109,7 @@ int sd_step(sd_sim* s, float dt) {
     if (!s) return fail(SD_E_ARG, "step: null handle");
     DeviceGuard g(s->device);
     if (int rc_settle = settle(s)) return rc_settle;
+    update_merge_policy(s);
     const bool sort = sort_due(s);
     int rc = do_step(s, dt, sort, true);
     if (rc) return rc;
@@ -1253,6 +1297,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
     const bool graphable = (s->cfg.sort_interval == 0 || s->cfg.sort_interval == 1) &&
                            (!hydro_on(s) || cooling_period(s) == 2);
     int done = 0;
+    update_merge_policy(s);
     // leapfrog opening kick and odd counts run eagerly
     while (done < nsteps && (!graphable || (s->cfg.integrator == SD_INT_KDK && !s->lf_open))) {
         int rc = do_step(s, dt, sort_due(s), false);
@@ -1275,7 +1320,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
         // buffer of the pair, the cooling phase moved, or its first step would sort
         // differently (a merge needs the last step's change bits).
         if (!s->graph || s->graph_dt != dt || s->graph_pos != s->pos || s->graph_phase != phase ||
-            s->graph_incr != incr_now) {
+            s->graph_incr != incr_now || s->graph_merge_off != s->merge_off) {
             if (s->graph) cudaGraphExecDestroy(s->graph);
             s->graph = nullptr;
             cudaGraph_t graph = nullptr;
@@ -1318,6 +1363,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
             s->graph_pos = s->pos;
             s->graph_phase = phase;
             s->graph_incr = incr_now;
+            s->graph_merge_off = s->merge_off;
         }
         if (SD_CUDA(cudaGraphLaunch(s->graph, s->stream))) return sim_error(s, SD_E_CUDA);
         count_launch(s->graph_launches);
@@ -1326,7 +1372,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
         s->mean_pending = true;
         s->keys_valid = true;
         {  // the graph's last step leaves what do_step leaves after a sorted step
-            const bool incr_next = sort && s->rs_base && incr_possible(s);
+            const bool incr_next = sort && merge_next(s);
             s->counts_valid = sort && !incr_next;
             s->incr_ready = incr_next;
             if (incr_next) s->chg_dirty = true;
@@ -1491,6 +1537,8 @@ double sd_sim_time(const sd_sim* s) { return s ? s->sim_time : 0.0; }
 int sd_grid_size(const sd_sim* s) { return s ? s->G : 0; }
 int sd_particle_count(const sd_sim* s) { return s ? s->N : 0; }
 int sd_particle_capacity(const sd_sim* s) { return s ? s->capacity : 0; }
+double sd_changed_fraction(const sd_sim* s) { return s ? s->chg_frac : -1.0; }
+int sd_merge_sorting(const sd_sim* s) { return (s && s->rs_base && incr_possible(s) && !s->merge_off) ? 1 : 0; }
 int sd_active_count(const sd_sim* s) { return s ? s->active : 0; }
 int sd_step_count(const sd_sim* s) { return s ? s->step_count : 0; }
 

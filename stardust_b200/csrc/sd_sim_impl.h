@@ -50,6 +50,14 @@ struct sd_sim {
     bool incr_ready = false;     // the last step left change bits and its row table: merge-sort next
     bool chg_dirty = false;      // change bits written and not consumed yet (cleared before reuse)
     bool allow_incr = true;      // merge sorting allowed (ensemble members sort in full)
+    // Merge or full sort, by the share of keys that changed: each merge copies its
+    // changed-key count to chg_host (pinned); above kMergeMaxFraction the steps
+    // run the full sort, with one probing merge every kMergeProbe steps
+    int* chg_host = nullptr;
+    double chg_frac = -1.0;      // the last measured share (-1: none yet)
+    bool merge_off = false;
+    int merge_probe_at = 0;
+    bool graph_merge_off = false;  // merge_off when the sd_steps graph was captured
     void* rs_base = nullptr;     // merge-sort buffers (tiled order, periodic)
     sd::ResortBufs rs;
     sd::PoissonPlan plan;

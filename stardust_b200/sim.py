@@ -320,6 +320,13 @@ class Sim:
     def step_count(self) -> int:
         return int(L.lib().sd_step_count(self._h))
 
+    def changed_fraction(self) -> float:
+        """Share of keys the last merge sort found changed (-1 before the first)."""
+        return float(L.lib().sd_changed_fraction(self._h))
+
+    def merge_sorting(self) -> bool:
+        return bool(L.lib().sd_merge_sorting(self._h))
+
     def measure_total_grid_mass(self) -> float:
         return float(L.lib().sd_measure_total_grid_mass(self._h))
 

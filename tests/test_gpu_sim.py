@@ -358,6 +358,33 @@ def test_pipelined_offload_equals_offload_step(cuda, order):
         assert s.get_particles(n)[0].shape == (n, 4)
 
 
+@pytest.mark.parametrize("speed,merges", [(0.05, True), (3.0, False)])
+def test_merge_gives_way_to_the_full_sort_when_many_keys_change(cuda, speed, merges):
+    """The merge sort measures the share of changed keys; above 10 % the steps run
+    the full radix sort instead. Slow particles keep merging, fast ones switch;
+    either way every step equals the full sort's bit for bit, eagerly and in
+    graph replay."""
+    G, n = 64, 300_000
+    pos, vel = _mover_scene(n, 7, speed)
+    outs = []
+    for full in (0, 1):
+        with make_sim(cuda, n, G, gravity=100.0, softening_cells=1.0, order=L.SD_ORDER_TILED, full_sort=full) as s:
+            s.set_particles(pos, vel)
+            for _ in range(4):
+                s.step(1e-3)
+            s.get_particles()  # the measured share reaches the host by the time this returns
+            s.steps(1e-3, 6)
+            s.step(1e-3)
+            outs.append(s.get_particles())
+            if not full:
+                frac = s.changed_fraction()
+                assert 0.0 <= frac <= 1.0
+                assert (frac <= 0.10) == merges
+                assert s.merge_sorting() == merges
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a.view(np.int32), b.view(np.int32))
+
+
 def _mover_scene(n, seed, speed):
     """Particles moving fast enough that many cross rows (y and z, across the
     4x4-row bundles) every step, with empty slots."""
