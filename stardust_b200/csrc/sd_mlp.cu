@@ -53,6 +53,20 @@ __device__ __forceinline__ float tanh_approx(float x) {
     return y;
 }
 __device__ __forceinline__ float sigmoid(float z) { return fmaf(0.5f, tanh_approx(0.5f * z), 0.5f); }
+
+// SiLU of two pre-activations, computed and returned as packed BF16 (the inference's
+// next-layer input): z is rounded to BF16 first, then z * (1/2 + tanh(z/2) / 2) with
+// the packed BF16 tanh, so one special-function instruction serves two units.
+__device__ __forceinline__ unsigned silu_bf16x2(float z0, float z1) {
+    const __nv_bfloat162 z = __floats2bfloat162_rn(z0, z1);
+    const __nv_bfloat162 half = __floats2bfloat162_rn(0.5f, 0.5f);
+    const __nv_bfloat162 hz = __hmul2(z, half);  // exact: a power of two
+    unsigned t;
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(*reinterpret_cast<const unsigned*>(&hz)));
+    const __nv_bfloat162 s = __hfma2(*reinterpret_cast<const __nv_bfloat162*>(&t), half, half);
+    const __nv_bfloat162 r = __hmul2(z, s);
+    return *reinterpret_cast<const unsigned*>(&r);
+}
 __device__ __forceinline__ float silu(float z) { return z * sigmoid(z); }
 __device__ __forceinline__ float silu_grad(float z) {
     const float s = sigmoid(z);
@@ -147,10 +161,10 @@ __device__ __forceinline__ void mlp_tile(const __nv_bfloat16 (*xs)[kXPad], int r
 #pragma unroll
     for (int j = 0; j < kH / 16; ++j) {
         const int c0 = 16 * j + 2 * t, c1 = c0 + 8;
-        h[j][0] = pack_bf16(silu(acc[2 * j][0] + bias[c0]), silu(acc[2 * j][1] + bias[c0 + 1]));
-        h[j][1] = pack_bf16(silu(acc[2 * j][2] + bias[c0]), silu(acc[2 * j][3] + bias[c0 + 1]));
-        h[j][2] = pack_bf16(silu(acc[2 * j + 1][0] + bias[c1]), silu(acc[2 * j + 1][1] + bias[c1 + 1]));
-        h[j][3] = pack_bf16(silu(acc[2 * j + 1][2] + bias[c1]), silu(acc[2 * j + 1][3] + bias[c1 + 1]));
+        h[j][0] = silu_bf16x2(acc[2 * j][0] + bias[c0], acc[2 * j][1] + bias[c0 + 1]);
+        h[j][1] = silu_bf16x2(acc[2 * j][2] + bias[c0], acc[2 * j][3] + bias[c0 + 1]);
+        h[j][2] = silu_bf16x2(acc[2 * j + 1][0] + bias[c1], acc[2 * j + 1][1] + bias[c1 + 1]);
+        h[j][3] = silu_bf16x2(acc[2 * j + 1][2] + bias[c1], acc[2 * j + 1][3] + bias[c1 + 1]);
     }
 #pragma unroll
     for (int nt = 0; nt < kH / 8; ++nt)
@@ -166,10 +180,10 @@ __device__ __forceinline__ void mlp_tile(const __nv_bfloat16 (*xs)[kXPad], int r
 #pragma unroll
     for (int j = 0; j < kH / 16; ++j) {
         const int c0 = 16 * j + 2 * t, c1 = c0 + 8;
-        h[j][0] = pack_bf16(silu(acc[2 * j][0] + bias[kH + c0]), silu(acc[2 * j][1] + bias[kH + c0 + 1]));
-        h[j][1] = pack_bf16(silu(acc[2 * j][2] + bias[kH + c0]), silu(acc[2 * j][3] + bias[kH + c0 + 1]));
-        h[j][2] = pack_bf16(silu(acc[2 * j + 1][0] + bias[kH + c1]), silu(acc[2 * j + 1][1] + bias[kH + c1 + 1]));
-        h[j][3] = pack_bf16(silu(acc[2 * j + 1][2] + bias[kH + c1]), silu(acc[2 * j + 1][3] + bias[kH + c1 + 1]));
+        h[j][0] = silu_bf16x2(acc[2 * j][0] + bias[kH + c0], acc[2 * j][1] + bias[kH + c0 + 1]);
+        h[j][1] = silu_bf16x2(acc[2 * j][2] + bias[kH + c0], acc[2 * j][3] + bias[kH + c0 + 1]);
+        h[j][2] = silu_bf16x2(acc[2 * j + 1][0] + bias[kH + c1], acc[2 * j + 1][1] + bias[kH + c1 + 1]);
+        h[j][3] = silu_bf16x2(acc[2 * j + 1][2] + bias[kH + c1], acc[2 * j + 1][3] + bias[kH + c1 + 1]);
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) y[q] = 0.f;

@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(256) k_deposit_plan(const int* __restrict__ rs
 // (Summing equal corners across a warp's lanes first, with __match_any_sync and
 // __reduce_add_sync, made dense scenes slower, not faster: 0.27 against 0.18 ms
 // at 4M particles / 256^3.)
-template <int G>
+template <int G, bool SHARED>
 __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, const float4* __restrict__ pos,
                                                const int* __restrict__ perm, const int* __restrict__ row_start,
                                                float* __restrict__ rho_keep, float2* __restrict__ spec,
@@ -306,8 +306,8 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
     }
     __syncthreads();
     const int total = r_off[7];
-    const int f_lo = (int)((long long)total * slice / items);
-    const int f_hi = (int)((long long)total * (slice + 1) / items);
+    const int f_lo = SHARED ? (int)((long long)total * slice / items) : 0;
+    const int f_hi = SHARED ? (int)((long long)total * (slice + 1) / items) : total;
     // A weight q <= 2^32 is added as (q >> 16) into the high word and (q & 0xffff)
     // into the low word: with fewer than 2^16 particles in this share neither 32-bit
     // sum can overflow, so plain adds keep the 64-bit total exact. Larger shares
@@ -377,7 +377,7 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
     }
     __syncthreads();
     int sh = split16 ? 16 : 32;  // value of a cell: (hi << sh) + lo
-    if (items > 1) {
+    if constexpr (SHARED) {
         // a shared bundle: every CTA adds its rows into the fixed-point grid; the last
         // to arrive reads the complete sums back (and leaves the grid zero)
         unsigned long long* g = reinterpret_cast<unsigned long long*>(w.acc);
@@ -482,7 +482,6 @@ __global__ void __launch_bounds__(kDepositThreads, G >= 512 ? 3 : 2)
                          const float2* __restrict__ tw_g, DepositWork w) {
     using P = DepPlan<G>;
     extern __shared__ float2 sm[];
-    for (int i = threadIdx.x; i < G; i += kDepositThreads) sm[i] = tw_g[i];  // ordered by the first barrier
     const int* items = w.ints + P::kItems;
     const int* xpre = w.ints + P::kXpre;
     const int* cta_pre = w.ints + P::kCtaPre;
@@ -490,6 +489,8 @@ __global__ void __launch_bounds__(kDepositThreads, G >= 512 ? 3 : 2)
     const int X = (int)gridDim.x - P::NB;
     const bool first = (int)blockIdx.x >= X;  // a bundle's first share, then done
     const int extras = first ? 0 : cta_pre[P::NC];
+    if (!first && (int)blockIdx.x >= extras) return;  // no extra share for this CTA
+    for (int i = threadIdx.x; i < G; i += kDepositThreads) sm[i] = tw_g[i];  // ordered by a later barrier
     for (int e = first ? 0 : (int)blockIdx.x; first || e < extras; e += X) {
         int b, slice;
         if (first) {
@@ -506,8 +507,17 @@ __global__ void __launch_bounds__(kDepositThreads, G >= 512 ? 3 : 2)
             b = lo;
             slice = 1 + e - (cta_pre[lo >> 8] + xpre[lo]);
         }
-        deposit_bundle<G>(b, slice, items[b], pos, perm, row_start, rho_keep, spec, w, arrive,
-                          !first && e != (int)blockIdx.x);
+        // a bundle that one CTA covers whole takes the instantiation without the
+        // shared-bundle code: a path that may run costs registers and time even when
+        // it does not (0.513 against 0.479 ms at 16M / 512^3)
+        // (at 512^3; smaller grids, whose registers the two copies would spill, keep one)
+        const int nb = items[b];
+        if (G >= 512 && nb == 1)
+            deposit_bundle<G, false>(b, 0, 1, pos, perm, row_start, rho_keep, spec, w, arrive,
+                                     !first && e != (int)blockIdx.x);
+        else
+            deposit_bundle<G, true>(b, slice, nb, pos, perm, row_start, rho_keep, spec, w, arrive,
+                                    !first && e != (int)blockIdx.x);
         if (first) break;
     }
 }
