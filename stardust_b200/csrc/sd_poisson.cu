@@ -546,51 +546,6 @@ __device__ __forceinline__ void load_lines(float2* s, const float2* __restrict__
     __syncthreads();
 }
 
-// Polls of a bulk copy's barrier before a CTA gives up (far beyond any copy's time);
-// a CTA that gives up counts itself here, waits once more, and leaves its bricks as
-// they were (the solve's results are then wrong, which the checks of a caller see).
-constexpr int kBulkWaitPolls = 1 << 22;
-__device__ unsigned g_bulk_wait_timeouts = 0;
-
-// z-lines of CTA (bx, by): its bricks (bx, by, bz), bz = 0..NBZ-1, each 512 bytes of
-// global memory, land contiguously (brick bz at s + 64 bz): warp 0 issues one bulk
-// copy per brick on a barrier that counts the bytes, and every thread waits for it.
-template <int G>
-__device__ __forceinline__ bool load_lines_bulk(float2* s, const float2* __restrict__ spec, int bx, int by,
-                                                unsigned long long* bar) {
-    using T = Geo<G>;
-    constexpr int NB = T::NBZ;
-    constexpr unsigned kBrick = 64 * sizeof(float2);
-    if (threadIdx.x == 0) fft::mbar_init(bar, 1);
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        if (threadIdx.x == 0) fft::mbar_expect_tx(bar, NB * kBrick);
-        __syncwarp();
-        for (int b = threadIdx.x; b < NB; b += 32) fft::bulk_load(s + b * 64, spec + T::brick(bx, by, b), kBrick, bar);
-    }
-    if (fft::mbar_wait(bar, 0, kBulkWaitPolls)) return true;
-    if (threadIdx.x == 0) atomicAdd(&g_bulk_wait_timeouts, 1u);
-    fft::mbar_wait(bar, 0, kBulkWaitPolls);  // the copies may still be writing
-    return false;
-}
-
-// The transformed z-lines back to their bricks: every thread fences its shared-memory
-// writes for the bulk copies, then warp 0 issues one bulk store per brick and waits
-// until they have read the buffer.
-template <int G>
-__device__ __forceinline__ void store_lines_bulk(const float2* s, float2* __restrict__ spec, int bx, int by) {
-    using T = Geo<G>;
-    constexpr int NB = T::NBZ;
-    constexpr unsigned kBrick = 64 * sizeof(float2);
-    fft::fence_async_shared();
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        for (int b = threadIdx.x; b < NB; b += 32) fft::bulk_store(spec + T::brick(bx, by, b), s + b * 64, kBrick);
-        fft::bulk_commit();
-        fft::bulk_wait_read();
-    }
-}
-
 template <int G, int DIR>
 __device__ __forceinline__ void store_lines(const float2* s, float2* __restrict__ spec, int bx, int b1) {
     using T = Geo<G>;
@@ -653,12 +608,10 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_c(float2* __restrict__ spe
         line_g[l] = (kx <= H) ? -scale * (gexp_g[kx] * gexp_g[abs(kyf)]) : 0.f;  // the global table: no barrier yet
         line_k2[l] = kx * kx + kyf * kyf;
     }
-    __shared__ unsigned long long bar;
-    if (!load_lines_bulk<G>(s, spec, bx, by, &bar)) return;
-    __syncthreads();  // the twiddle, exponent and per-line tables are in place
+    load_lines<G, 2>(s, spec, bx, by);  // ends with a barrier
     if (MODE == 1) {
         fft::lines16<G, kFftThreads, 1, false>(s, tw);
-        store_lines_bulk<G>(s, spec, bx, by);
+        store_lines<G, 2>(s, spec, bx, by);
         return;
     }
     // forward, Green's function, inverse; the multiply happens in registers between
@@ -679,7 +632,7 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_c(float2* __restrict__ spe
         return make_float2(x.x * m, x.y * m);
     };
     fft::convolve16<G, kFftThreads, 1>(s, tw, green);
-    store_lines_bulk<G>(s, spec, bx, by);
+    store_lines<G, 2>(s, spec, bx, by);
 }
 
 // Real part of a forward spectrum (bricked) into table[|ky|][kx][|kz|], ky, kz, kx <= H.
