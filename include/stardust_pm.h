@@ -103,8 +103,11 @@ typedef struct sd_config {
     float pressure_k;            /* SimConfig::pressureK (Sim.h:320), default 0.45 */
     int32_t cooling_enabled;     /* SimConfig::coolingEnabled (Sim.h:327) */
     float cooling_rate;          /* SimConfig::coolingRate (Sim.h:345), default 0.08 */
-    int32_t full_sort;           /* 1: always the full radix sort; 0: a step after a sorted step merges
-                                    the few keys that changed into the rest (tiled order, periodic) */
+    int32_t full_sort;           /* the sort of a step after a sorted step (tiled order, periodic):
+                                    1 always the full radix sort; 0 (default) a merge of the keys that
+                                    changed into the rest for 2^22 particles or more while at most 10 %
+                                    change, else the full sort; -1 the merge whenever possible.
+                                    Every choice gives the same permutation. */
     int32_t reserved[7];
 } sd_config;
 
@@ -278,10 +281,11 @@ int sd_particle_capacity(const sd_sim* sim);                        /* slots all
 int sd_active_count(const sd_sim* sim);                             /* Sim::activeCount */
 int sd_step_count(const sd_sim* sim);
 /* The merge sort (tiled order, periodic; no reference counterpart) measures the
- * share of particles whose row key changed since the last sorted step. Above 10 %
- * the steps run the full radix sort instead (the same permutation), with one
- * probing merge every 64 steps. sd_changed_fraction: the last measured share
- * (-1 before the first merge); sd_merge_sorting: 1 while merges are chosen. */
+ * share of particles whose row key changed since the last sorted step. With
+ * full_sort = 0, above 10 % (or below 2^22 particles) the steps run the full radix
+ * sort instead (the same permutation), with one probing merge every 64 steps.
+ * sd_changed_fraction: the last measured share (-1 before the first merge);
+ * sd_merge_sorting: 1 while merges are chosen. */
 double sd_changed_fraction(const sd_sim* sim);
 int sd_merge_sorting(const sd_sim* sim);
 double sd_measure_total_grid_mass(sd_sim* sim);                     /* Sim.cu:4890-4906 */

@@ -261,6 +261,7 @@ int validate_config(const sd_config* c) {
     if (c->boundary != SD_BOUNDARY_PERIODIC && c->boundary != SD_BOUNDARY_ISOLATED)
         return fail(SD_E_ARG, "config: bad boundary %d", c->boundary);
     if (c->order < SD_ORDER_ROWMAJOR || c->order > SD_ORDER_TILED) return fail(SD_E_ARG, "config: bad order");
+    if (c->full_sort < -1 || c->full_sort > 1) return fail(SD_E_ARG, "config: full_sort must be -1, 0 or 1");
     if (c->integrator != SD_INT_KD && c->integrator != SD_INT_KDK) return fail(SD_E_ARG, "config: bad integrator");
     if (c->units != SD_UNITS_REFERENCE && c->units != SD_UNITS_NEWTON) return fail(SD_E_ARG, "config: bad units");
     if (c->preset != SD_PRESET_FILAMENT && c->preset != SD_PRESET_EMPTY) return fail(SD_E_ARG, "config: bad preset");
@@ -295,23 +296,30 @@ void invalidate_keys(sd_sim* s) {
 }
 
 bool incr_possible(const sd_sim* s) {
-    return s->allow_incr && !s->cfg.full_sort && s->cfg.order == SD_ORDER_TILED && !isolated(s);
+    return s->allow_incr && s->cfg.full_sort != 1 && s->cfg.order == SD_ORDER_TILED && !isolated(s);
 }
 
 // Above this share of changed keys the full radix sort is cheaper than the merge
 // (4M particles on 256^3 with a third of the keys changing: merge 0.146 ms, full
 // sort with its row table 0.093 ms; 16M on 512^3 with 0.8 % changing: merge
-// 0.12 ms, full sort 0.23 ms).
+// 0.12 ms, full sort 0.23 ms). Below kMergeMinParticles the merge's dozen launches
+// cost more than a full sort whatever changes (262,144 particles on 64^3 with 9 %
+// changing: merge 0.107 ms, full sort and row table 0.05 ms).
 constexpr double kMergeMaxFraction = 0.10;
 constexpr int kMergeProbe = 64;
+constexpr int kMergeMinParticles = 1 << 22;
 
 // The next sorted step leaves change bits for a merge (otherwise first-pass counts).
-bool merge_next(const sd_sim* s) { return s->rs_base && incr_possible(s) && !s->merge_off; }
+bool merge_next(const sd_sim* s) {
+    if (!s->rs_base || !incr_possible(s)) return false;
+    return s->cfg.full_sort == -1 || (!s->merge_off && s->N >= kMergeMinParticles);
+}
 
 // Read the share of keys the last merge found changed (written to pinned memory
 // by the device, possibly a step or more behind) and choose merge or full sort.
 void update_merge_policy(sd_sim* s) {
     if (!s->rs_base || !s->chg_host) return;
+    if (s->cfg.full_sort == -1) s->merge_off = false;  // merges asked for whatever changes
     const int c = *reinterpret_cast<volatile int*>(s->chg_host);
     if (c >= 0 && s->N > 0) s->chg_frac = (double)c / (double)s->N;
     if (!s->merge_off) {
@@ -1538,7 +1546,7 @@ int sd_grid_size(const sd_sim* s) { return s ? s->G : 0; }
 int sd_particle_count(const sd_sim* s) { return s ? s->N : 0; }
 int sd_particle_capacity(const sd_sim* s) { return s ? s->capacity : 0; }
 double sd_changed_fraction(const sd_sim* s) { return s ? s->chg_frac : -1.0; }
-int sd_merge_sorting(const sd_sim* s) { return (s && s->rs_base && incr_possible(s) && !s->merge_off) ? 1 : 0; }
+int sd_merge_sorting(const sd_sim* s) { return (s && merge_next(s)) ? 1 : 0; }
 int sd_active_count(const sd_sim* s) { return s ? s->active : 0; }
 int sd_step_count(const sd_sim* s) { return s ? s->step_count : 0; }
 

@@ -51,7 +51,7 @@ class SimConfig:
     pressure_k: float = 0.45             # Sim.h:320
     cooling_enabled: int = 0             # Sim.h:327
     cooling_rate: float = 0.08           # Sim.h:345
-    full_sort: int = 0                   # 1: no merge sort of the changed keys
+    full_sort: int = 0                   # 1: always the full sort; 0: merge when worthwhile; -1: merge always
 
     def to_c(self) -> L.SdConfig:
         c = L.SdConfig()
