@@ -47,6 +47,129 @@ struct Geo {
     }
 };
 
+// ---- pass A's x transform at G = 512: one warp per line ---------------------------
+// A row of 512 reals is packed as 256 complex z[m] = x[2m] + i x[2m+1]; lane t
+// holds z[t + 32k], k = 0..7. The 256-point transform is factored 8 x 32
+// (m = t + 32k, f = f1 + 8 f2): a radix-8 DFT over k in registers and the twiddle
+// W256^(t f1); then the 32-point DFTs over t, factored 8 x 4 (t = j + 4i,
+// f2 = g1 + 8 g2) after a transpose through the warp's own shared scratch: lane
+// (f1, j) takes a radix-8 DFT over i and the twiddle W32^(j g1); a second
+// transpose hands lane L the output groups gA = L and gB = 64 - L (lane 0: 0 and
+// 32), each finished by a radix-4 DFT over j into Z[g + 64 g2]. Both members of
+// every pair (k, H - k) of the real-to-complex unpacking then sit in one lane.
+// The bins go to a brick-ordered staging buffer, from which the CTA stores whole
+// 512-byte bricks (a warp storing its own line would touch 65 bricks per line).
+// Only __syncwarp orders the scratch; XOR swizzles keep every 8-byte access of the
+// scratch and the staging buffer at two wavefronts.
+namespace xl {
+constexpr int kTw2 = 3 * 32 + 3 * 4;   // float2 entries of the two twiddle tables
+constexpr int kStage = 16 * 4 * 65;     // float2: 65 bricks of 16 lines x 4 bins
+
+// Twiddle tables, lane-contiguous so every load is conflict-free: tw[p*32 + t] =
+// W256^(t 2^p) and then tw[96 + p*4 + j] = W32^(j 2^p), p = 0..2, copied from the
+// table tw_g[m] = W512^m. Other powers are products of at most two of these.
+__device__ __forceinline__ void fill_twiddles(float2* tw2, const float2* __restrict__ tw_g) {
+    for (int e = threadIdx.x; e < kTw2; e += blockDim.x)
+        tw2[e] = e < 96 ? tw_g[(2 * (e & 31)) << (e >> 5)] : tw_g[(16 * ((e - 96) & 3)) << ((e - 96) >> 2)];
+}
+
+// v[q] *= w^q for q = 1..7, given w, w^2, w^4
+__device__ __forceinline__ void twiddle8(float2 (&v)[8], float2 w1, float2 w2, float2 w4) {
+    const float2 w3 = fft::cmul(w1, w2);
+    v[1] = fft::cmul(v[1], w1);
+    v[2] = fft::cmul(v[2], w2);
+    v[3] = fft::cmul(v[3], w3);
+    v[4] = fft::cmul(v[4], w4);
+    v[5] = fft::cmul(v[5], fft::cmul(w1, w4));
+    v[6] = fft::cmul(v[6], fft::cmul(w2, w4));
+    v[7] = fft::cmul(v[7], fft::cmul(w3, w4));
+}
+
+// Staging position of bin kx of line l = z_l*4 + y_l: brick kx/4, element
+// z_l*16 + y_l*4 + kx%4 (the spectrum's brick layout), bits 2-3 of the element
+// XORed with the brick's low bits. 16-byte pairs (kx even, kx + 1) stay adjacent.
+__device__ __forceinline__ int stage_pos(int kx, int l) {
+    const int b = kx >> 2;
+    return b * 64 + ((((l >> 2) << 4) + ((l & 3) << 2) + (kx & 3)) ^ ((b & 3) << 2));
+}
+
+// One pair of the unpacking: from Z[k] and Z[H-k], X[k] = E + W512^k O and
+// X[H-k] = conj E + W512^(H-k) conj O with E = (Z[k] + conj Z[H-k]) / 2,
+// O = (Z[k] - conj Z[H-k]) / (2i); W512^(H-k) = -conj W512^k.
+__device__ __forceinline__ void unpack_pair(float2 zk, float2 zc, int k, const float2* tw, float2* st, int l) {
+    constexpr int H = 256;
+    const float er = 0.5f * (zk.x + zc.x), ei = 0.5f * (zk.y - zc.y);
+    const float orr = 0.5f * (zk.y + zc.y), oi = -0.5f * (zk.x - zc.x);
+    const float2 w = tw[k];
+    st[stage_pos(k, l)] = make_float2(er + (w.x * orr - w.y * oi), ei + (w.x * oi + w.y * orr));
+    if (2 * k != H)
+        st[stage_pos(H - k, l)] = make_float2(er + (w.y * oi - w.x * orr), -ei + (w.y * orr + w.x * oi));
+}
+
+// z: this lane's inputs z[t + 32k] (destroyed); sc: the warp's 256-float2 scratch,
+// free on entry and on return; tw: W512^m in shared memory; st: the staging
+// buffer, which receives bins 0..259 of line l (257..259 zero).
+__device__ __forceinline__ void r2c512(float2 (&z)[8], float2* sc, const float2* tw, const float2* tw2, float2* st,
+                                       int l) {
+    const int lane = threadIdx.x & 31;
+    fft::dft<8, false>(z);
+    twiddle8(z, tw2[lane], tw2[32 + lane], tw2[64 + lane]);  // W256^(t f1)
+    __syncwarp();
+#pragma unroll
+    for (int f1 = 0; f1 < 8; ++f1) sc[f1 * 32 + (lane ^ (4 * (f1 & 3)))] = z[f1];
+    __syncwarp();
+    const int f1 = lane >> 2, j = lane & 3;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) z[i] = sc[f1 * 32 + ((j + 4 * i) ^ (4 * (f1 & 3)))];
+    fft::dft<8, false>(z);
+    twiddle8(z, tw2[96 + j], tw2[100 + j], tw2[104 + j]);  // W32^(j g1)
+    __syncwarp();
+#pragma unroll
+    for (int g1 = 0; g1 < 8; ++g1) {
+        const int g = f1 + 8 * g1;
+        sc[4 * g + (j ^ ((g >> 2) & 3))] = z[g1];
+    }
+    __syncwarp();
+    const int ga = lane, gb = lane ? 64 - lane : 32;
+    float2 a[4], b[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        a[q] = sc[4 * ga + (q ^ ((ga >> 2) & 3))];
+        b[q] = sc[4 * gb + (q ^ ((gb >> 2) & 3))];
+    }
+    __syncwarp();  // the scratch is free again
+    fft::dft<4, false>(a);  // a[g2] = Z[ga + 64 g2]
+    fft::dft<4, false>(b);  // b[g2] = Z[gb + 64 g2]
+    if (lane) {
+        unpack_pair(a[0], b[3], lane, tw, st, l);
+        unpack_pair(a[1], b[2], 64 + lane, tw, st, l);
+        unpack_pair(b[1], a[2], 128 - lane, tw, st, l);
+        unpack_pair(b[0], a[3], 64 - lane, tw, st, l);
+    } else {
+        st[stage_pos(0, l)] = make_float2(a[0].x + a[0].y, 0.f);
+        st[stage_pos(256, l)] = make_float2(a[0].x - a[0].y, 0.f);
+        st[stage_pos(257, l)] = make_float2(0.f, 0.f);
+        st[stage_pos(258, l)] = make_float2(0.f, 0.f);
+        st[stage_pos(259, l)] = make_float2(0.f, 0.f);
+        unpack_pair(a[1], a[3], 64, tw, st, l);
+        unpack_pair(a[2], a[2], 128, tw, st, l);
+        unpack_pair(b[0], b[3], 32, tw, st, l);
+        unpack_pair(b[1], b[2], 96, tw, st, l);
+    }
+}
+
+// The staged bricks (kx/4 = 0..64) of bundle (by, bz) to the spectrum, 16 bytes
+// per thread: each warp instruction writes one whole brick.
+template <int G>
+__device__ __forceinline__ void store_bricks(const float2* st, float2* __restrict__ spec, int by, int bz) {
+    for (int u = threadIdx.x; u < 65 * 32; u += blockDim.x) {
+        const int b = u >> 5, c = u & 31;
+        const float4 v = *reinterpret_cast<const float4*>(st + b * 64 + ((2 * c) ^ ((b & 3) << 2)));
+        *reinterpret_cast<float4*>(spec + Geo<G>::brick(b, by, bz) + 2 * c) = v;
+    }
+}
+}  // namespace xl
+
 // ---- pass A: rows (y = 4by + y_l, z = 4bz + z_l) -> kx bins -----------------
 // line l = z_l*4 + y_l; positions m < H hold z[m] = x[2m] + i x[2m+1].
 // SRC 0: float grid, 1: int64 fixed-point grid (zeroed after reading). The source
@@ -65,6 +188,42 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_a(const float* __restrict_
     float2* s = sm + G;
     const int by = blockIdx.x, bz = blockIdx.y;
     for (int i = threadIdx.x; i < G; i += kFftThreads) tw[i] = tw_g[i];
+    if constexpr (G == 512) {
+        // one warp per line, two lines per warp (the fused deposit's transform);
+        // shared: tw | twiddle tables | 8 warp scratches | brick staging
+        float2* tw2 = sm + G;
+        xl::fill_twiddles(tw2, tw_g);
+        __syncthreads();
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        float2* sc = tw2 + xl::kTw2 + warp * 256;
+        float2* st = tw2 + xl::kTw2 + (kFftThreads / 32) * 256;
+#pragma unroll 1
+        for (int l = warp; l < 16; l += kFftThreads / 32) {
+            const int y = by * 4 + (l & 3), z = bz * 4 + (l >> 2);
+            const size_t row = ((size_t)z * src_g + y) * src_g;
+            const bool in_rows = y < src_g && z < src_g;
+            float2 v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int m = lane + 32 * k;
+                v[k] = make_float2(0.f, 0.f);
+                if (in_rows && 2 * m < src_g) {
+                    if (SRC == 0) {
+                        v[k] = *reinterpret_cast<const float2*>(rho + row + 2 * m);
+                    } else {
+                        const longlong2 q = *reinterpret_cast<const longlong2*>(acc + row + 2 * m);
+                        *reinterpret_cast<longlong2*>(acc + row + 2 * m) = make_longlong2(0, 0);
+                        v[k] = make_float2(fixed_to_float(q.x), fixed_to_float(q.y));
+                    }
+                    if (rho_keep) *reinterpret_cast<float2*>(rho_keep + row + 2 * m) = v[k];
+                }
+            }
+            xl::r2c512(v, sc, tw, tw2, st, l);
+        }
+        __syncthreads();
+        xl::store_bricks<G>(st, spec, by, bz);
+        return;
+    }
 
     float4 v[PER];
 #pragma unroll
@@ -407,6 +566,34 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
         if (threadIdx.x == 0) arrive[b] = 0u;
         __syncthreads();
     }
+    if constexpr (G == 512) {
+        // warp l converts row l and transforms it (the generic pass A's routine, so
+        // both deposit paths give the same bits); its lo row is then its scratch
+        static_assert(NT == 16 * 32, "one warp per line");
+        const int l = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const unsigned* lo = acc_lo + l * RS;
+        const unsigned* hi = acc_hi + l * RS;
+        const size_t grow = ((size_t)(bz * 4 + (l >> 2)) * G + by * 4 + (l & 3)) * G;
+        float2 v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int m = lane + 32 * k;
+            const uint2 lw = *reinterpret_cast<const uint2*>(lo + 2 * m);
+            const uint2 hw = *reinterpret_cast<const uint2*>(hi + 2 * m);
+            v[k] = make_float2(fixed_to_float((long long)(((unsigned long long)hw.x << sh) + lw.x)),
+                               fixed_to_float((long long)(((unsigned long long)hw.y << sh) + lw.y)));
+            if (rho_keep) *reinterpret_cast<float2*>(rho_keep + grow + 2 * m) = v[k];
+        }
+        // every row is in registers: the sums' storage becomes 16 warp scratches
+        // (256 float2 each) and the brick staging (16 * 256 + kStage = 16 * RS float2)
+        static_assert(16 * 256 + xl::kStage == 16 * RS, "scratch and staging fill the sums");
+        __syncthreads();
+        float2* R = reinterpret_cast<float2*>(acc_lo);
+        xl::r2c512(v, R + l * 256, tw, sm + G + 16 * RS, R + 16 * 256, l);
+        __syncthreads();
+        xl::store_bricks<G>(R + 16 * 256, spec, by, bz);
+        return;
+    }
     // int64 rows -> complex positions z[m] = x[2m] + i x[2m+1] on line l = z_l*4 + y_l,
     // staged through registers because the line buffer overlays the sums.
     constexpr int CITEMS = 16 * (H / 2);
@@ -491,6 +678,7 @@ __global__ void __launch_bounds__(kDepositThreads, G >= 512 ? 3 : 2)
     const int extras = first ? 0 : cta_pre[P::NC];
     if (!first && (int)blockIdx.x >= extras) return;  // no extra share for this CTA
     for (int i = threadIdx.x; i < G; i += kDepositThreads) sm[i] = tw_g[i];  // ordered by a later barrier
+    if constexpr (G == 512) xl::fill_twiddles(sm + G + 16 * (G + 4), tw_g);  // the twiddle tables, after the sums
     for (int e = first ? 0 : (int)blockIdx.x; first || e < extras; e += X) {
         int b, slice;
         if (first) {
@@ -734,13 +922,19 @@ template <int G>
 struct Launcher {
     using T = Geo<G>;
     static size_t smem_ae() { return sizeof(float2) * ((size_t)G + 16 * (size_t)T::PX); }
+    // pass A from a grid: at G = 512 the twiddle tables, 8 warp scratches and the brick staging
+    static size_t smem_a() {
+        return G == 512 ? sizeof(float2) * ((size_t)G + xl::kTw2 + 8 * 256 + xl::kStage) : smem_ae();
+    }
     static size_t smem_bd() { return sizeof(float2) * ((size_t)G + 16 * (size_t)G); }
     static size_t smem_c() { return sizeof(float2) * ((size_t)G + (T::H + 2) / 2 + 1 + 16 * (size_t)G); }
-    // the line buffer (16 * PX float2) overlays the 32-bit sum words (2 * 16 * (G + 4))
-    // the line buffer (16 * PX float2) overlays the 32-bit sum words (2 * 16 * (G + 4))
+    // the line buffer (16 * PX float2) overlays the 32-bit sum words (2 * 16 * (G + 4));
+    // at G = 512 the warp-per-line transform's twiddle tables follow the sums
     static size_t smem_bal() {
         const size_t lines = sizeof(float2) * 16 * (size_t)T::PX, sums = 2 * sizeof(unsigned) * 16 * (size_t)(G + 4);
-        return sizeof(float2) * (size_t)G + (lines > sums ? lines : sums);
+        const size_t xtab = G == 512 ? sizeof(float2) * xl::kTw2 : 0;
+        static_assert(G != 512 || 16 * (G + 4) >= 16 * T::PX, "the sums are the larger overlay");
+        return sizeof(float2) * (size_t)G + (lines > sums ? lines : sums) + xtab;
     }
     // CTAs that take the extra shares of heavy bundles
     static int extra_ctas() {
@@ -762,8 +956,8 @@ struct Launcher {
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_e<G>, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a_deposit_bal<G>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                            carve));
-        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a<G, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ae()));
-        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a<G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ae()));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a<G, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a()));
+        rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_a<G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a()));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_y<G, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem_bd()));
         rc |= SD_CUDA(cudaFuncSetAttribute(k_pass_y<G, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -789,10 +983,10 @@ struct Launcher {
             k_pass_a_deposit_bal<G><<<extra_ctas() + DepPlan<G>::NB, kDepositThreads, smem_bal(), s>>>(
                 pos, perm, row_start, keep, spec, p.tw, *dw);
         } else if (acc)
-            k_pass_a<G, 1><<<grid_rows, kFftThreads, smem_ae(), s>>>(nullptr, const_cast<long long*>(acc), keep, spec,
+            k_pass_a<G, 1><<<grid_rows, kFftThreads, smem_a(), s>>>(nullptr, const_cast<long long*>(acc), keep, spec,
                                                                      p.tw, src_g);
         else
-            k_pass_a<G, 0><<<grid_rows, kFftThreads, smem_ae(), s>>>(rho, nullptr, keep, spec, p.tw, src_g);
+            k_pass_a<G, 0><<<grid_rows, kFftThreads, smem_a(), s>>>(rho, nullptr, keep, spec, p.tw, src_g);
         SD_LAUNCHED(s);
         if (ev) cudaEventRecord(ev[0], s);
         k_pass_y<G, false><<<grid_y, kFftThreads, smem_bd(), s>>>(spec, p.tw);

@@ -1323,12 +1323,15 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
         }
         const int phase = hydro_on(s) ? (s->step_count & 1) : 0;
         const bool incr_now = s->incr_ready && s->keys_valid;  // the first captured step merge-sorts
+        // a full sort with change bits pending records their clearing (the merge consumes them)
+        const bool dirty_now = !incr_now && s->chg_dirty;
         // A captured graph covers two steps so the pos/pos2 ping-pong returns to the
         // same buffers; it is rebuilt when dt changes, the particles sit in the other
         // buffer of the pair, the cooling phase moved, or its first step would sort
-        // differently (a merge needs the last step's change bits).
+        // differently (a merge needs the last step's change bits; stale bits must be
+        // cleared before the gather marks new ones).
         if (!s->graph || s->graph_dt != dt || s->graph_pos != s->pos || s->graph_phase != phase ||
-            s->graph_incr != incr_now || s->graph_merge_off != s->merge_off) {
+            s->graph_incr != incr_now || s->graph_dirty != dirty_now || s->graph_merge_off != s->merge_off) {
             if (s->graph) cudaGraphExecDestroy(s->graph);
             s->graph = nullptr;
             cudaGraph_t graph = nullptr;
@@ -1371,6 +1374,7 @@ int sd_steps(sd_sim* s, float dt, int nsteps) {
             s->graph_pos = s->pos;
             s->graph_phase = phase;
             s->graph_incr = incr_now;
+            s->graph_dirty = dirty_now;
             s->graph_merge_off = s->merge_off;
         }
         if (SD_CUDA(cudaGraphLaunch(s->graph, s->stream))) return sim_error(s, SD_E_CUDA);

@@ -39,6 +39,7 @@ struct sd_sim {
     sd::HydroGrids hydro;        // pressure / cooling grids, allocated while either is on
     int graph_phase = 0;         // step count parity the captured graph was made at (hydro)
     bool graph_incr = false;     // whether the captured graph's first step merge-sorts
+    bool graph_dirty = false;    // whether it clears change bits left by an unmerged gather first
     double* partials = nullptr;  // gather / energy / reduction partials
     size_t partials_count = 0;
     double* mom = nullptr;       // 8 doubles: momentum sums of the last step, energy results

@@ -197,7 +197,8 @@ def test_kernel_launches_counted(cuda):
         assert Sim.kernel_launches() - before >= 10
 
 
-@pytest.mark.parametrize("G,n,clustered", [(16, 30_000, True), (64, 262_144, True), (128, 400_000, False)])
+@pytest.mark.parametrize("G,n,clustered", [(16, 30_000, True), (64, 262_144, True), (128, 400_000, False),
+                                         (512, 2_000_000, True)])
 def test_fused_tiled_deposit_equals_generic_path(cuda, G, n, clustered):
     """The tiled order deposits inside the first FFT pass; the row-major order uses
     int64 atomics on a grid. Both are fixed-point, so after sorting the same
