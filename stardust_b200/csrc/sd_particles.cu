@@ -34,6 +34,21 @@ constexpr int kGatherThreads = 256;
 constexpr int kGatherMaxBlocks = 4096;
 constexpr int kKeysPlain = 0, kKeysCounts = 1, kKeysChanged = 2;  // the gather's KEYS modes
 
+// 16-byte global -> shared copy that does not hold registers while in flight
+// (L2 only); copy groups and the wait until at most N of this thread's most
+// recent groups are pending.
+__device__ __forceinline__ void cp_async16(float4* smem, const float4* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+// records (pos, vel) of the gather's next particles in flight ahead of the one in use
+constexpr int kAhead = 1;
+
 __global__ void __launch_bounds__(256) k_deposit_fixed(const float4* __restrict__ pos, int n, int G,
                                                        unsigned long long* __restrict__ acc, int periodic) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -256,19 +271,53 @@ __global__ void __launch_bounds__(kGatherThreads, 3) k_gather_kick_drift(
     // thread's own shared-memory slot: held in registers they crowd out the stencil's
     // loads at the kernel's register limit. The summation order is the same.
     __shared__ double acc[6][kGatherThreads];
+    // Software pipeline over the grid-stride loop: the records (pos, vel) of this
+    // thread's next kAhead particles are in flight into its own shared-memory slots
+    // (cp.async, one copy group per particle), and the permutation index of the
+    // particle after them is loaded, so the dependent perm -> record loads overlap
+    // the stencils of the particles before them instead of preceding each one.
+    // kAhead + 1 slots rotate; each thread reads and fills only its own, so no
+    // barrier is involved.
+    __shared__ float4 rec[kAhead + 1][2][kGatherThreads];
     const int me = threadIdx.x;
 #pragma unroll
     for (int q = 0; q < 6; ++q) acc[q][me] = 0.0;
     const unsigned cmask = (1u << count_bits) - 1u;
     const float mx = mean_vel ? mean_vel[0] : 0.f, my = mean_vel ? mean_vel[1] : 0.f,
                 mz = mean_vel ? mean_vel[2] : 0.f;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int stride = gridDim.x * blockDim.x;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    // prologue: the records of this thread's first kAhead particles, one copy group
+    // each, and the permutation index of the particle after them
+#pragma unroll
+    for (int q = 0; q < kAhead; ++q) {
+        const int iq = i + q * stride;
+        if (iq < n) {
+            const int jq = perm ? perm[iq] : iq;
+            cp_async16(&rec[q][0][me], pos_in + jq);
+            cp_async16(&rec[q][1][me], vel_in + jq);
+        }
+        cp_async_commit();
+    }
+    int jn = 0;
+    if (i + kAhead * stride < n) jn = perm ? perm[i + kAhead * stride] : i + kAhead * stride;
+    for (int slot = 0; i < n; i += stride, slot = (slot == kAhead) ? 0 : slot + 1) {
         uint32_t key = 0u;      // the order key written for output i (0: empty or lost)
         uint32_t key_old = 0u;  // the key of the step-start position (the one output i was sorted by)
+        cp_async_wait_group<kAhead - 1>();  // this thread's copies of particle i
+        float4 p = rec[slot][0][me];
+        float4 v = rec[slot][1][me];
+        {
+            const int ia = i + kAhead * stride;  // the particle whose record goes in flight now
+            const int sa = (slot == 0) ? kAhead : slot - 1;
+            if (ia < n) {
+                cp_async16(&rec[sa][0][me], pos_in + jn);
+                cp_async16(&rec[sa][1][me], vel_in + jn);
+                if (ia + stride < n) jn = perm ? perm[ia + stride] : ia + stride;
+            }
+            cp_async_commit();
+        }
         do {
-            const int j = perm ? perm[i] : i;
-            float4 p = pos_in[j];
-            float4 v = vel_in[j];
             if (p.x < 0.f) {
                 if (perm) {
                     pos_out[i] = p;
