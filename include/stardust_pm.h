@@ -385,9 +385,14 @@ int sd_mlp_param_count(void);
 /* features (bf16[n][32]) of pos[perm[i]] (perm may be NULL) from the density rho[G^3] */
 int sd_mlp_features(const float* pos, const int32_t* perm, int n, const float* rho, int grid_size, float inv_mean,
                     void* features_bf16, void* stream);
-/* residual accelerations float4[n] (w = 0; empty slots get 0) */
+/* residual accelerations float4[n] (w = 0; empty slots get 0). Runs on the
+ * 5th-generation tensor cores (tcgen05.mma, accumulators in tensor memory). */
 int sd_mlp_infer(const float* params, const float* pos, const int32_t* perm, int n, const float* rho,
                  int grid_size, float inv_mean, float out_scale, float* out, void* stream);
+/* Bounded waits of the inference on tensor-core completion that gave up since the
+ * library was loaded on the current device (0 unless the hardware stalled; the
+ * affected outputs are NaN). Synchronises the device. */
+int sd_mlp_wait_timeouts(void);
 /* gradient (FP32 [params]) of the mean squared error over rows and the 3 outputs
  * of one batch (rows a multiple of 16); *sse = sum of squared errors (device) */
 size_t sd_mlp_train_workspace_bytes(int rows);

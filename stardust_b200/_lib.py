@@ -169,6 +169,7 @@ SIGNATURES = [
     ("sd_mlp_param_count", _I, []),
     ("sd_mlp_features", _I, [_P, _P, _I, _P, _I, _F, _P, _P]),
     ("sd_mlp_infer", _I, [_P, _P, _P, _I, _P, _I, _F, _F, _P, _P]),
+    ("sd_mlp_wait_timeouts", _I, []),
     ("sd_mlp_train_workspace_bytes", _S, [_I]),
     ("sd_mlp_loss_grad", _I, [_P, _P, _P, _I, _P, _P, _P, _S, _P]),
     ("sd_mlp_adam", _I, [_P, _P, _P, _P, _I, _F, _F, _F, _F, _P]),

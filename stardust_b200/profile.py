@@ -2,6 +2,11 @@
 
     python -m stardust_b200.profile --workload cosmic_web_512 --steps 2
     python -m stardust_b200.profile --stage poisson --grid 512
+    python -m stardust_b200.profile --stage mlp --steps 3
+
+--stage mlp runs the learned correction's inference (sd_mlp_infer) on the
+learned configuration's scene: 2,097,152 particles (Zel'dovich field, 128^3
+lattice, seed 1) on a 128^3 grid, random weights.
 
 Steps run eagerly (no CUDA graph) so each kernel appears as its own launch.
 Prints per-phase device times of the last step.
@@ -20,7 +25,7 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="cosmic_web_512")
     ap.add_argument("--steps", type=int, default=2)
-    ap.add_argument("--stage", choices=["step", "poisson"], default="step")
+    ap.add_argument("--stage", choices=["step", "poisson", "mlp"], default="step")
     ap.add_argument("--grid", type=int, default=512)
     ap.add_argument("--order", type=int, default=2)
     a = ap.parse_args(argv)
@@ -43,6 +48,23 @@ def main(argv=None) -> int:
                                    ws.numel(), None), "sd_poisson")
         torch.cuda.synchronize()
         print(json.dumps({"stage": "poisson", "grid": G}))
+        return 0
+
+    if a.stage == "mlp":
+        pos, _ = scenes.zeldovich(128, 1)
+        n, G = len(pos), 128
+        rng = np.random.default_rng(0)
+        rho = torch.from_numpy(rng.random(G ** 3, dtype=np.float32) * 3).cuda()
+        params = torch.from_numpy((rng.standard_normal(int(L.lib().sd_mlp_param_count())) * 0.2).astype(np.float32)).cuda()
+        pd = torch.from_numpy(pos).cuda()
+        out = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+        for _ in range(max(1, a.steps)):
+            L.check(L.lib().sd_mlp_infer(params.data_ptr(), pd.data_ptr(), None, n, rho.data_ptr(), G,
+                                         ctypes.c_float(1.0), ctypes.c_float(1.0), out.data_ptr(), None),
+                    "sd_mlp_infer")
+        torch.cuda.synchronize()
+        print(json.dumps({"stage": "mlp", "particles": n, "grid": G,
+                          "wait_timeouts": int(L.lib().sd_mlp_wait_timeouts())}))
         return 0
 
     if a.workload == "cosmic_web_512":

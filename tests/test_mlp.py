@@ -59,8 +59,9 @@ def test_gpu_features_match_oracle(cuda, lib, oracle):
 
 
 @pytest.mark.gpu
-def test_gpu_infer_matches_oracle(cuda, lib, oracle):
-    G, n = 32, 3001
+@pytest.mark.parametrize("G,n", [(32, 3001), (64, 300_001)])
+def test_gpu_infer_matches_oracle(cuda, lib, oracle, G, n):
+    # 300,001 particles: 2,344 tiles of 128, more than one per CTA of the tensor-core kernel
     pos, _ = random_particles(n, 5, clustered=True)
     rho = oracle.density_fixed(pos, G)
     inv_mean = G ** 3 / n
@@ -76,6 +77,7 @@ def test_gpu_infer_matches_oracle(cuda, lib, oracle):
     err = np.abs(got[:, :3] - ref).max() / np.abs(ref).max()
     assert err < 2e-2, err
     assert np.all(got[:, 3] == 0)
+    assert lib.sd_mlp_wait_timeouts() == 0
 
 
 @pytest.mark.gpu
