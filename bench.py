@@ -424,7 +424,9 @@ def run_ensemble(rank, world, steps: int = 100, warmup: int = 3, dt: float = 1e-
             "scenes": len(members), "particles": int(n_total),
             "grids": {str(g): sum(1 for m in members if m["grid"] == g) for g in (32, 64, 128)},
             "graph_launches_per_step": 1, "kernels_per_graph_rank0": kernels,
-            "autotune": {"seconds": tune_s, "tiled_deposit_scenes": tiled, "atomic_deposit_scenes": len(tuning) - tiled},
+            "autotune": {"seconds": tune_s, "tiled_deposit_scenes": tiled, "atomic_deposit_scenes": len(tuning) - tiled,
+                         "deposit_share_particles": sorted({tt["deposit_split"] for tt in tuning if tt["order"] == "tiled"}),
+                         "gather_caps": sorted({tt["gather_blocks"] for tt in tuning})},
             "partition": f"LPT over {world} rank(s)"}
 
 

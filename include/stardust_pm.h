@@ -347,8 +347,8 @@ int sd_poisson(const float* rho, int grid_size, float softening_cells, float* ph
 /* The same Poisson solve for callers that cannot allocate device memory: no
  * counterpart in the reference. Some callers cannot call cudaMalloc, or be handed
  * a workspace, on this path: code inside another component's allocation-free
- * hot loop, under a fixed memory budget that forbids growth after start-up, or
- * enqueuing work on a stream that someone else is capturing. This entry point
+ * hot loop, or under a fixed memory budget that forbids growth after start-up.
+ * This entry point
  * allocates nothing: its spectrum and tables live in fixed device storage of
  * the library, which every GPU that loads the library holds (about 9 MB) until
  * the process exits. grid_size must be a power of two in [16, 128]; larger
@@ -418,7 +418,7 @@ typedef struct sd_scene_tuning {
     int order;          /* SD_ORDER_TILED (fused deposit) or SD_ORDER_ROWMAJOR (atomic deposit) */
     int gather_blocks;  /* gather grid cap in CTAs (0: one CTA per 256 particles, at most 4096) */
     float step_ms;      /* median step time of the chosen variant alone; -1 before tuning */
-    int reserved;
+    int deposit_split;  /* window particles per CTA share of the fused deposit (0 with the atomic deposit) */
 } sd_scene_tuning;
 int sd_ensemble_create(sd_ensemble** out, int device);
 int sd_ensemble_destroy(sd_ensemble* ens);
@@ -426,7 +426,8 @@ int sd_ensemble_destroy(sd_ensemble* ens);
 int sd_ensemble_add(sd_ensemble* ens, const sd_config* cfg, const float* pos, const float* vel, int n, int where);
 int sd_ensemble_size(const sd_ensemble* ens);
 sd_sim* sd_ensemble_scene(sd_ensemble* ens, int index);
-/* times each scene's deposit path and gather grid on a snapshot (restored) and keeps the fastest */
+/* times each scene's deposit path, deposit share size and gather grid on a snapshot
+ * (restored) and keeps the fastest */
 int sd_ensemble_autotune(sd_ensemble* ens, float dt, int reps);
 int sd_ensemble_get_tuning(const sd_ensemble* ens, int index, sd_scene_tuning* out);
 /* nsteps steps of every scene: one graph launch per step, no host synchronisation */

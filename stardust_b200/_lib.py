@@ -78,7 +78,7 @@ class SdView(ctypes.Structure):
 
 class SdSceneTuning(ctypes.Structure):
     _fields_ = [("order", ctypes.c_int32), ("gather_blocks", ctypes.c_int32), ("step_ms", ctypes.c_float),
-                ("reserved", ctypes.c_int32)]
+                ("deposit_split", ctypes.c_int32)]
 
 
 class SdDiagnostics(ctypes.Structure):

@@ -11,6 +11,9 @@
 // The autotuner times, for every scene, each combination of
 //   deposit path  : fused tiled (pass A deposits from the row table) or
 //                   int64 atomics (row-major sort, separate deposit kernel)
+//   deposit share : for the fused path, the window particles one CTA takes before
+//                   a heavy bundle is split among several (3, 10 or 30 times the
+//                   mean window)
 //   gather grid   : 2, 4 or 8 CTAs per SM, or one CTA per 256 particles
 // on a snapshot of the scene (restored afterwards) and keeps the fastest.
 // The density of every choice is the same integer fixed-point sum, so the
@@ -42,7 +45,7 @@ struct SceneSlot {
     sd_scene_tuning tuning{};
     // what the graphs were captured with; any difference makes them stale
     const float4* expect_pos = nullptr;
-    int order = 0, gather_blocks = 0, N = 0, G = 0;
+    int order = 0, gather_blocks = 0, dep_split = 0, N = 0, G = 0;
     bool mlp_on = false;
 };
 
@@ -166,6 +169,7 @@ int build_graphs(sd_ensemble* e, float dt) {
         sl.expect_pos = s->pos;
         sl.order = s->cfg.order;
         sl.gather_blocks = s->gather_blocks;
+        sl.dep_split = s->dep_split;
         sl.N = s->N;
         sl.G = s->G;
         sl.mlp_on = s->mlp_on;
@@ -178,7 +182,7 @@ bool graphs_current(const sd_ensemble* e, float dt) {
     for (const auto& sl : e->scenes) {
         const sd_sim* s = sl.sim;
         if (s->pos != sl.expect_pos || s->cfg.order != sl.order || s->gather_blocks != sl.gather_blocks ||
-            s->N != sl.N || s->G != sl.G || s->mlp_on != sl.mlp_on || !graphable(s))
+            s->dep_split != sl.dep_split || s->N != sl.N || s->G != sl.G || s->mlp_on != sl.mlp_on || !graphable(s))
             return false;
     }
     return true;
@@ -322,6 +326,7 @@ int sd_ensemble_add(sd_ensemble* e, const sd_config* cfg, const float* pos, cons
     sl.tuning.order = s->cfg.order;
     sl.tuning.gather_blocks = 0;
     sl.tuning.step_ms = -1.f;
+    sl.tuning.deposit_split = 0;
     e->scenes.push_back(sl);
     drop_graphs(e);
     return (int)e->scenes.size() - 1;
@@ -343,6 +348,7 @@ int sd_ensemble_autotune(sd_ensemble* e, float dt, int reps) {
     if (SD_CUDA(cudaEventCreate(&a)) || SD_CUDA(cudaEventCreate(&b))) return SD_E_CUDA;
     const int orders[2] = {SD_ORDER_TILED, SD_ORDER_ROWMAJOR};
     const int caps[4] = {2 * kSmCount, 4 * kSmCount, 8 * kSmCount, 0};
+    const int mults[3] = {3, 10, 30};  // deposit share: times a window's mean particle count
     int rc = SD_OK;
     for (auto& sl : e->scenes) {
         if (rc) break;
@@ -353,28 +359,33 @@ int sd_ensemble_autotune(sd_ensemble* e, float dt, int reps) {
         Snapshot sn;
         rc = take_snapshot(s, sn);
         float best = 1e30f;
-        int best_order = s->cfg.order, best_cap = s->gather_blocks;
+        int best_order = s->cfg.order, best_cap = s->gather_blocks, best_split = s->dep_split;
         for (int o = 0; o < 2 && !rc; ++o)
-            for (int c = 0; c < 4 && !rc; ++c) {
-                s->cfg.order = orders[o];
-                s->gather_blocks = caps[c];
-                rc = restore_snapshot(s, sn);
-                float ms = 0.f;
-                if (!rc) rc = time_scene(s, dt, reps, a, b, &ms);
-                if (!rc && ms < best) {
-                    best = ms;
-                    best_order = orders[o];
-                    best_cap = caps[c];
+            for (int m = 0; m < (orders[o] == SD_ORDER_TILED ? 3 : 1) && !rc; ++m)
+                for (int c = 0; c < 4 && !rc; ++c) {
+                    s->cfg.order = orders[o];
+                    s->dep_split = orders[o] == SD_ORDER_TILED ? deposit_split(s->N, s->G, mults[m]) : 0;
+                    s->gather_blocks = caps[c];
+                    rc = restore_snapshot(s, sn);
+                    float ms = 0.f;
+                    if (!rc) rc = time_scene(s, dt, reps, a, b, &ms);
+                    if (!rc && ms < best) {
+                        best = ms;
+                        best_order = orders[o];
+                        best_cap = caps[c];
+                        best_split = s->dep_split;
+                    }
                 }
-            }
         s->cfg.order = best_order;
         s->gather_blocks = best_cap;
+        s->dep_split = best_split;
         if (!rc) rc = restore_snapshot(s, sn);
         if (!rc) rc = SD_CUDA(cudaStreamSynchronize(s->stream));
         free_snapshot(sn);
         sl.tuning.order = best_order;
         sl.tuning.gather_blocks = best_cap;
         sl.tuning.step_ms = best;
+        sl.tuning.deposit_split = best_split;
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);

@@ -149,9 +149,17 @@ constexpr int last_stage_ns(int N, int NT) {
     return ns;
 }
 
-// Stages from sub-transform length Ns on, stopping before the stage at STOP.
-template <int N, int Ns, int NT, int TWS, bool INV, int STOP = N>
-__device__ __forceinline__ void stages16(float2* s, const float2* tw) {
+// Element `pos` of line l as the first stage reads it: plainly, or through a
+// caller's functor that forms it from what s holds (a pre-processing step fused
+// into the first stage's loads, saving a shared-memory round trip and a barrier).
+struct PlainLoad {
+    __device__ __forceinline__ float2 operator()(const float2* s, int l, int pos) const { return s[pos * 16 + l]; }
+};
+
+// Stages from sub-transform length Ns on, stopping before the stage at STOP; the
+// stage at Ns = 1 reads through `load`.
+template <int N, int Ns, int NT, int TWS, bool INV, int STOP = N, class Load = PlainLoad>
+__device__ __forceinline__ void stages16(float2* s, const float2* tw, Load load = Load()) {
     if constexpr (Ns < N && Ns < STOP) {
         constexpr int R = radix_of<N / Ns, N, NT>::value;
         constexpr int NB = N / R;
@@ -165,7 +173,7 @@ __device__ __forceinline__ void stages16(float2* s, const float2* tw) {
                 const int l = u & 15, j = u >> 4, k = j % Ns;
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    float2 x = s[(j + r * NB) * 16 + l];
+                    float2 x = (Ns == 1) ? load(s, l, j + r * NB) : s[(j + r * NB) * 16 + l];
                     if (Ns > 1 && r > 0) {
                         float2 w = tw[(k * r * (N / (Ns * R))) * TWS];
                         if (INV) w.y = -w.y;
@@ -248,15 +256,16 @@ __device__ __forceinline__ void convolve16(float2* s, const float2* tw, Mul mul)
 }
 
 // lines16, with the last stage writing its outputs row-major (line l at
-// s[l * RS + position]) instead of interleaved, for callers that store rows.
-template <int N, int NT, int TWS, bool INV, int RS>
-__device__ __forceinline__ void lines16_rows(float2* s, const float2* tw) {
+// s[l * RS + position]) instead of interleaved, for callers that store rows; the
+// first stage reads through `load`.
+template <int N, int NT, int TWS, bool INV, int RS, class Load = PlainLoad>
+__device__ __forceinline__ void lines16_rows(float2* s, const float2* tw, Load load = Load()) {
     constexpr int NsL = last_stage_ns(N, NT);
     constexpr int R = N / NsL;
     constexpr int NB = N / R;
     constexpr int TOT = 16 * NB;
     constexpr int PER = (TOT + NT - 1) / NT;
-    stages16<N, 1, NT, TWS, INV, NsL>(s, tw);
+    stages16<N, 1, NT, TWS, INV, NsL>(s, tw, load);
     float2 v[PER][R];
 #pragma unroll
     for (int p = 0; p < PER; ++p) {
@@ -265,7 +274,7 @@ __device__ __forceinline__ void lines16_rows(float2* s, const float2* tw) {
             const int l = u & 15, j = u >> 4;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                float2 x = s[(j + r * NB) * 16 + l];
+                float2 x = (NsL == 1) ? load(s, l, j + r * NB) : s[(j + r * NB) * 16 + l];
                 if (NsL > 1 && r > 0) {
                     float2 w = tw[(j * r) * TWS];
                     if (INV) w.y = -w.y;

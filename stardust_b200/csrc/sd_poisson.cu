@@ -882,34 +882,25 @@ __global__ void __launch_bounds__(kFftThreads, 5) k_pass_e(const float2* __restr
         }
     }
     __syncthreads();
-    // X -> Z, pairs (k, H-k) in place:
-    //   Z[k] = E + i O,  E = X[k] + conj X[H-k],  O = (X[k] - conj X[H-k]) * exp(+2 pi i k / G)
-    // (imaginary parts of the k = 0 and k = H bins are dropped, as a C2R transform does)
-    constexpr int PAIRS = 16 * (H / 2 + 1);
-    for (int u = threadIdx.x; u < PAIRS; u += kFftThreads) {
-        const int l = u & 15, k = u >> 4;
+    // X -> Z inside the first stage's loads: Z[k] = E + i O with
+    //   E = X[k] + conj X[H-k],  O = (X[k] - conj X[H-k]) * exp(+2 pi i k / G)
+    // (imaginary parts of the k = 0 and k = H bins are dropped, as a C2R transform
+    // does), read from the staged bins, which the stage overwrites only after its
+    // barrier. This saves the separate pass over the pairs and its barrier.
+    auto c2r_load = [tw](const float2* s, int l, int k) {
         float2 a = s[k * 16 + l], b = s[(H - k) * 16 + l];
         if (k == 0) { a.y = 0.f; b.y = 0.f; }
-        {
-            const float2 w = tw[k];
-            const float er = a.x + b.x, ei = a.y - b.y, dr = a.x - b.x, di = a.y + b.y;
-            const float orr = dr * w.x + di * w.y, oi = di * w.x - dr * w.y;
-            s[k * 16 + l] = make_float2(er - oi, ei + orr);
-        }
-        if (k != 0 && 2 * k != H) {
-            const float2 w = tw[H - k];
-            const float er = b.x + a.x, ei = b.y - a.y, dr = b.x - a.x, di = b.y + a.y;
-            const float orr = dr * w.x + di * w.y, oi = di * w.x - dr * w.y;
-            s[(H - k) * 16 + l] = make_float2(er - oi, ei + orr);
-        }
-    }
-    __syncthreads();
+        const float2 w = tw[k];
+        const float er = a.x + b.x, ei = a.y - b.y, dr = a.x - b.x, di = a.y + b.y;
+        const float orr = dr * w.x + di * w.y, oi = di * w.x - dr * w.y;
+        return make_float2(er - oi, ei + orr);
+    };
     // The last stage leaves the lines row-major (stride H + 2 float2, 16-byte
     // aligned), so each warp then writes 512 contiguous bytes of one row instead
     // of 32 bytes of each of 16 rows.
     constexpr int RS = H + 2;
     static_assert(16 * RS <= 16 * T::PX, "row staging fits the line buffer");
-    fft::lines16_rows<H, kFftThreads, 2, true, RS>(s, tw);
+    fft::lines16_rows<H, kFftThreads, 2, true, RS>(s, tw, c2r_load);
     for (int u = threadIdx.x; u < 16 * (H / 2); u += kFftThreads) {
         const int l = u / (H / 2), mp = u % (H / 2);
         const size_t row = ((size_t)(bz * 4 + (l >> 2)) * G + by * 4 + (l & 3)) * G;
@@ -1054,12 +1045,12 @@ size_t deposit_work_ints(int G) {
     }
 }
 
-int deposit_split(int n, int G) {
-    // about ten times a window's mean particle count (a window spans 25 rows for a
-    // bundle's 16), and at least 2048: 4M particles on 256^3 (two galaxies) deposit in
-    // 0.163 ms with this, 0.179 with 5x, 0.196 with 3x, 0.218 with 2x
+int deposit_split(int n, int G, int mult) {
+    // by default about ten times a window's mean particle count (a window spans 25 rows
+    // for a bundle's 16), and at least 2048: 4M particles on 256^3 (two galaxies)
+    // deposit in 0.163 ms with this, 0.179 with 5x, 0.196 with 3x, 0.218 with 2x
     const long long nb = (long long)G * G / 16;
-    const long long t = 10ll * (long long)n / (nb > 0 ? nb : 1);
+    const long long t = (long long)(mult > 0 ? mult : 10) * (long long)n / (nb > 0 ? nb : 1);
     return (int)(t < 2048 ? 2048 : (t > (1 << 30) ? (1 << 30) : t));
 }
 
@@ -1152,8 +1143,8 @@ int build_green_table(const PoissonPlan& p, float softening_cells, float* kernel
 //
 // For callers that must not allocate device memory: code running where
 // cudaMalloc is not allowed, such as inside another library's allocator-free
-// hot loop, under a strict memory budget that forbids growth after start-up,
-// or on a stream being captured by someone else's graph. Its working memory
+// hot loop, or under a strict memory budget that forbids growth after start-up.
+// Its working memory
 // is file-scope device storage of fixed size, so grids are limited to
 // kNoAllocMaxGrid^3. Every GPU that loads this library holds that storage
 // (about 9 MB) until the process exits, and all calls on a device share it:

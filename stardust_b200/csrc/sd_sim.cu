@@ -524,7 +524,7 @@ int do_step(sd_sim* s, float dt, bool sort, bool timed) {
     DepositWork dw;
     dw.acc = s->acc;
     dw.ints = s->dep_ints;
-    dw.split = deposit_split(s->N, s->G);
+    dw.split = s->dep_split > 0 ? s->dep_split : deposit_split(s->N, s->G);
     if ((rc = launch_poisson_ex(s->plan, fused ? nullptr : s->acc, nullptr, fused ? s->pos : nullptr, perm,
                                 s->row_start, keep ? s->rho : nullptr, s->spec, s->phi, s->stream,
                                 timed ? s->pev : nullptr, iso_opts(s, io), &dw)))

@@ -98,6 +98,7 @@ struct sd_sim {
     bool mlp_on = false;
 
     int gather_blocks = 0;   // cap of the gather grid (0: the default); set by the ensemble autotuner
+    int dep_split = 0;       // window particles per CTA share of the fused deposit (0: deposit_split's default)
 
     // per-step FP64 diagnostics ring (cfg.diagnostics): kDiagCap records of 8 doubles
     double* diag_rec = nullptr;

@@ -81,7 +81,7 @@ class Ensemble:
         t = L.SdSceneTuning()
         L.check(L.lib().sd_ensemble_get_tuning(self._h, i, ctypes.byref(t)), "sd_ensemble_get_tuning")
         return {"order": ["rowmajor", "morton", "tiled"][t.order], "gather_blocks": t.gather_blocks,
-                "step_ms": t.step_ms}
+                "step_ms": t.step_ms, "deposit_split": t.deposit_split}
 
     def steps(self, dt: float, n: int) -> None:
         L.check(L.lib().sd_ensemble_steps(self._h, float(dt), int(n)), "sd_ensemble_steps")

@@ -101,6 +101,8 @@ def test_ensemble_density_bit_exact_against_solo_runs(cuda, tune):
         if tune:
             tun = ens.autotune(dt)
             assert all(t["step_ms"] > 0 for t in tun)
+            # the fused deposit's share size is tuned too (at least 2048 window particles per CTA)
+            assert all((t["deposit_split"] >= 2048) == (t["order"] == "tiled") for t in tun)
             orders = [{"tiled": L.SD_ORDER_TILED, "rowmajor": L.SD_ORDER_ROWMAJOR}[t["order"]] for t in tun]
         ens.steps(dt, 1)
         ens.synchronize()
