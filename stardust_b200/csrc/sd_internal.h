@@ -89,7 +89,8 @@ struct DepositWork {
 };
 size_t deposit_work_ints(int G);
 // the particles per CTA above which a window is split: mult times a window's mean count
-int deposit_split(int n, int G, int mult = 10);
+// (mult 0: 10 where the grid has at least 1024 row bundles, 5 below)
+int deposit_split(int n, int G, int mult = 0);
 int launch_poisson_ex(const PoissonPlan& p, const long long* acc, const float* rho, const float4* pos,
                       const int* perm, const int* row_start, float* keep, float2* spec, float* phi, cudaStream_t s,
                       cudaEvent_t* ev = nullptr, const PoissonIso* iso = nullptr, const DepositWork* dw = nullptr);

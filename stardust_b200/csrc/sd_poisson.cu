@@ -663,7 +663,7 @@ __device__ __forceinline__ void deposit_bundle(int b, int slice, int items, cons
 // early), then one CTA per bundle for its first share. 40 registers at G = 512
 // keep three 70 KB CTAs per SM; smaller grids need more for their FFT stages.
 template <int G>
-__global__ void __launch_bounds__(kDepositThreads, G >= 512 ? 3 : 2)
+__global__ void __launch_bounds__(kDepositThreads, G >= 128 ? 3 : 2)
     k_pass_a_deposit_bal(const float4* __restrict__ pos, const int* __restrict__ perm,
                          const int* __restrict__ row_start, float* __restrict__ rho_keep, float2* __restrict__ spec,
                          const float2* __restrict__ tw_g, DepositWork w) {
@@ -1046,11 +1046,14 @@ size_t deposit_work_ints(int G) {
 }
 
 int deposit_split(int n, int G, int mult) {
-    // by default about ten times a window's mean particle count (a window spans 25 rows
-    // for a bundle's 16), and at least 2048: 4M particles on 256^3 (two galaxies)
-    // deposit in 0.163 ms with this, 0.179 with 5x, 0.196 with 3x, 0.218 with 2x
+    // by default ten times a window's mean particle count (a window spans 25 rows for a
+    // bundle's 16) where the grid has at least 1024 bundles, five times below that, and at
+    // least 2048: 4M particles on 256^3 (two galaxies) deposit in 0.153 ms with 10x, 0.155
+    // with 5x, 0.163 with 3x; 262,144 on 64^3 (one disk, 256 bundles) in 0.048 ms with 10x,
+    // 0.040 with 5x, 0.042 with 3x
     const long long nb = (long long)G * G / 16;
-    const long long t = (long long)(mult > 0 ? mult : 10) * (long long)n / (nb > 0 ? nb : 1);
+    if (mult <= 0) mult = nb >= 1024 ? 10 : 5;
+    const long long t = (long long)mult * (long long)n / (nb > 0 ? nb : 1);
     return (int)(t < 2048 ? 2048 : (t > (1 << 30) ? (1 << 30) : t));
 }
 
