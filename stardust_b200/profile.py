@@ -3,6 +3,7 @@
     python -m stardust_b200.profile --workload cosmic_web_512 --steps 2
     python -m stardust_b200.profile --stage poisson --grid 512
     python -m stardust_b200.profile --stage mlp --steps 3
+    python -m stardust_b200.profile --workload zeldovich --lattice 128 --grid 512 --order 0
 
 --stage mlp runs the learned correction's inference (sd_mlp_infer) on the
 learned configuration's scene: 2,097,152 particles (Zel'dovich field, 128^3
@@ -28,6 +29,8 @@ def main(argv=None) -> int:
     ap.add_argument("--stage", choices=["step", "poisson", "mlp"], default="step")
     ap.add_argument("--grid", type=int, default=512)
     ap.add_argument("--order", type=int, default=2)
+    ap.add_argument("--lattice", type=int, default=0,
+                    help="with --workload zeldovich: the Zel'dovich field on this lattice (seed 2) on --grid")
     a = ap.parse_args(argv)
 
     import torch
@@ -67,7 +70,10 @@ def main(argv=None) -> int:
                           "wait_timeouts": int(L.lib().sd_mlp_wait_timeouts())}))
         return 0
 
-    if a.workload == "cosmic_web_512":
+    if a.workload == "zeldovich":
+        pos, vel = scenes.zeldovich(a.lattice or 128, 2)
+        G, dt = a.grid, 1e-3
+    elif a.workload == "cosmic_web_512":
         pos, vel = scenes.zeldovich(256, 2)
         G, dt = 512, 1e-3
     elif a.workload == "two_galaxy_256":
