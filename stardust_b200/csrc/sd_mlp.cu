@@ -129,8 +129,8 @@ __global__ void k_features(const float4* __restrict__ pos, const int* __restrict
 //
 // Measured against the mma.sync kernel it replaced (2,097,152 particles on 128^3,
 // identical outputs): 0.165 against 0.153 ms. The tensor pipe is 8 % busy; the
-// kernel is bound by the SiLU and feature work (special-function pipe 77 % with
-// the activations in shared memory), not by the products.
+// kernel waits on the feature gathers from L2 and on the SiLU's dependent chains
+// at four CTAs per SM (the tensor-memory columns), not on the products.
 namespace tc {
 constexpr int kThreads = 128;                  // one warpgroup: TMEM lanes 0..127
 constexpr int kTmemCols = 128;                 // FP32 accumulator (columns 0..63) + BF16 operand A (64..95)
@@ -143,6 +143,7 @@ constexpr int kBias = kB3 + kN3 * kH * 2;      // b1[64], b2[64], b3[8] (float)
 constexpr int kBar = kBias + (2 * kH + kOut) * 4 + 8;  // mbarrier (8-byte aligned)
 constexpr int kTaddr = kBar + 8;
 constexpr int kSmem = kTaddr + 8;
+constexpr int kSmemLaunch = 46 * 1024;  // at most four CTAs per SM (see launch_mlp_infer)
 static_assert(kBar % 8 == 0 && kB2 % 16 == 0 && kB3 % 16 == 0, "alignment");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -528,10 +529,14 @@ size_t mlp_param_count() { return kParams; }
 int launch_mlp_infer(const float* params, const float4* pos, const int* perm, int n, const float* rho, int G,
                      float inv_mean, float out_scale, float4* out, cudaStream_t s) {
     if (n <= 0) return SD_OK;
-    // tiles of 128 particles; four CTAs (128 TMEM columns each) fit on an SM
+    // tiles of 128 particles; four CTAs fill an SM's 512 tensor-memory columns (128 each).
+    // The dynamic shared memory is padded so that no fifth CTA is placed on an SM, where
+    // its tcgen05.alloc would wait for one of the four to finish.
+    static_assert(tc::kSmemLaunch >= tc::kSmem && 5 * (tc::kSmemLaunch + 1024) > 228 * 1024, "four CTAs per SM");
     const int tiles = (n + tc::kThreads - 1) / tc::kThreads;
     const int blocks = tiles < 148 * 4 ? tiles : 148 * 4;
-    k_mlp_infer_tc<<<blocks, tc::kThreads, tc::kSmem, s>>>(params, pos, perm, n, rho, G, inv_mean, out_scale, out);
+    k_mlp_infer_tc<<<blocks, tc::kThreads, tc::kSmemLaunch, s>>>(params, pos, perm, n, rho, G, inv_mean, out_scale,
+                                                                 out);
     SD_LAUNCHED(s);
     return SD_OK;
 }
