@@ -451,13 +451,44 @@ __global__ void k_copy_keys(const uint32_t* __restrict__ kin, const int32_t* __r
     vout[i] = vin ? vin[i] : i;
 }
 
-// Sorted row keys (tiled order: key = row) -> row_start[r] = first i with key >= r,
-// for r in [0, rows]; keys are below `rows`, so row_start[rows] = n.
-// One thread per row runs a lower-bound search over the keys. The work is the
-// same for every row, however the particles cluster: a scan that fills the rows
-// between consecutive keys leaves one thread to write every row of a long empty
-// run, and a clustered scene is mostly empty rows. Neighbouring rows take the
-// same first steps of the search, so those loads are shared in L1/L2.
+// Sorted row keys (tiled order: key = row, below `rows`) -> row_start[r] = first
+// position whose key is >= r, r = 0..rows (row_start[rows] = n). Thread per
+// position i in [0, n]: the rows r in (key[i-1], key[i]] start at i (position 0
+// takes the rows up to key[0], position n the rows after key[n-1]). One coalesced
+// pass over the keys instead of a lower-bound search per row (a chain of dependent
+// loads): a short run of empty rows is written by its own thread, a longer one is
+// queued and written by the whole CTA, so no thread walks a long empty stretch of
+// a clustered scene alone. Above 2^20 keys the CTAs of this pass outnumber a few
+// waves and a lower-bound search per row (k_row_bounds) is faster (4M keys of the
+// two-galaxy scene on 256^3: search 0.013 ms, this pass 0.017 ms; 262,144 keys of
+// the disk on 64^3: search 0.011 ms, this pass 0.007 ms).
+constexpr int kRowShortRun = 8;
+__global__ void __launch_bounds__(256) k_row_marks(const uint32_t* __restrict__ keys, int n, int rows,
+                                                   int* __restrict__ row_start) {
+    __shared__ int q_lo[256], q_hi[256], q_val[256];
+    __shared__ int q_count;
+    if (threadIdx.x == 0) q_count = 0;
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i <= n) {
+        const int prev = (i == 0) ? -1 : (int)__ldg(keys + i - 1);
+        const int cur = (i == n) ? rows : (int)__ldg(keys + i);
+        const int run = cur - prev;  // rows prev + 1 .. cur
+        if (run > kRowShortRun) {
+            const int slot = atomicAdd(&q_count, 1);
+            q_lo[slot] = prev + 1;
+            q_hi[slot] = cur;
+            q_val[slot] = i;
+        } else {
+            for (int r = prev + 1; r <= cur; ++r) row_start[r] = i;
+        }
+    }
+    __syncthreads();
+    for (int q = 0; q < q_count; ++q)
+        for (int r = q_lo[q] + (int)threadIdx.x; r <= q_hi[q]; r += blockDim.x) row_start[r] = q_val[q];
+}
+
+// One thread per row: a lower-bound search over the keys.
 __global__ void k_row_bounds(const uint32_t* __restrict__ keys, int n, int rows, int* __restrict__ row_start) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r > rows) return;
@@ -477,7 +508,10 @@ __global__ void k_row_bounds(const uint32_t* __restrict__ keys, int n, int rows,
 }  // namespace
 
 int launch_row_bounds(const uint32_t* keys, int n, int rows, int* row_start, cudaStream_t s) {
-    k_row_bounds<<<(rows + 1 + 255) / 256, 256, 0, s>>>(keys, n, rows, row_start);
+    if (n <= (1 << 20))
+        k_row_marks<<<(n + 1 + 255) / 256, 256, 0, s>>>(keys, n, rows, row_start);
+    else
+        k_row_bounds<<<(rows + 1 + 255) / 256, 256, 0, s>>>(keys, n, rows, row_start);
     SD_LAUNCHED(s);
     return SD_OK;
 }
