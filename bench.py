@@ -255,7 +255,7 @@ def run_ours(args, rank, world):
     e2e_ms = float(t.item())
     # the force error of the step's field: the accelerations of the current
     # positions against FP64 particle-mesh on the same grid, at 65,536 sampled
-    # particles (the FP64 direct/Ewald judge is reported by the learned comparison)
+    # particles (the error against FP64 Ewald forces is reported by the learned comparison)
     from stardust_b200.ewald import force_error, pm_accel_f64
 
     p_now, _ = sim.get_particles()

@@ -473,7 +473,7 @@ int sd_render_field(int field, const float* density, int grid_size, const float*
                     const sd_view* view, int width, int height, void* workspace, size_t workspace_bytes,
                     void* rgba_out, void* stream);
 
-/* ---- FP64 reference forces (force-error judge; not on the step) ------------
+/* ---- FP64 reference forces (force-error reference; not on the step) ------------
  * Periodic Newtonian accelerations (G = 1, each source of mass 1/n_src, mean
  * density removed) of Gaussian-smoothed masses of width `softening` (box units;
  * the PM step's softening_cells / grid_size), by Ewald summation in FP64:

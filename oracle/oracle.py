@@ -353,7 +353,7 @@ def force_error(a: np.ndarray, a_ref: np.ndarray) -> dict:
 
 def ewald_forces_f64(src: np.ndarray, tgt: np.ndarray, softening: float, split_b: float, nmax: int) -> np.ndarray:
     """FP64 Ewald forces of Gaussian-smoothed masses, vectorised numpy (small
-    systems only): the same split as the GPU judge, written independently.
+    systems only): the same split as the GPU Ewald kernels, written independently.
     Long range over modes 0 < |n| <= nmax (all of them, no half-space folding),
     short range over all sources at their nearest image with the pair kernel
     -m [erf(r/a) - erf(r/b)]/r, a = sqrt(2) softening."""

@@ -1,4 +1,4 @@
-// sd_ewald.cu -- FP64 reference forces by Ewald summation (the accuracy judge).
+// sd_ewald.cu -- FP64 reference forces by Ewald summation (the accuracy reference).
 //
 // The model is the one the periodic PM step approximates (Green's function of
 // kPoissonPeriodic, Sim.cu:528-557): Newtonian gravity in the unit periodic box,
@@ -13,7 +13,7 @@
 //   phi_s(r) = -m [erf(r/a) - erf(r/b)] / r,   a = sqrt(2) s,
 // which decays like a Gaussian of width b and is summed over all sources at
 // their nearest periodic image (r_cut = 0.5 must exceed a few b).
-// Everything is FP64. These kernels judge force errors; they are not on the
+// Everything is FP64. These kernels measure force errors; they are not on the
 // simulation path.
 #include <cuda_runtime.h>
 #include <math.h>

@@ -1,4 +1,4 @@
-"""FP64 reference forces and force errors (the accuracy judge of the PM step).
+"""FP64 reference forces and force errors (the accuracy reference for the PM step).
 
 ``ewald_forces`` calls the library's FP64 Ewald summation (sd_ewald_forces):
 periodic Newtonian gravity of Gaussian-smoothed masses (G = 1, total mass 1),
@@ -50,7 +50,7 @@ def pm_accel_f64(pos, sample, grid: int, pot_scale: float, softening_cells: floa
     units), the periodic Green's function -exp(-k^2 s^2 / 2) / (4 pi^2 k^2) with
     s = 2 pi softening_cells / grid (k = 0 dropped), central differences
     -(phi[+1] - phi[-1]) * grid / 2 * pot_scale at the 8 CIC corners, the CIC
-    weights again (the conventions of Sim.cu:503-629). The judge of the FP32
+    weights again (the conventions of Sim.cu:503-629). The reference for the FP32
     step's arithmetic: the same method, with no rounding to speak of.
 
     pos: float32 (n, 4) host array; sample: indices of live particles."""

@@ -6,7 +6,7 @@ accumulation on the tensor cores) maps a particle's coarse-grid features -- the
 its sub-cell offset -- to the residual between a fine-grid PM acceleration and
 the coarse one. The step adds ``out_scale * MLP(features)`` to the coarse PM
 acceleration before the kick (``Sim.set_correction``); plain PM stays the
-fallback (no correction set) and the judge of the error.
+fallback (no correction set) and the yardstick of the error.
 
 Everything on the GPU runs through the library's own kernels: features
 (``sd_mlp_features``), forward and backward passes (``sd_mlp_loss_grad``), the
@@ -258,7 +258,7 @@ def equal_error_rate(err: float, plain: dict) -> float | None:
 def compare(train_seeds=range(8), eval_seed: int = 1000, n_side: int = 128, coarse: int = 128, fine: int = 512,
             softening: float = 1.0 / 128, n_targets: int = 65_536, epochs: int = 10, steps: int = 20,
             log=None) -> dict:
-    """Train on (coarse, fine) pairs of `train_seeds`, then judge plain PM on
+    """Train on (coarse, fine) pairs of `train_seeds`, then measure plain PM on
     coarse..fine grids and coarse + correction on a held-out scene against FP64
     Ewald forces at `n_targets` particles, and time each step."""
     torch = _torch()
@@ -291,7 +291,7 @@ def compare(train_seeds=range(8), eval_seed: int = 1000, n_side: int = 128, coar
     eq = equal_error_rate(learned["error"], plain)
     out = {
         "scene": f"Zel'dovich {n_side}^3 lattice (seed {eval_seed}), softening {softening:.6g} box",
-        "judge": f"FP64 Ewald, {n_targets} targets, all {len(pos)} sources",
+        "error_reference": f"FP64 Ewald, {n_targets} targets, all {len(pos)} sources",
         "plain": {str(k): v for k, v in plain.items()},
         "learned": learned,
         "train": {"seeds": list(train_seeds), "pairs": f"{coarse}^3 vs {fine}^3", "epochs": epochs,

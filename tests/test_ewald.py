@@ -1,4 +1,4 @@
-"""The FP64 Ewald judge: oracle self-consistency (CPU) and the GPU kernel against
+"""The FP64 Ewald reference forces: oracle self-consistency (CPU) and the GPU kernel against
 the oracle (GPU)."""
 import numpy as np
 import pytest
@@ -59,8 +59,8 @@ def test_gpu_ewald_two_particles_is_newtonian_at_short_range(cuda, lib):
     assert a[0, 0] == pytest.approx(m / r ** 2, rel=2e-3)
 
 
-def test_fp64_pm_judge_matches_the_oracle(oracle):
-    """The FP64 particle-mesh judge the benchmark reports the force error against
+def test_fp64_pm_reference_matches_the_oracle(oracle):
+    """The FP64 particle-mesh reference the benchmark reports the force error against
     (stardust_b200.ewald.pm_accel_f64) is the oracle's FP64 PM on the same grid."""
     from stardust_b200.ewald import pm_accel_f64
 

@@ -1,6 +1,6 @@
 """The learned sub-grid correction inside the step: the correction off or zero is
 the plain PM step, the in-step inference matches the oracle MLP, eager and
-graph-replayed steps agree, and a trained network lowers the FP64-judged force
+graph-replayed steps agree, and a trained network lowers the FP64-measured force
 error of the coarse grid on a scene it was not trained on."""
 import numpy as np
 import pytest
@@ -81,7 +81,7 @@ def test_graph_replay_with_correction_matches_eager_steps(cuda):
 @pytest.mark.gpu
 def test_trained_correction_lowers_fp64_force_error(cuda):
     """32^3-particle scenes, 32^3 coarse grid, 128^3 fine grid, one softening
-    (1/32 box) for both: train on 4 seeds, judge a held-out seed against the
+    (1/32 box) for both: train on 4 seeds, measure a held-out seed against the
     FP64 Ewald forces of the same smoothed-mass model."""
     from stardust_b200.ewald import ewald_forces, force_error
     from stardust_b200.learned import Correction, PMField, train, training_pairs
