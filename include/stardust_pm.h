@@ -353,8 +353,8 @@ int sd_poisson(const float* rho, int grid_size, float softening_cells, float* ph
  * the library, which every GPU that loads the library holds (about 9 MB) until
  * the process exits. grid_size must be a power of two in [16, 128]; larger
  * grids are rejected with SD_E_ARG. The first call on a device resolves that
- * storage and uploads the twiddle tables (synchronously), so make it before any
- * stream capture. All calls on a device share the storage: calls that overlap
+ * storage and uploads the twiddle tables, synchronously (it waits for the
+ * device). All calls on a device share the storage: calls that overlap
  * on the GPU (different streams, no ordering between them) race and give wrong
  * results. rho and phi are caller device buffers of grid_size^3 floats. */
 int sd_poisson_noalloc(const float* rho, int grid_size, float softening_cells, float* phi, void* stream);
